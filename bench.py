@@ -1,0 +1,374 @@
+"""Benchmark of the B200 assembly + Jacobi-PCG path.
+
+Default workload: 3D vector-P1 linear elasticity on the box [0,4]x[0,1]x[0,1],
+128x32x32 hexahedra split into 6 tetrahedra each (786,432 tets, 421,443 dofs),
+E = 210e9, nu = 0.3, clamped at x = 0, body force (0, 0, -7.8e4); solved to
+1e-8 relative residual with mixed-precision refined PCG (FP32 SpMV/axpy inside
+FP64 residual replacement), next to the plain FP64 PCG on the same card.
+
+One step = assemble the stiffness (FP64 + FP32 values) + body force +
+Dirichlet elimination + mixed PCG to 1e-8, inputs resident in HBM. The
+metric is dofs / step time (DOF/s). Inputs are synthetic (generated meshes).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+                    [--config c2|c2p|c1|c3|c4|c5]
+
+--impl reference times the CPU restatement of the reference path (the
+reference itself is Rust and cannot be built here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "fenics-rs_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "DOF/s to 1e-8 rel. residual: mixed-prec vs FP64 CG on 1 B200; assembly GB/s"
+
+CONFIGS = {
+    # name: (description, builder kwargs)
+    "c2": dict(workload="3D vector-P1 elasticity, box [0,4]x[0,1]x[0,1], 128x32x32 hexes x 6 tets "
+                        "(786,432 tets, 421,443 dofs), E=210e9, nu=0.3, clamped x=0, body force (0,0,-7.8e4), "
+                        "mixed-precision refined PCG to 1e-8 vs FP64 PCG",
+               L=4.0, W=1.0, H=1.0, nx=128, ny=32, nz=32),
+    "c2p": dict(workload="3D vector-P1 elasticity, box [0,4]x[0,1]x[0,1], 200x50x50 hexes x 6 tets "
+                         "(3,000,000 tets, 1,568,403 dofs), E=210e9, nu=0.3, clamped x=0, body force (0,0,-7.8e4), "
+                         "mixed-precision refined PCG to 1e-8 vs FP64 PCG",
+                L=4.0, W=1.0, H=1.0, nx=200, ny=50, nz=50),
+}
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _profile_traffic(name: str):
+    """DRAM bytes per launch recorded by an ncu capture summary under profiles/."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU (oracle) timing — the reference arm and the cpu_baseline leg
+# ---------------------------------------------------------------------------
+
+def cpu_reference_run(cfg, iters_full: int | None, sample_iters: int = 150):
+    """Time the CPU restatement: OpenMP assembly (rayon par_iter equivalent) +
+    serial faer-style triplet->CSC build, serial body force, Dirichlet, and a
+    bounded sample of sequential Jacobi-PCG iterations (cg.rs is sequential),
+    extrapolated to the full iteration count."""
+    import oracle as O
+    om = O.box_beam(cfg["L"], cfg["W"], cfg["H"], cfg["nx"], cfg["ny"], cfg["nz"])
+    dofs = O.clamp_dofs(om)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    K = O.assemble_elasticity_3d(om, 210e9, 0.3, threads=cores)
+    f = O.body_force_3d(om, [0.0, 0.0, -7.8e4])
+    Kb, fb = O.apply_dirichlet_bc(K, f, dofs, np.zeros(len(dofs)))
+    t_setup = time.perf_counter() - t0
+    del K
+    t1 = time.perf_counter()
+    _, rel = O.cg_fixed_iters(Kb, fb, sample_iters)
+    t_iter = (time.perf_counter() - t1) / sample_iters
+    if iters_full is None:
+        iters_full = 2010  # FP64 Jacobi-PCG iterations to 1e-8 at 128x32x32 (scipy probe of the same iteration)
+    t_total = t_setup + t_iter * iters_full
+    n = 3 * om.nv
+    return {
+        "value": n / t_total, "unit": "DOF/s", "cores": cores, "kind": "port",
+        "sample": f"assembly+body force+Dirichlet in full ({t_setup:.2f} s, {cores} threads for the cell loop), "
+                  f"{sample_iters} sequential PCG iterations ({t_iter * 1e3:.1f} ms each) extrapolated to "
+                  f"{iters_full} iterations",
+        "seconds_sampled": t_setup + t_iter * sample_iters,
+    }
+
+
+# ---------------------------------------------------------------------------
+# GPU run
+# ---------------------------------------------------------------------------
+
+def run_cuda(args, cfg):
+    import torch
+    import fenics_cuda as fcu
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    if dist:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = local if dist else 0
+    torch.cuda.set_device(dev)
+    ctx = fcu.Context(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{dev}")
+
+    mesh = fcu.box_beam(cfg["L"], cfg["W"], cfg["H"], cfg["nx"], cfg["ny"], cfg["nz"])
+    nv, nc = mesh.nv, mesh.nc
+    n = 3 * nv
+    clamp_v = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+    dofs = (3 * clamp_v[:, None] + np.arange(3)).ravel().astype(np.int64)
+    fbody = np.array([0.0, 0.0, -7.8e4])
+
+    # setup (untimed): mesh upload, pattern, matrix storage, device inputs
+    t_setup0 = time.perf_counter()
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+    M = fcu.Matrix(ctx, V)
+    t_setup = time.perf_counter() - t_setup0
+    dofs_d = torch.from_numpy(dofs).to(f"cuda:{dev}")
+    vals_d = torch.zeros(len(dofs), dtype=torch.float64, device=f"cuda:{dev}")
+    fbody_d = torch.from_numpy(fbody).to(f"cuda:{dev}")
+    b_d = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
+    x_d = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")  # 256 MiB > L2
+
+    def step(precision):
+        M.assemble_elasticity(210e9, 0.3)
+        V.body_force(fbody_d, out=b_d)
+        M.apply_dirichlet(b_d, dofs_d, vals_d)
+        _, info = M.pcg(b_d, x=x_d, tol=1e-8, max_iter=100000, precision=precision)
+        return info
+
+    def timed_steps(k, precision):
+        times, infos = [], []
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            infos.append(step(precision))
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return times, infos
+
+    # warm-up (also captures the CUDA graphs)
+    for _ in range(args.warmup):
+        step(fcu.FCU_MIXED)
+        step(fcu.FCU_FP64)
+
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    with ClockSampler(dev) as clk:
+        t_mixed, info_mixed = timed_steps(args.steps, fcu.FCU_MIXED)
+    torch.cuda.synchronize()
+    launches = ctx.kernel_launches - launches0
+    if dist:
+        tdist.barrier()
+    t_fp64, info_fp64 = timed_steps(max(1, args.steps), fcu.FCU_FP64)
+
+    ms_mixed = sum(t_mixed) / len(t_mixed)
+    ms_fp64 = sum(t_fp64) / len(t_fp64)
+    if dist:
+        tt = torch.tensor([ms_mixed, ms_fp64], device=f"cuda:{dev}")
+        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+        ms_mixed, ms_fp64 = tt.tolist()
+
+    # assembly alone: FP64 + FP32 values of the raw pattern, events on the ctx stream
+    reps = 10
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        flush.fill_(2.0)
+    e0.record(stream)
+    for _ in range(reps):
+        M.assemble_elasticity(210e9, 0.3)
+    e1.record(stream)
+    e1.synchronize()
+    ms_asm = e0.elapsed_time(e1) / reps
+    nnzb = V.nnz // 9
+    asm_bytes = nc * (4 * 4 + 4 * 16 + 8) + nv * 3 * 8 + (nnzb * 9) * (8 + 4)
+    # re-establish the solved system for the SpMV timing
+    step(fcu.FCU_MIXED)
+
+    # dominant kernel: the FP32 3x3-block SpMV of the mixed PCG
+    spmv_ms, spmv_bytes = M.time_spmv(fcu.FCU_MIXED, reps=50)
+    spmv64_ms, spmv64_bytes = M.time_spmv(fcu.FCU_FP64, reps=20)
+    peak, peak_kind = _peaks()
+    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    traffic = _profile_traffic("spmv_bsr3_fp32_elasticity_c2.txt")
+
+    # e2e through the public API from pinned host buffers
+    e2e_ms = []
+    host_coords = torch.from_numpy(mesh.coords).pin_memory()
+    host_cells = torch.from_numpy(mesh.cells).pin_memory()
+    bc = fcu.VectorDirichletBC([(int(d), 0.0) for d in dofs])
+    material = fcu.ElasticMaterial(210e9, 0.3)
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m_h = fcu.Mesh(host_coords.numpy(), host_cells.numpy())
+        sol = fcu.solve_elasticity_3d(m_h, material, fbody, bc, 1e-8, 100000, ctx=ctx, precision=fcu.FCU_MIXED)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        m_h.release()
+    h2d = mesh.coords.nbytes + mesh.cells.nbytes + len(dofs) * 16 + 24
+    d2h = n * 8
+
+    it_m = info_mixed[-1].iterations
+    it_f = info_fp64[-1].iterations
+    res = {
+        "metric": METRIC,
+        "value": n * world / (ms_mixed * 1e-3),
+        "unit": "DOF/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_mixed,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 SpMV/axpy + f64 residual/dots (mixed); f64 assembly",
+        "data": "synthetic (generated box mesh, no dataset)",
+        "config": {"workload": cfg["workload"], "ndofs": n, "cells": nc, "l2": "256 MiB write between steps",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp64": {"value": n * world / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64, "iterations": it_f},
+        "mixed": {"iterations": it_m, "residual_replacements": info_mixed[-1].outer_updates,
+                  "rel_residual_fp64": info_mixed[-1].rel_residual},
+        "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
+        "assembly": {"ms": ms_asm, "gbs": asm_bytes / (ms_asm * 1e-3) / 1e9, "bytes": asm_bytes,
+                     "frac_of_" + peak_kind + "_hbm": asm_bytes / (ms_asm * 1e-3) / 1e9 / peak},
+        "spmv_fp64": {"ms": spmv64_ms, "gbs": spmv64_bytes / (spmv64_ms * 1e-3) / 1e9, "bytes": spmv64_bytes},
+        "roofline": {"kernel": "k_spmv_ap<3,16,float> (FP32 3x3-block SpMV + p.Ap)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "bytes_per_launch": spmv_bytes},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+        "e2e": {"value": n / (min(e2e_ms) * 1e-3), "unit": "DOF/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms": min(e2e_ms),
+                "what": "fenics_cuda.solve_elasticity_3d from pinned host mesh/BC arrays: mesh upload, pattern "
+                        "build, assembly, body force, Dirichlet, mixed PCG, solution download"},
+        "setup_s": t_setup,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        res["cpu_baseline"] = cpu_reference_run(cfg, it_f)
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    ctx.close()
+    return res if rank == 0 else None
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    runs = []
+    for _ in range(max(1, args.steps)):
+        runs.append(cpu_reference_run(cfg, None, sample_iters=60))
+    vals = [r["value"] for r in runs]
+    v = statistics.median(vals)
+    base = runs[0]
+    return {
+        "metric": METRIC, "value": v, "unit": "DOF/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated box mesh)",
+        "config": {"workload": cfg["workload"]}, "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "DOF/s", "cores": base["cores"], "kind": "port",
+                         "sample": base["sample"]},
+        "e2e": {"value": v, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (Rust) cannot be built in this image; its path is timed through the C++ "
+                "restatement under oracle/",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    res = run_reference(args, cfg) if args.impl == "reference" else run_cuda(args, cfg)
+    if res is not None:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,559 @@
+// Matrix assembly kernels (scalar P1/P2 Poisson stiffness, vector-P1
+// elasticity), Dirichlet elimination, and the adjoint gradient kernel.
+//
+// Layout in HBM
+//   scalar spaces: CSR over dofs, val[p] for slot p of row i (p in row_ptr[i]..)
+//   vector space : CSR over vertices with 3x3 blocks, val[9p + 3*alpha + beta]
+//                  is the (3i+alpha, 3j+beta) entry of block slot p = (i, j)
+// Both FP64 and FP32 values are written by the same pass.
+//
+// Work decomposition: one warp per row. The warp first evaluates, for each
+// cell that contains the row's node (the row's "contributions", ascending
+// cell id), that cell's element row into shared memory; then each lane owns a
+// slot and sums the entries listed for it, in ascending cell order; finally
+// the row is written with coalesced stores. Each cell is evaluated once per
+// node it has (k times), and every value is written exactly once, so no
+// atomics and no zero-fill pass are needed, and the result is deterministic.
+
+#include "internal.cuh"
+
+namespace {
+
+constexpr int WARPS = 8;   // warps per block, scalar assembly
+constexpr int EWARPS = 6;  // warps per block, elasticity assembly (shared-memory bound)
+// Staging rows use odd strides (in doubles) so that lanes writing "their" row
+// hit distinct banks.
+constexpr int odd_stride(int k) { return (k % 2) ? k : k + 1; }
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  *total = __shfl_sync(FULL, x, 31);
+  return x - v;
+}
+
+// ---------------------------------------------------------------------------
+// Scalar stiffness: P1 triangle (k=3), P1 tetrahedron (k=4), P2 tet (k=10).
+// Element row a of cell c is staged as stage[t][b] = K_e[a][b].
+// ---------------------------------------------------------------------------
+
+// Symmetrised reference tensors of the P2 tetrahedron for the degree-2 Keast
+// rule: R[m][a][b] with m over the metric entries (00,11,22,01,02,12); the
+// off-diagonal ones hold R^{de}+R^{ed}. Filled from the host at first use.
+__constant__ double c_p2_R[6][10][10];
+
+template <int K, int DIM>
+__device__ __forceinline__ void p1_element_row(const double* __restrict__ X, const int* __restrict__ cn, int c, int a,
+                                               double coef, double* out) {
+  int v[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) v[i] = cn[(i64)c * K + i];
+  if (DIM == 3) {
+    Geo3 g = tet_geometry(X, v);
+    // gradients of the P1 basis: g_0 = -(G e0 + G e1 + G e2), g_i = G e_{i-1}
+    double gr[4][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      gr[1][r] = g.G[r][0];
+      gr[2][r] = g.G[r][1];
+      gr[3][r] = g.G[r][2];
+      gr[0][r] = -g.G[r][0] - g.G[r][1] - g.G[r][2];
+    }
+    double s = (1.0 / 6.0) * fabs(g.det) * coef;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) out[b] = (gr[a][0] * gr[b][0] + gr[a][1] * gr[b][1] + gr[a][2] * gr[b][2]) * s;
+  } else {
+    Geo2 g = tri_geometry(X, v);
+    double gr[3][2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      gr[1][r] = g.G[r][0];
+      gr[2][r] = g.G[r][1];
+      gr[0][r] = -g.G[r][0] - g.G[r][1];
+    }
+    double s = 0.5 * fabs(g.det) * coef;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) out[b] = (gr[a][0] * gr[b][0] + gr[a][1] * gr[b][1]) * s;
+  }
+}
+
+// Metric S = G^T G scaled by kappa*|det J| (6 entries, off-diagonals doubled
+// are folded into the tensors instead).
+__device__ __forceinline__ void p2_metric(const double* __restrict__ X, const int* __restrict__ cn, int c, double coef,
+                                          double* S) {
+  int v[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = cn[(i64)c * 10 + i];
+  Geo3 g = tet_geometry(X, v);
+  double s = fabs(g.det) * coef;
+  // (G^T G)_{de} = sum_r G[r][d] G[r][e]
+  const int D[6] = {0, 1, 2, 0, 0, 1}, E[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int m = 0; m < 6; ++m)
+    S[m] = (g.G[0][D[m]] * g.G[0][E[m]] + g.G[1][D[m]] * g.G[1][E[m]] + g.G[2][D[m]] * g.G[2][E[m]]) * s;
+}
+
+template <int K, int DIM, bool IS_P2>
+__global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
+    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+    const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
+    const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ coef, i64 nrows,
+    double* __restrict__ v64, float* __restrict__ v32) {
+  constexpr int KS = odd_stride(K);
+  __shared__ double stage_all[WARPS][32][KS];
+  __shared__ double metric_all[IS_P2 ? WARPS : 1][32][7];
+  __shared__ int sa_all[IS_P2 ? WARPS : 1][32];
+  __shared__ double R[IS_P2 ? 6 * 100 : 1];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (IS_P2) {
+    for (int t = threadIdx.x; t < 600; t += blockDim.x) R[t] = (&c_p2_R[0][0][0])[t];
+    __syncthreads();
+  }
+  double(*stage)[KS] = stage_all[wib];
+  const i64 nwarps = (i64)gridDim.x * WARPS;
+  for (i64 row = (i64)blockIdx.x * WARPS + wib; row < nrows; row += nwarps) {
+    const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
+    const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
+    const i64 ebase = (i64)K * cs;
+    int run = 0;  // entries consumed by earlier slot groups
+    for (int g0 = 0; g0 < L; g0 += 32) {
+      const int s = g0 + lane;
+      const int cnt = (s < L) ? (int)slot_cnt[rs + s] : 0;
+      int tot;
+      const int off = warp_excl_scan(cnt, lane, &tot);
+      i64 e = ebase + run + off;
+      const i64 e1 = e + cnt;
+      run += tot;
+      double acc = 0.0;
+      for (int ch = 0; ch < nct; ch += 32) {
+        // stage element rows of contributions ch .. ch+31
+        const int t = ch + lane;
+        if (IS_P2) {
+          if (t < nct) {
+            int cc = contrib[cs + t];
+            p2_metric(X, cn, cc >> 4, coef ? coef[cc >> 4] : 1.0, metric_all[wib][lane]);
+            sa_all[wib][lane] = cc & 15;
+          }
+          __syncwarp();
+          const int nt = min(32, nct - ch);
+          for (int q = lane; q < nt * K; q += 32) {
+            const int tt = q / K, b = q - tt * K;
+            const int a = sa_all[wib][tt];
+            const double* S = metric_all[wib][tt];
+            double v = 0.0;
+#pragma unroll
+            for (int m = 0; m < 6; ++m) v += S[m] * R[m * 100 + a * 10 + b];
+            stage[tt][b] = v;
+          }
+        } else {
+          if (t < nct) {
+            int cc = contrib[cs + t];
+            p1_element_row<K, DIM>(X, cn, cc >> 4, cc & 15, coef ? coef[cc >> 4] : 1.0, stage[lane]);
+          }
+        }
+        __syncwarp();
+        while (e < e1) {
+          const unsigned ent = slot_ent[e];
+          const int tl = (int)(ent >> 4);
+          if (tl >= ch + 32) break;
+          acc += stage[tl - ch][ent & 15];
+          ++e;
+        }
+        __syncwarp();
+      }
+      if (s < L) {
+        v64[rs + s] = acc;
+        v32[rs + s] = (float)acc;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Vector-P1 elasticity (elasticity.rs:73-149). For block (i, j) of a cell:
+//   K_{i a, j b} = vol (lam g_j[b] g_i[a] + mu (g_i.g_j) d_ab + mu g_j[a] g_i[b])
+// = (lam M + mu M^T + mu tr(M) I)[a][b] with M = vol g_i g_j^T. The kernel sums
+// M over the cells of each block (per-cell moduli folded into vol), then forms
+// the block once. Staged per contribution: h = s_e g_i (3) and g_0..g_3 (12).
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
+    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+    const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
+    const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ cellE, double lam,
+    double mu, i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
+  __shared__ double st_all[EWARPS][32][17];
+  __shared__ double out_all[EWARPS][32 * 9];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double(*st)[17] = st_all[wib];
+  double* out = out_all[wib];
+  const i64 nwarps = (i64)gridDim.x * EWARPS;
+  for (i64 row = (i64)blockIdx.x * EWARPS + wib; row < nrows; row += nwarps) {
+    const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
+    const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
+    const i64 ebase = 4 * (i64)cs;
+    int run = 0;
+    for (int g0 = 0; g0 < L; g0 += 32) {
+      const int s = g0 + lane;
+      const int cnt = (s < L) ? (int)slot_cnt[rs + s] : 0;
+      int tot;
+      const int off = warp_excl_scan(cnt, lane, &tot);
+      i64 e = ebase + run + off;
+      const i64 e1 = e + cnt;
+      run += tot;
+      double M[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) M[q] = 0.0;
+      for (int ch = 0; ch < nct; ch += 32) {
+        const int t = ch + lane;
+        if (t < nct) {
+          const int cc = contrib[cs + t];
+          const int c = cc >> 4, a = cc & 15;
+          int v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) v[i] = cn[4 * (i64)c + i];
+          Geo3 g = tet_geometry(X, v);
+          double sc = (1.0 / 6.0) * fabs(g.det);
+          if (cellE) sc *= cellE[c];
+          double* w = st[lane];
+#pragma unroll
+          for (int r = 0; r < 3; ++r) {
+            w[3 + r] = -g.G[r][0] - g.G[r][1] - g.G[r][2];
+            w[6 + r] = g.G[r][0];
+            w[9 + r] = g.G[r][1];
+            w[12 + r] = g.G[r][2];
+          }
+#pragma unroll
+          for (int r = 0; r < 3; ++r) w[r] = sc * w[3 + 3 * a + r];
+        }
+        __syncwarp();
+        while (e < e1) {
+          const unsigned ent = slot_ent[e];
+          const int tl = (int)(ent >> 4);
+          if (tl >= ch + 32) break;
+          const double* w = st[tl - ch];
+          const int b = ent & 15;
+          const double h0 = w[0], h1 = w[1], h2 = w[2];
+          const double q0 = w[3 + 3 * b], q1 = w[4 + 3 * b], q2 = w[5 + 3 * b];
+          M[0] += h0 * q0; M[1] += h0 * q1; M[2] += h0 * q2;
+          M[3] += h1 * q0; M[4] += h1 * q1; M[5] += h1 * q2;
+          M[6] += h2 * q0; M[7] += h2 * q1; M[8] += h2 * q2;
+          ++e;
+        }
+        __syncwarp();
+      }
+      const double tr = mu * (M[0] + M[4] + M[8]);
+      if (s < L) {
+        double* o = out + 9 * lane;
+#pragma unroll
+        for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+          for (int b2 = 0; b2 < 3; ++b2)
+            o[3 * a2 + b2] = lam * M[3 * a2 + b2] + mu * M[3 * b2 + a2] + (a2 == b2 ? tr : 0.0);
+      }
+      __syncwarp();
+      const int nb = min(32, L - g0);
+      const i64 base = 9 * ((i64)rs + g0);
+      for (int q = lane; q < 9 * nb; q += 32) {
+        const double v = out[q];
+        v64[base + q] = v;
+        v32[base + q] = (float)v;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dirichlet elimination (poisson.rs:222-263, elasticity.rs:188-227)
+// ---------------------------------------------------------------------------
+
+__global__ void k_bc_mark(const i64* __restrict__ dofs, i64 nbc, i64 n, int* __restrict__ count, int* __restrict__ last,
+                          int* __restrict__ bad) {
+  for (i64 j = blockIdx.x * (i64)blockDim.x + threadIdx.x; j < nbc; j += (i64)gridDim.x * blockDim.x) {
+    i64 d = dofs[j];
+    if (d < 0 || d >= n) { atomicExch(bad, 1); continue; }
+    atomicAdd(&count[d], 1);
+    atomicMax(&last[d], (int)j);
+  }
+}
+
+__global__ void k_bc_flags(const int* __restrict__ count, const int* __restrict__ last, const double* __restrict__ vals,
+                           i64 n, unsigned char* __restrict__ dir, double* __restrict__ g, double* __restrict__ dcount) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    int c = count[i];
+    if (c > 0) {
+      dir[i] = 1;
+      g[i] = vals[last[i]];
+      dcount[i] = (double)c;
+    } else {
+      g[i] = 0.0;
+    }
+  }
+}
+
+// Lifting: b_r -= a_rc g_c over eliminated-now columns c in ascending order,
+// for rows r not eliminated now (uses values before elimination).
+template <int BS>
+__global__ void k_bc_lift(const int* __restrict__ row_ptr, const int* __restrict__ col_idx,
+                          const double* __restrict__ v64, const int* __restrict__ count, const double* __restrict__ g,
+                          i64 nn, double* __restrict__ b) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nn * BS; t += (i64)gridDim.x * blockDim.x) {
+    const i64 node = t / BS;
+    const int al = (int)(t - node * BS);
+    if (count[t] > 0) continue;
+    double acc = b[t];
+    for (int p = row_ptr[node]; p < row_ptr[node + 1]; ++p) {
+      const i64 j = col_idx[p];
+#pragma unroll
+      for (int be = 0; be < BS; ++be) {
+        const i64 c = j * BS + be;
+        if (count[c] > 0) acc -= v64[(i64)p * BS * BS + al * BS + be] * g[c];
+      }
+    }
+    b[t] = acc;
+  }
+}
+
+template <int BS>
+__global__ void k_bc_eliminate(const int* __restrict__ row_ptr, const int* __restrict__ col_idx,
+                               const int* __restrict__ count, const double* __restrict__ dcount, i64 nn,
+                               double* __restrict__ v64, float* __restrict__ v32) {
+  const int lane = threadIdx.x & 31;
+  const i64 w0 = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+  const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+  for (i64 node = w0; node < nn; node += nw) {
+    const int rs = row_ptr[node], re = row_ptr[node + 1];
+    for (i64 q = (i64)rs * BS * BS + lane; q < (i64)re * BS * BS; q += 32) {
+      const i64 p = q / (BS * BS);
+      const int rem = (int)(q - p * BS * BS);
+      const i64 r = node * BS + rem / BS;
+      const i64 c = (i64)col_idx[p] * BS + rem % BS;
+      if (count[r] > 0 || count[c] > 0) {
+        const double v = (r == c && count[r] > 0) ? dcount[r] : 0.0;
+        v64[q] = v;
+        v32[q] = (float)v;
+      }
+    }
+  }
+}
+
+__global__ void k_bc_rhs(const int* __restrict__ count, const double* __restrict__ g, i64 n, double* __restrict__ b) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    if (count[i] > 0) b[i] = g[i];
+}
+
+__global__ void k_or_mask(const unsigned char* __restrict__ add, i64 n, unsigned char* __restrict__ m) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    if (add[i]) m[i] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint gradient: grad_e = -(3 theta_e^2 E0) lam_e^T K_e^1 u_e with
+// lam^T K^1 u = vol (l1 tr(Dl) tr(Du) + m1 (Dl:Du + Dl:Du^T)), D = nodal
+// gradient of the field (D[a][b] = sum_i f_{i a} g_i[b]); l1, m1 the Lame
+// constants at E = 1.
+// ---------------------------------------------------------------------------
+
+__global__ void k_adjoint_grad(const double* __restrict__ X, const int* __restrict__ cells,
+                               const unsigned char* __restrict__ valid, i64 nc, double l1, double m1, double E0,
+                               const double* __restrict__ theta, const double* __restrict__ u,
+                               const double* __restrict__ la, double* __restrict__ grad) {
+  for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
+    if (!valid[c]) { grad[c] = 0.0; continue; }
+    int v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = cells[4 * c + i];
+    Geo3 g = tet_geometry(X, v);
+    double gr[4][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      gr[1][r] = g.G[r][0];
+      gr[2][r] = g.G[r][1];
+      gr[3][r] = g.G[r][2];
+      gr[0][r] = -g.G[r][0] - g.G[r][1] - g.G[r][2];
+    }
+    double Du[3][3] = {{0}}, Dl[3][3] = {{0}};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double* ui = u + 3 * (i64)v[i];
+      const double* li = la + 3 * (i64)v[i];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          Du[a][b] += ui[a] * gr[i][b];
+          Dl[a][b] += li[a] * gr[i][b];
+        }
+    }
+    double trU = Du[0][0] + Du[1][1] + Du[2][2], trL = Dl[0][0] + Dl[1][1] + Dl[2][2];
+    double dd = 0.0, dt = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        dd += Dl[a][b] * Du[a][b];
+        dt += Dl[a][b] * Du[b][a];
+      }
+    const double vol = (1.0 / 6.0) * fabs(g.det);
+    const double s = vol * (l1 * trL * trU + m1 * (dd + dt));
+    const double th = theta[c];
+    grad[c] = -(3.0 * th * th * E0) * s;
+  }
+}
+
+bool g_p2_tables_ready[64] = {false};
+
+void ensure_p2_tables(fcu_ctx ctx) {
+  if (g_p2_tables_ready[ctx->device & 63]) return;
+  // Degree-2 Keast rule (quadrature.rs:157-183) and P2 gradients
+  // (lagrange.rs:324-346): R^{de}_{ab} = sum_q w_q d_d phi_a(xi_q) d_e phi_b(xi_q).
+  const double s5 = std::sqrt(5.0);
+  const double A = (5.0 - s5) / 20.0, B = (5.0 + 3.0 * s5) / 20.0, W = 1.0 / 24.0;
+  const double P[4][3] = {{A, A, A}, {B, A, A}, {A, B, A}, {A, A, B}};
+  double Rde[3][3][10][10] = {};
+  for (int q = 0; q < 4; ++q) {
+    double x = P[q][0], y = P[q][1], z = P[q][2];
+    double l0 = 1.0 - x - y - z, l1 = x, l2 = y, l3 = z;
+    double G[10][3] = {{-(4 * l0 - 1), -(4 * l0 - 1), -(4 * l0 - 1)},
+                       {4 * l1 - 1, 0, 0},
+                       {0, 4 * l2 - 1, 0},
+                       {0, 0, 4 * l3 - 1},
+                       {4 * (l0 - l1), -4 * l1, -4 * l1},
+                       {4 * l2, 4 * l1, 0},
+                       {-4 * l2, 4 * (l0 - l2), -4 * l2},
+                       {-4 * l3, -4 * l3, 4 * (l0 - l3)},
+                       {4 * l3, 0, 4 * l1},
+                       {0, 4 * l3, 4 * l2}};
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e)
+        for (int a = 0; a < 10; ++a)
+          for (int b = 0; b < 10; ++b) Rde[d][e][a][b] += W * G[a][d] * G[b][e];
+  }
+  double R[6][10][10];
+  const int D[6] = {0, 1, 2, 0, 0, 1}, E[6] = {0, 1, 2, 1, 2, 2};
+  for (int m = 0; m < 6; ++m)
+    for (int a = 0; a < 10; ++a)
+      for (int b = 0; b < 10; ++b)
+        R[m][a][b] = (m < 3) ? Rde[D[m]][E[m]][a][b] : Rde[D[m]][E[m]][a][b] + Rde[E[m]][D[m]][a][b];
+  CUDA_CHECK(cudaMemcpyToSymbol(c_p2_R, R, sizeof(R)));
+  g_p2_tables_ready[ctx->device & 63] = true;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host entry points (called from api.cu)
+// ---------------------------------------------------------------------------
+
+int assembly_blocks(fcu_ctx ctx, i64 rows, int warps = WARPS) {
+  i64 need = (rows + warps - 1) / warps;
+  i64 cap = (i64)ctx->num_sms * 8;
+  return (int)std::max<i64>(1, std::min(need, cap));
+}
+
+void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
+  fcu_space s = m->space;
+  fcu_ctx ctx = m->ctx;
+  fcu_mesh me = s->mesh;
+  const int nb = assembly_blocks(ctx, s->nnodes);
+  if (s->kind == FCU_SPACE_P2) {
+    ensure_p2_tables(ctx);
+    k_assemble_scalar<10, 3, true><<<nb, WARPS * 32, 0, ctx->stream>>>(
+        s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
+        coef_dev, s->nnodes, m->val64.p, m->val32.p);
+  } else if (me->dim == 3) {
+    k_assemble_scalar<4, 3, false><<<nb, WARPS * 32, 0, ctx->stream>>>(
+        s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
+        coef_dev, s->nnodes, m->val64.p, m->val32.p);
+  } else {
+    k_assemble_scalar<3, 2, false><<<nb, WARPS * 32, 0, ctx->stream>>>(
+        s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
+        coef_dev, s->nnodes, m->val64.p, m->val32.p);
+  }
+  LAUNCH_CHECK(ctx);
+}
+
+void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* cellE_dev) {
+  fcu_space s = m->space;
+  fcu_ctx ctx = m->ctx;
+  // ElasticMaterial::lame_lambda / lame_mu (elasticity.rs:33-47)
+  const double Eref = cellE_dev ? 1.0 : E;
+  const double lam = (Eref * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  const double mu = Eref / (2.0 * (1.0 + nu));
+  const int nb = assembly_blocks(ctx, s->nnodes, EWARPS);
+  k_assemble_elasticity<<<nb, EWARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                            s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p,
+                                                            s->mesh->coords.p, cellE_dev, lam, mu, s->nnodes,
+                                                            m->val64.p, m->val32.p);
+  LAUNCH_CHECK(ctx);
+}
+
+void apply_dirichlet_impl(fcu_matrix m, double* b_dev, i64 nbc, const i64* dofs_dev, const double* vals_dev) {
+  fcu_ctx ctx = m->ctx;
+  const i64 n = m->n, nn = m->nnodes;
+  const int cap = ctx->num_sms * 16;
+  DBuf<int> count, last, bad;
+  DBuf<double> g;
+  DBuf<unsigned char> dnow;
+  count.alloc(n); last.alloc(n); bad.alloc(1); g.alloc(n); dnow.alloc(n);
+  if (!m->dirichlet.p) {
+    m->dirichlet.alloc(n);
+    CUDA_CHECK(cudaMemsetAsync(m->dirichlet.p, 0, n, ctx->stream));
+    m->diag_count.alloc(n);
+  }
+  CUDA_CHECK(cudaMemsetAsync(count.p, 0, n * sizeof(int), ctx->stream));
+  CUDA_CHECK(cudaMemsetAsync(last.p, 0xff, n * sizeof(int), ctx->stream));
+  CUDA_CHECK(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+  CUDA_CHECK(cudaMemsetAsync(dnow.p, 0, n, ctx->stream));
+  if (nbc > 0) {
+    k_bc_mark<<<grid_for(nbc, 256, cap), 256, 0, ctx->stream>>>(dofs_dev, nbc, n, count.p, last.p, bad.p);
+    LAUNCH_CHECK(ctx);
+  }
+  int hbad = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  if (hbad) fail(FCU_ERR_BAD_ARG, "Dirichlet dof index out of range");
+  k_bc_flags<<<grid_for(n, 256, cap), 256, 0, ctx->stream>>>(count.p, last.p, vals_dev, n, dnow.p, g.p,
+                                                             m->diag_count.p);
+  LAUNCH_CHECK(ctx);
+  if (m->bs == 3) {
+    k_bc_lift<3><<<grid_for(n, 128, cap), 128, 0, ctx->stream>>>(m->row_ptr, m->col_idx, m->val64.p, count.p, g.p, nn, b_dev);
+    LAUNCH_CHECK(ctx);
+    k_bc_eliminate<3><<<grid_for(nn * 32, 256, cap), 256, 0, ctx->stream>>>(m->row_ptr, m->col_idx, count.p,
+                                                                             m->diag_count.p, nn, m->val64.p, m->val32.p);
+  } else {
+    k_bc_lift<1><<<grid_for(n, 128, cap), 128, 0, ctx->stream>>>(m->row_ptr, m->col_idx, m->val64.p, count.p, g.p, nn, b_dev);
+    LAUNCH_CHECK(ctx);
+    k_bc_eliminate<1><<<grid_for(nn * 32, 256, cap), 256, 0, ctx->stream>>>(m->row_ptr, m->col_idx, count.p,
+                                                                             m->diag_count.p, nn, m->val64.p, m->val32.p);
+  }
+  LAUNCH_CHECK(ctx);
+  k_bc_rhs<<<grid_for(n, 256, cap), 256, 0, ctx->stream>>>(count.p, g.p, n, b_dev);
+  LAUNCH_CHECK(ctx);
+  k_or_mask<<<grid_for(n, 256, cap), 256, 0, ctx->stream>>>(dnow.p, n, m->dirichlet.p);
+  LAUNCH_CHECK(ctx);
+  std::vector<unsigned char> hm(n);
+  CUDA_CHECK(cudaMemcpyAsync(hm.data(), m->dirichlet.p, n, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  i64 nd = 0;
+  for (unsigned char v : hm) nd += v;
+  m->n_dirichlet = nd;
+  m->bc_applied = true;
+}
+
+void adjoint_gradient_impl(fcu_space s, double E0, double nu, const double* theta, const double* u, const double* la,
+                           double* grad) {
+  fcu_ctx ctx = s->ctx;
+  fcu_mesh me = s->mesh;
+  const double l1 = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  const double m1 = 1.0 / (2.0 * (1.0 + nu));
+  k_adjoint_grad<<<grid_for(me->nc, 128, ctx->num_sms * 16), 128, 0, ctx->stream>>>(
+      me->coords.p, me->cells.p, me->valid.p, me->nc, l1, m1, E0, theta, u, la, grad);
+  LAUNCH_CHECK(ctx);
+}

@@ -1,0 +1,308 @@
+// Internal types of the fenics_cuda library: handles, device buffers, error
+// plumbing and small device helpers shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/fenics_cuda.h"
+
+typedef int64_t i64;
+
+// ---------------------------------------------------------------------------
+// Errors: every internal routine throws FcuError; the C ABI layer converts it
+// into a status code and the context's last-error string.
+// ---------------------------------------------------------------------------
+
+struct FcuError {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw FcuError{code, msg}; }
+
+#define CUDA_CHECK(expr)                                                                        \
+  do {                                                                                          \
+    cudaError_t e_ = (expr);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      fail(FCU_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_) + " at " __FILE__); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Device buffer (RAII, stream-ordered allocation on the context stream)
+// ---------------------------------------------------------------------------
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count) {
+      // 16 extra bytes so vector loads that round a range outward stay inside.
+      cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T) + 16);
+      if (e != cudaSuccess) { p = nullptr; fail(FCU_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
+    }
+    n = count;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------------------
+// Handles
+// ---------------------------------------------------------------------------
+
+struct Workspace;  // solver state, defined in solver.cu
+
+struct fcu_ctx_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  i64 launches = 0;          // kernels launched by this library on this context
+  DBuf<unsigned char> temp;  // reusable scratch (CUB temporary storage)
+  int num_sms = 148;
+  unsigned char* temp_bytes(size_t b) {
+    if (temp.n < b) temp.alloc(b);
+    return temp.p;
+  }
+};
+
+struct fcu_mesh_s {
+  fcu_ctx ctx = nullptr;
+  int dim = 0, nodes = 0;
+  i64 nv = 0, nc = 0;
+  DBuf<double> coords;    // nv*dim, AoS as the reference stores Vec<[f64;DIM]>
+  DBuf<int> cells;        // nc*nodes, int32
+  DBuf<unsigned char> valid;  // 1 if |det J| >= 1e-14
+  i64 n_degenerate = -1;
+};
+
+// Sparsity pattern at node level (node = dof for scalar spaces, vertex for
+// the vector space whose 3x3 blocks are stored contiguously) plus the
+// row-gather structures the assembly kernels read.
+struct fcu_space_s {
+  fcu_ctx ctx = nullptr;
+  fcu_mesh mesh = nullptr;
+  int kind = 0;
+  int k = 0;        // nodes per cell (3, 4, 10)
+  int bs = 1;       // dofs per node (1 or 3)
+  i64 nnodes = 0;   // rows of the node pattern
+  i64 ndofs = 0;
+  i64 nedges = 0;   // P2 only
+  i64 nnzb = 0;     // stored node-pattern entries (diagonals always present)
+  i64 nnz_ref = 0;  // entries of the raw reference pattern (scalar)
+  int max_row = 0;  // longest node row
+  int max_contrib = 0;
+  DBuf<int> cell_nodes;    // nc*k  (P1: the mesh cells; P2: vertex + edge dofs)
+  DBuf<int> edge_verts;    // P2: nedges*2
+  DBuf<int> row_ptr;       // nnodes+1
+  DBuf<int> col_idx;       // nnzb
+  DBuf<int> diag_pos;      // nnodes: position of (i,i)
+  DBuf<int> contrib_ptr;   // nnodes+1
+  DBuf<int> contrib;       // (cell << 4) | local, sorted by cell within a row
+  DBuf<unsigned short> slot_cnt;   // nnzb: contributions to each slot
+  DBuf<unsigned short> slot_ent;   // k*ncontrib: (t_local << 4) | b, per slot in cell order
+  DBuf<int> tpos;          // nnzb: position of the transposed entry (built on demand)
+};
+
+struct fcu_matrix_s {
+  fcu_ctx ctx = nullptr;
+  fcu_space space = nullptr;   // nullptr for a wrapped CSC/CSR
+  i64 n = 0;                   // scalar order
+  i64 nnodes = 0;              // block rows (== n when bs == 1)
+  int bs = 1;
+  i64 nnzb = 0;
+  // Pattern (owned copies for wrapped matrices, else the space's arrays).
+  const int* row_ptr = nullptr;
+  const int* col_idx = nullptr;
+  const int* diag_pos = nullptr;
+  DBuf<int> own_row_ptr, own_col_idx, own_diag_pos;
+  bool wrapped_general = false;  // wrapped CSC (export needs the stored layout)
+  DBuf<double> val64;   // nnzb*bs*bs
+  DBuf<float> val32;
+  DBuf<unsigned char> dirichlet;  // n: 1 if eliminated (empty when no BC applied)
+  i64 n_dirichlet = 0;
+  DBuf<double> diag_count;        // n: diagonal value for eliminated dofs
+  bool bc_applied = false;
+  bool has_values = false;
+  DBuf<unsigned char> diag_struct;  // node rows whose diagonal is in the raw pattern
+  DBuf<i64> csc_colptr, csc_rowidx; // wrapped CSC: the caller's layout, for export
+  DBuf<int> csr_of;                 // wrapped CSC: CSC position -> CSR slot
+  Workspace* ws = nullptr;
+  ~fcu_matrix_s();
+};
+
+// ---------------------------------------------------------------------------
+// Host <-> device helpers
+// ---------------------------------------------------------------------------
+
+inline bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Copy `count` elements from a host or device pointer into a device buffer.
+template <class T>
+inline void upload(fcu_ctx ctx, DBuf<T>& dst, const T* src, size_t count) {
+  dst.alloc(count);
+  if (count) CUDA_CHECK(cudaMemcpyAsync(dst.p, src, count * sizeof(T), cudaMemcpyDefault, ctx->stream));
+}
+
+template <class T>
+inline void download(fcu_ctx ctx, T* dst, const T* src_dev, size_t count) {
+  if (count) CUDA_CHECK(cudaMemcpyAsync(dst, src_dev, count * sizeof(T), cudaMemcpyDefault, ctx->stream));
+}
+
+// A read-only view of a caller array on the device: the caller's pointer when
+// it is device memory, else a staged copy.
+template <class T>
+struct DevIn {
+  const T* p = nullptr;
+  DBuf<T> staged;
+  DevIn(fcu_ctx ctx, const T* src, size_t count) {
+    if (!src || !count) { p = nullptr; return; }
+    if (is_device_ptr(src)) { p = src; return; }
+    upload(ctx, staged, src, count);
+    p = staged.p;
+  }
+};
+
+// A writable device view of a caller output: writes land directly in device
+// memory, or in a staging buffer copied back by finish().
+template <class T>
+struct DevOut {
+  T* p = nullptr;
+  T* host = nullptr;
+  size_t count = 0;
+  DBuf<T> staged;
+  DevOut(T* dst, size_t n, const T* init_from = nullptr, fcu_ctx ctx = nullptr) : count(n) {
+    if (!dst || !n) return;
+    if (is_device_ptr(dst)) { p = dst; }
+    else {
+      host = dst;
+      staged.alloc(n);
+      p = staged.p;
+    }
+    if (init_from && ctx && init_from != p)
+      CUDA_CHECK(cudaMemcpyAsync(p, init_from, n * sizeof(T), cudaMemcpyDefault, ctx->stream));
+  }
+  void finish(fcu_ctx ctx) {
+    if (host) download(ctx, host, p, count);
+  }
+  bool on_host() const { return host != nullptr; }
+};
+
+// Launch bookkeeping: count and check every kernel launch.
+#define LAUNCH_CHECK(ctx)                 \
+  do {                                    \
+    (ctx)->launches++;                    \
+    CUDA_CHECK(cudaGetLastError());       \
+  } while (0)
+
+inline unsigned grid_for(i64 work, int block, int cap_blocks) {
+  i64 g = (work + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap_blocks) g = cap_blocks;
+  return (unsigned)g;
+}
+
+// ---------------------------------------------------------------------------
+// Device geometry shared by assembly, RHS and adjoint kernels.
+// ---------------------------------------------------------------------------
+
+// AffineSimplexMap (jacobian.rs:18-41, 60-85): J columns v_i - v0, det by
+// cofactor expansion along the first row, J^{-T} from the adjugate.
+struct Geo3 {
+  double G[3][3];  // J^{-T}
+  double det;
+  bool ok;
+};
+
+__device__ __forceinline__ Geo3 tet_geometry(const double* __restrict__ X, const int* v) {
+  Geo3 g;
+  double a[3][3];
+  const double* p0 = X + 3 * (i64)v[0];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double* pc = X + 3 * (i64)v[c + 1];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) a[r][c] = pc[r] - p0[r];
+  }
+  double m1 = a[1][1] * a[2][2] - a[2][1] * a[1][2];
+  double m2 = a[1][0] * a[2][2] - a[2][0] * a[1][2];
+  double m3 = a[1][0] * a[2][1] - a[2][0] * a[1][1];
+  double d = a[0][0] * m1 - a[0][1] * m2 + a[0][2] * m3;
+  g.det = d;
+  g.ok = fabs(d) >= 1e-14;
+  double id = 1.0 / d;
+  // inverse (row-major) then transposed into G
+  double inv[3][3];
+  inv[0][0] = m1 * id;
+  inv[0][1] = (a[0][2] * a[2][1] - a[2][2] * a[0][1]) * id;
+  inv[0][2] = (a[0][1] * a[1][2] - a[1][1] * a[0][2]) * id;
+  inv[1][0] = -m2 * id;
+  inv[1][1] = (a[0][0] * a[2][2] - a[2][0] * a[0][2]) * id;
+  inv[1][2] = (a[1][0] * a[0][2] - a[0][0] * a[1][2]) * id;
+  inv[2][0] = m3 * id;
+  inv[2][1] = (a[2][0] * a[0][1] - a[0][0] * a[2][1]) * id;
+  inv[2][2] = (a[0][0] * a[1][1] - a[1][0] * a[0][1]) * id;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g.G[r][c] = inv[c][r];
+  return g;
+}
+
+struct Geo2 {
+  double G[2][2];
+  double det;
+  bool ok;
+};
+
+__device__ __forceinline__ Geo2 tri_geometry(const double* __restrict__ X, const int* v) {
+  Geo2 g;
+  const double* p0 = X + 2 * (i64)v[0];
+  const double* p1 = X + 2 * (i64)v[1];
+  const double* p2 = X + 2 * (i64)v[2];
+  double a00 = p1[0] - p0[0], a10 = p1[1] - p0[1];
+  double a01 = p2[0] - p0[0], a11 = p2[1] - p0[1];
+  double d = a00 * a11 - a10 * a01;
+  g.det = d;
+  g.ok = fabs(d) >= 1e-14;
+  double id = 1.0 / d;
+  // inv = [a11, -a01; -a10, a00] / d ; G = inv^T
+  g.G[0][0] = a11 * id;
+  g.G[0][1] = -a10 * id;
+  g.G[1][0] = -a01 * id;
+  g.G[1][1] = a00 * id;
+  return g;
+}
+
+// Kernels implemented in the .cu files and used across them.
+void build_mesh_validity(fcu_mesh m);
+void build_space_pattern(fcu_space s);
+void build_transpose_positions(fcu_space s);

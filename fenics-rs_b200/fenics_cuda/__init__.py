@@ -1,0 +1,726 @@
+"""fenics_cuda — B200 FEM assembly + Jacobi-PCG behind the fenics-rs interface.
+
+Python mirror of the reference's hot-path API over the C ABI of
+``libfenics_cuda.so`` (include/fenics_cuda.h). Function names, argument
+meaning and error behaviour follow GlassOnTin/fenics-rs:
+
+  crates/fenics-mesh       unit_square, box_beam, unit_cube  (generators.rs)
+  crates/fenics-assembly   assemble_stiffness_2d/3d, assemble_rhs_2d/3d,
+                           apply_dirichlet_bc, boundary_dofs_2d/3d,
+                           assemble_elasticity_stiffness_3d,
+                           assemble_elasticity_body_force_3d,
+                           apply_vector_dirichlet_bc, assemble_surface_traction_3d
+  crates/fenics-solver     solve_cg, solve_csr_cg_gpu, solve_cg_gpu_or_cpu,
+                           solve_poisson_2d/3d, solve_elasticity_3d
+
+All compute runs in CUDA kernels on the device; there is no CPU fallback (a
+missing library or device raises). Arrays may be numpy (host) or torch CUDA
+tensors (device); device arrays are used in place.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import (FCU_FP64, FCU_MIXED, FCU_SPACE_P1, FCU_SPACE_P1_VEC3, FCU_SPACE_P2, FCU_SRC_CONSTANT,
+                   FCU_SRC_NODAL, FCU_SRC_SIN_PRODUCT, SolveInfo)
+
+__all__ = [
+    "Context", "Mesh", "FunctionSpace", "Matrix", "CscMatrix", "FcuError", "CgError",
+    "unit_square", "box_beam", "unit_cube", "default_context",
+    "assemble_stiffness_2d", "assemble_stiffness_3d", "assemble_rhs_2d", "assemble_rhs_3d",
+    "apply_dirichlet_bc", "boundary_dofs_2d", "boundary_dofs_3d", "DirichletBC",
+    "ElasticMaterial", "VectorDirichletBC", "assemble_elasticity_stiffness_3d",
+    "assemble_elasticity_body_force_3d", "apply_vector_dirichlet_bc", "assemble_surface_traction_3d",
+    "extract_boundary_facets", "solve_cg", "solve_csr_cg_gpu", "solve_cg_gpu_or_cpu", "GpuSolveResult",
+    "solve_poisson_2d", "solve_poisson_3d", "solve_elasticity_3d", "spmv",
+    "FCU_FP64", "FCU_MIXED",
+]
+
+
+class FcuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[fcu error {code}] {msg}")
+        self.code = code
+
+
+class CgError(FcuError):
+    """Err(String) of solve_cg (cg.rs:102-107, 139-148)."""
+
+
+def _L():
+    return _abi.lib()
+
+
+# ---------------------------------------------------------------------------
+# pointers: numpy (host) or torch CUDA tensors (device)
+# ---------------------------------------------------------------------------
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a, dtype=None):
+    """(address, keepalive) of a contiguous array, converting numpy dtypes."""
+    if a is None:
+        return None, None
+    if _is_torch(a):
+        if not a.is_contiguous():
+            raise ValueError("torch tensors must be contiguous")
+        return a.data_ptr(), a
+    arr = np.ascontiguousarray(a, dtype=dtype) if dtype is not None else np.ascontiguousarray(a)
+    return arr.ctypes.data, arr
+
+
+def _check(ctx: "Context", rc: int):
+    if rc != _abi.FCU_OK:
+        msg = _L().fcu_last_error(ctx.h if ctx else None)
+        msg = msg.decode() if msg else ""
+        if rc in (_abi.FCU_ERR_NO_CONVERGENCE, _abi.FCU_ERR_BREAKDOWN):
+            raise CgError(rc, msg)
+        raise FcuError(rc, msg)
+
+
+# ---------------------------------------------------------------------------
+# context
+# ---------------------------------------------------------------------------
+
+class Context:
+    """A device, a stream and the library state on them (CudaSession, gpu.rs:325-430)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        rc = _L().fcu_ctx_create(device, C.byref(h))
+        if rc != _abi.FCU_OK:
+            raise FcuError(rc, (_L().fcu_last_error(None) or b"").decode())
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            _L().fcu_ctx_destroy(self.h)
+            self.h = None
+
+    def synchronize(self):
+        _check(self, _L().fcu_ctx_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return _L().fcu_ctx_stream(self.h) or 0
+
+    @property
+    def kernel_launches(self) -> int:
+        return _L().fcu_ctx_kernel_launches(self.h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+# ---------------------------------------------------------------------------
+# meshes (fenics-mesh)
+# ---------------------------------------------------------------------------
+
+class Mesh:
+    """SimplicialMesh<DIM, NODES> (mesh.rs:11-20): host vertices and cells, with
+    device copies created per context on first use."""
+
+    def __init__(self, coords, cells):
+        self.coords = np.ascontiguousarray(coords, dtype=np.float64)
+        self.cells = np.ascontiguousarray(cells, dtype=np.int64)
+        if self.coords.ndim != 2 or self.cells.ndim != 2 or self.cells.shape[1] != self.coords.shape[1] + 1:
+            raise ValueError("coords must be [nv, dim] and cells [nc, dim+1]")
+        self._dev = {}
+
+    @property
+    def dim(self) -> int:
+        return self.coords.shape[1]
+
+    def num_vertices(self) -> int:
+        return self.coords.shape[0]
+
+    def num_cells(self) -> int:
+        return self.cells.shape[0]
+
+    nv = property(num_vertices)
+    nc = property(num_cells)
+
+    def handle(self, ctx: Context):
+        key = id(ctx)
+        if key not in self._dev:
+            h = C.c_void_p()
+            _check(ctx, _L().fcu_mesh_create(ctx.h, self.dim, self.nv, self.coords.ctypes.data, self.nc,
+                                             self.cells.ctypes.data, C.byref(h)))
+            self._dev[key] = (ctx, h)
+        return self._dev[key][1]
+
+    def release(self):
+        for ctx, h in self._dev.values():
+            _L().fcu_mesh_destroy(h)
+        self._dev.clear()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def unit_square(nx: int, ny: int) -> Mesh:
+    """generators.rs:24-55: vertices row by row, each square split along v00-v11."""
+    if nx <= 0 or ny <= 0:
+        raise ValueError("nx and ny must be at least 1")
+    j, i = np.meshgrid(np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    coords = np.stack([i.ravel() / nx, j.ravel() / ny], axis=1)
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    v00 = (jj * (nx + 1) + ii).ravel()
+    v10, v01, v11 = v00 + 1, v00 + nx + 1, v00 + nx + 2
+    cells = np.empty((2 * nx * ny, 3), np.int64)
+    cells[0::2] = np.stack([v00, v10, v11], 1)
+    cells[1::2] = np.stack([v00, v11, v01], 1)
+    return Mesh(coords, cells)
+
+
+def box_beam(length, width, height, nx, ny, nz) -> Mesh:
+    """generators.rs:58-111: x fastest, Kuhn split of each hexahedron into 6 tets."""
+    if nx <= 0 or ny <= 0 or nz <= 0:
+        raise ValueError("nx, ny, and nz must be at least 1")
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    coords = np.stack([(i.ravel() / nx) * length, (j.ravel() / ny) * width, (k.ravel() / nz) * height], axis=1)
+    kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    sx, sy = 1, nx + 1
+    sz = (nx + 1) * (ny + 1)
+    p0 = (kk * sz + jj * sy + ii).ravel()
+    p1, p2, p3 = p0 + sx, p0 + sy, p0 + sx + sy
+    p4, p5, p6, p7 = p0 + sz, p0 + sz + sx, p0 + sz + sy, p0 + sz + sx + sy
+    tets = [(p0, p1, p3, p7), (p0, p3, p2, p7), (p0, p2, p6, p7), (p0, p6, p4, p7), (p0, p4, p5, p7), (p0, p5, p1, p7)]
+    cells = np.empty((6 * nx * ny * nz, 4), np.int64)
+    for t, tet in enumerate(tets):
+        cells[t::6] = np.stack(tet, 1)
+    return Mesh(coords, cells)
+
+
+def unit_cube(nx, ny, nz) -> Mesh:
+    return box_beam(1.0, 1.0, 1.0, nx, ny, nz)
+
+
+def extract_boundary_facets(mesh: Mesh, ctx: Context | None = None):
+    """extract_boundary_facets (mesh.rs:79-113, 145-210) on the device.
+    Returns (vertices [nf, dim], cell_idx [nf], local_facet_idx [nf]), sorted by
+    facet key; 3D facets are oriented outward."""
+    ctx = ctx or default_context()
+    h = mesh.handle(ctx)
+    n = C.c_int64(0)
+    _check(ctx, _L().fcu_boundary_facets(ctx.h, h, None, None, None, C.byref(n)))
+    v = np.empty((n.value, mesh.dim), np.int64)
+    c = np.empty(n.value, np.int64)
+    lo = np.empty(n.value, np.int64)
+    if n.value:
+        _check(ctx, _L().fcu_boundary_facets(ctx.h, h, v.ctypes.data, c.ctypes.data, lo.ctypes.data, C.byref(n)))
+    return v, c, lo
+
+
+# ---------------------------------------------------------------------------
+# spaces and matrices
+# ---------------------------------------------------------------------------
+
+class FunctionSpace:
+    """Dof map + sparsity pattern of P1 / P2 / vector-P1 on a mesh, on the device."""
+
+    def __init__(self, ctx: Context, mesh: Mesh, kind: int):
+        self.ctx, self.mesh, self.kind = ctx, mesh, kind
+        h = C.c_void_p()
+        _check(ctx, _L().fcu_space_create(ctx.h, mesh.handle(ctx), kind, C.byref(h)))
+        self.h = h
+        nd, nz, ne = C.c_int64(), C.c_int64(), C.c_int64()
+        _L().fcu_space_info(h, C.byref(nd), C.byref(nz), C.byref(ne))
+        self.ndofs, self.nnz, self.nedges = nd.value, nz.value, ne.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            _L().fcu_space_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def boundary_dofs(self) -> np.ndarray:
+        n = C.c_int64(0)
+        _check(self.ctx, _L().fcu_space_boundary_dofs(self.ctx.h, self.h, None, C.byref(n)))
+        out = np.empty(n.value, np.int64)
+        if n.value:
+            _check(self.ctx, _L().fcu_space_boundary_dofs(self.ctx.h, self.h, out.ctypes.data, C.byref(n)))
+        return out
+
+    def p2_dofmap(self):
+        cd = np.empty((self.mesh.nc, 10), np.int64)
+        ev = np.empty((self.nedges, 2), np.int64)
+        _check(self.ctx, _L().fcu_space_p2_dofmap(self.ctx.h, self.h, cd.ctypes.data, ev.ctypes.data))
+        return cd, ev
+
+    def quadrature_points(self) -> np.ndarray:
+        nq = 3 if self.mesh.dim == 2 else 4
+        out = np.empty((self.mesh.nc * nq, self.mesh.dim))
+        _check(self.ctx, _L().fcu_quadrature_points(self.ctx.h, self.h, out.ctypes.data))
+        return out
+
+    def rhs_values(self, fq, out=None):
+        out = np.empty(self.ndofs) if out is None else out
+        pf, kf = _ptr(fq, np.float64)
+        pb, kb = _ptr(out)
+        _check(self.ctx, _L().fcu_assemble_rhs_values(self.ctx.h, self.h, pf, pb))
+        return out
+
+    def rhs_source(self, kind, params=(), nodal=None, out=None):
+        out = np.empty(self.ndofs) if out is None else out
+        par = np.ascontiguousarray(list(params) + [0.0, 0.0], dtype=np.float64)
+        pn, kn = _ptr(nodal, np.float64)
+        pb, kb = _ptr(out)
+        _check(self.ctx, _L().fcu_assemble_rhs_source(self.ctx.h, self.h, kind, par.ctypes.data, pn, pb))
+        return out
+
+    def body_force(self, f_body, out=None):
+        out = np.empty(self.ndofs) if out is None else out
+        f = np.ascontiguousarray(f_body, dtype=np.float64)
+        pb, kb = _ptr(out)
+        _check(self.ctx, _L().fcu_assemble_body_force(self.ctx.h, self.h, f.ctypes.data, pb))
+        return out
+
+    def surface_traction(self, facets, tq, out=None):
+        out = np.empty(self.ndofs) if out is None else out
+        pf, kf = _ptr(facets, np.int64)
+        pt, kt = _ptr(tq, np.float64)
+        pb, kb = _ptr(out)
+        nf = len(facets)
+        _check(self.ctx, _L().fcu_assemble_surface_traction(self.ctx.h, self.h, nf, pf, pt, pb))
+        return out
+
+    def adjoint_gradient(self, E0, nu, theta, u, lam, out=None):
+        out = np.empty(self.mesh.nc) if out is None else out
+        pt, kt = _ptr(theta, np.float64)
+        pu, ku = _ptr(u, np.float64)
+        pl, kl = _ptr(lam, np.float64)
+        pg, kg = _ptr(out)
+        _check(self.ctx, _L().fcu_adjoint_gradient(self.ctx.h, self.h, E0, nu, pt, pu, pl, pg))
+        return out
+
+
+@dataclass
+class CscMatrix:
+    """faer SparseColMat<usize, f64> as exported: column pointers, row indices
+    sorted inside each column, explicit zeros kept."""
+    n: int
+    colptr: np.ndarray
+    rowidx: np.ndarray
+    vals: np.ndarray
+    _device: object = field(default=None, repr=False, compare=False)
+
+    def nrows(self) -> int:
+        return self.n
+
+    @property
+    def nnz(self) -> int:
+        return int(self.colptr[-1])
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csc_matrix((self.vals, self.rowidx, self.colptr), shape=(self.n, self.n))
+
+
+class Matrix:
+    """A matrix on the device: FP64 values and their FP32 copy on a space's
+    pattern, or a wrapped caller CSC."""
+
+    def __init__(self, ctx: Context, space: FunctionSpace | None = None, h=None):
+        self.ctx, self.space = ctx, space
+        if h is None:
+            h = C.c_void_p()
+            _check(ctx, _L().fcu_matrix_create(ctx.h, space.h, C.byref(h)))
+        self.h = h
+        n = C.c_int64()
+        _L().fcu_matrix_info(h, C.byref(n), None)
+        self.n = n.value
+
+    @classmethod
+    def from_csc(cls, ctx: Context, A: CscMatrix) -> "Matrix":
+        h = C.c_void_p()
+        cp, kc = _ptr(A.colptr, np.int64)
+        ri, kr = _ptr(A.rowidx, np.int64)
+        va, kv = _ptr(A.vals, np.float64)
+        _check(ctx, _L().fcu_matrix_from_csc(ctx.h, A.n, cp, ri, va, C.byref(h)))
+        return cls(ctx, None, h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _L().fcu_matrix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nnz(self) -> int:
+        z = C.c_int64()
+        _check(self.ctx, _L().fcu_matrix_info(self.h, None, C.byref(z)))
+        return z.value
+
+    def assemble_stiffness(self, coef=None):
+        pc, kc = _ptr(coef, np.float64)
+        _check(self.ctx, _L().fcu_assemble_stiffness(self.ctx.h, self.h, pc))
+        return self
+
+    def assemble_elasticity(self, E, nu, cell_E=None):
+        pc, kc = _ptr(cell_E, np.float64)
+        _check(self.ctx, _L().fcu_assemble_elasticity(self.ctx.h, self.h, float(E), float(nu), pc))
+        return self
+
+    def apply_dirichlet(self, b, dofs, vals):
+        """In place on the matrix and b (numpy array or CUDA tensor)."""
+        pb, kb = _ptr(b)
+        pd, kd = _ptr(dofs, np.int64)
+        pv, kv = _ptr(vals, np.float64)
+        _check(self.ctx, _L().fcu_apply_dirichlet(self.ctx.h, self.h, pb, len(dofs), pd, pv))
+        return b
+
+    def export_csc(self) -> CscMatrix:
+        nnz = self.nnz
+        cp = np.empty(self.n + 1, np.int64)
+        ri = np.empty(nnz, np.int64)
+        va = np.empty(nnz, np.float64)
+        _check(self.ctx, _L().fcu_matrix_export_csc(self.ctx.h, self.h, cp.ctypes.data, ri.ctypes.data,
+                                                    va.ctypes.data))
+        return CscMatrix(self.n, cp, ri, va)
+
+    def spmv(self, x, y=None):
+        y = np.empty(self.n) if y is None else y
+        px, kx = _ptr(x, np.float64)
+        py, ky = _ptr(y)
+        _check(self.ctx, _L().fcu_spmv(self.ctx.h, self.h, px, py))
+        return y
+
+    def time_spmv(self, precision=FCU_FP64, reps=20):
+        """(ms per launch, algorithmic bytes per launch) of the PCG SpMV kernel."""
+        ms, by = C.c_double(), C.c_double()
+        _check(self.ctx, _L().fcu_time_spmv(self.ctx.h, self.h, precision, reps, C.byref(ms), C.byref(by)))
+        return ms.value, by.value
+
+    def pcg(self, b, x=None, x0=None, tol=1e-8, max_iter=10000, precision=FCU_FP64, raise_on_error=True):
+        """Jacobi-PCG (cg.rs:40-149). Returns (x, SolveInfo)."""
+        x = np.empty(self.n) if x is None else x
+        pb, kb = _ptr(b, np.float64)
+        p0, k0 = _ptr(x0, np.float64)
+        px, kx = _ptr(x)
+        info = SolveInfo()
+        rc = _L().fcu_pcg(self.ctx.h, self.h, pb, p0, px, float(tol), int(max_iter), precision, C.byref(info))
+        if raise_on_error:
+            _check(self.ctx, rc)
+        return x, info
+
+
+# ---------------------------------------------------------------------------
+# fenics-assembly mirror
+# ---------------------------------------------------------------------------
+
+def _assembled(kind, mesh, ctx, fill) -> CscMatrix:
+    ctx = ctx or default_context()
+    V = FunctionSpace(ctx, mesh, kind)
+    M = Matrix(ctx, V)
+    fill(M)
+    A = M.export_csc()
+    M.close()
+    V.close()
+    return A
+
+
+def assemble_stiffness_2d(mesh: Mesh, ctx: Context | None = None, kappa=None) -> CscMatrix:
+    """assemble_stiffness_2d (poisson.rs:23-69)."""
+    if mesh.dim != 2:
+        raise ValueError("triangle mesh expected")
+    return _assembled(FCU_SPACE_P1, mesh, ctx, lambda M: M.assemble_stiffness(kappa))
+
+
+def assemble_stiffness_3d(mesh: Mesh, ctx: Context | None = None, kappa=None) -> CscMatrix:
+    """assemble_stiffness_3d (poisson.rs:124-165)."""
+    if mesh.dim != 3:
+        raise ValueError("tetrahedron mesh expected")
+    return _assembled(FCU_SPACE_P1, mesh, ctx, lambda M: M.assemble_stiffness(kappa))
+
+
+def _rhs(mesh: Mesh, f, ctx):
+    ctx = ctx or default_context()
+    V = FunctionSpace(ctx, mesh, FCU_SPACE_P1)
+    q = V.quadrature_points()
+    fq = np.asarray(f(*[q[:, d] for d in range(mesh.dim)]), dtype=np.float64)
+    fq = np.broadcast_to(fq, (len(q),)).copy()
+    return V.rhs_values(fq)
+
+
+def assemble_rhs_2d(mesh: Mesh, f, ctx: Context | None = None) -> np.ndarray:
+    """assemble_rhs_2d (poisson.rs:72-121); f is evaluated (vectorised) at the
+    rule's physical points, as the reference evaluates its closure there."""
+    return _rhs(mesh, f, ctx)
+
+
+def assemble_rhs_3d(mesh: Mesh, f, ctx: Context | None = None) -> np.ndarray:
+    """assemble_rhs_3d (poisson.rs:168-218)."""
+    return _rhs(mesh, f, ctx)
+
+
+@dataclass
+class DirichletBC:
+    """poisson.rs:15-20"""
+    dofs: np.ndarray
+    values: np.ndarray
+
+
+def _apply_bc(mat: CscMatrix, rhs, dofs, vals, ctx):
+    ctx = ctx or default_context()
+    M = Matrix.from_csc(ctx, mat)
+    b = np.array(rhs, dtype=np.float64, copy=True)
+    M.apply_dirichlet(b, np.asarray(dofs, np.int64), np.asarray(vals, np.float64))
+    A = M.export_csc()
+    M.close()
+    return A, b
+
+
+def apply_dirichlet_bc(mat: CscMatrix, rhs, bc: DirichletBC, ctx: Context | None = None):
+    """apply_dirichlet_bc (poisson.rs:222-263) -> (matrix, rhs)."""
+    return _apply_bc(mat, rhs, bc.dofs, bc.values, ctx)
+
+
+def boundary_dofs_2d(mesh: Mesh, ctx: Context | None = None) -> np.ndarray:
+    """boundary_dofs_2d (poisson.rs:266-275): sorted, unique."""
+    return _boundary_dofs(mesh, ctx)
+
+
+def boundary_dofs_3d(mesh: Mesh, ctx: Context | None = None) -> np.ndarray:
+    """boundary_dofs_3d (poisson.rs:278-287)."""
+    return _boundary_dofs(mesh, ctx)
+
+
+def _boundary_dofs(mesh: Mesh, ctx):
+    ctx = ctx or default_context()
+    h = mesh.handle(ctx)
+    n = C.c_int64(0)
+    _check(ctx, _L().fcu_boundary_dofs(ctx.h, h, None, C.byref(n)))
+    out = np.empty(n.value, np.int64)
+    if n.value:
+        _check(ctx, _L().fcu_boundary_dofs(ctx.h, h, out.ctypes.data, C.byref(n)))
+    return out
+
+
+@dataclass
+class ElasticMaterial:
+    """elasticity.rs:14-48"""
+    youngs_modulus: float
+    poissons_ratio: float
+
+    def __post_init__(self):
+        if not (-1.0 < self.poissons_ratio < 0.5):
+            raise ValueError("Poisson's ratio must be in (-1.0, 0.5) for physical stability")
+
+    def lame_lambda(self) -> float:
+        e, nu = self.youngs_modulus, self.poissons_ratio
+        return (e * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu))
+
+    def lame_mu(self) -> float:
+        return self.youngs_modulus / (2.0 * (1.0 + self.poissons_ratio))
+
+
+@dataclass
+class VectorDirichletBC:
+    """elasticity.rs:65-69: list of (dof, value)."""
+    prescribed_dofs: list
+
+    def arrays(self):
+        if len(self.prescribed_dofs) == 0:
+            return np.empty(0, np.int64), np.empty(0)
+        d, v = zip(*self.prescribed_dofs)
+        return np.asarray(d, np.int64), np.asarray(v, np.float64)
+
+
+def assemble_elasticity_stiffness_3d(mesh: Mesh, material: ElasticMaterial, ctx: Context | None = None,
+                                     cell_E=None) -> CscMatrix:
+    """assemble_elasticity_stiffness_3d (elasticity.rs:73-149)."""
+    return _assembled(FCU_SPACE_P1_VEC3, mesh, ctx,
+                      lambda M: M.assemble_elasticity(material.youngs_modulus, material.poissons_ratio, cell_E))
+
+
+def assemble_elasticity_body_force_3d(mesh: Mesh, f_body, ctx: Context | None = None) -> np.ndarray:
+    """assemble_elasticity_body_force_3d (elasticity.rs:153-185)."""
+    ctx = ctx or default_context()
+    return FunctionSpace(ctx, mesh, FCU_SPACE_P1_VEC3).body_force(f_body)
+
+
+def apply_vector_dirichlet_bc(mat: CscMatrix, rhs, bc: VectorDirichletBC, ctx: Context | None = None):
+    """apply_vector_dirichlet_bc (elasticity.rs:188-227) -> (matrix, rhs)."""
+    d, v = bc.arrays()
+    return _apply_bc(mat, rhs, d, v, ctx)
+
+
+def assemble_surface_traction_3d(mesh: Mesh, facets, traction_fn, ctx: Context | None = None) -> np.ndarray:
+    """assemble_surface_traction_3d (boundary.rs:48-108). `facets` is an [nf, 3]
+    vertex array (e.g. from extract_boundary_facets); traction_fn(x, y, z) is
+    evaluated (vectorised) at each facet's three edge midpoints."""
+    ctx = ctx or default_context()
+    fa = np.ascontiguousarray(facets, dtype=np.int64).reshape(-1, 3)
+    X = mesh.coords
+    p0, p1, p2 = X[fa[:, 0]], X[fa[:, 1]], X[fa[:, 2]]
+    mids = np.stack([0.5 * (p0 + p1), 0.5 * (p1 + p2), 0.5 * (p2 + p0)], axis=1).reshape(-1, 3)
+    t = traction_fn(mids[:, 0], mids[:, 1], mids[:, 2])
+    tq = np.stack(np.broadcast_arrays(*t), axis=1).astype(np.float64)
+    return FunctionSpace(ctx, mesh, FCU_SPACE_P1_VEC3).surface_traction(fa, tq)
+
+
+# ---------------------------------------------------------------------------
+# fenics-solver mirror
+# ---------------------------------------------------------------------------
+
+def solve_cg(mat, b, x0=None, tol=1e-10, max_iter=1000, ctx: Context | None = None, precision=FCU_FP64):
+    """solve_cg (cg.rs:40-149) -> (x, iterations, absolute residual); raises
+    CgError on breakdown or non-convergence like the reference's Err."""
+    ctx = ctx or default_context()
+    M = mat if isinstance(mat, Matrix) else Matrix.from_csc(ctx, mat)
+    try:
+        x, info = M.pcg(b, x0=x0, tol=tol, max_iter=max_iter, precision=precision)
+    finally:
+        if M is not mat:
+            M.close()
+    return x, info.iterations, info.residual
+
+
+def spmv(mat: CscMatrix, x, ctx: Context | None = None) -> np.ndarray:
+    """spmv (cg.rs:7-23)."""
+    ctx = ctx or default_context()
+    M = Matrix.from_csc(ctx, mat)
+    y = M.spmv(x)
+    M.close()
+    return y
+
+
+@dataclass
+class GpuSolveResult:
+    """gpu.rs:24-34"""
+    solution: np.ndarray
+    iterations: int
+    final_residual: float
+    wall_ms: float
+    kernel_ms: float
+    gflops: float
+    effective_bw_gbps: float
+    devices_used: list
+
+
+def solve_csr_cg_gpu(row_ptr, col_idx, vals, inv_diag, b, x0=None, rtol=1e-8, max_iter=1000,
+                     device_index: int | None = None) -> GpuSolveResult:
+    """solve_csr_cg_gpu (gpu.rs:1145-1442): u32 CSR, caller inverse diagonal,
+    relative residual, Ok even when the iteration limit is hit."""
+    import time
+    t0 = time.perf_counter()
+    ctx = default_context() if device_index in (None, 0) else Context(device_index)
+    n = len(b)
+    rp, k1 = _ptr(row_ptr, np.uint32)
+    ci, k2 = _ptr(col_idx, np.uint32)
+    va, k3 = _ptr(vals, np.float64)
+    idg, k4 = _ptr(inv_diag, np.float64)
+    bb, k5 = _ptr(b, np.float64)
+    xx0, k6 = _ptr(x0, np.float64)
+    x = np.empty(n)
+    info = SolveInfo()
+    _check(ctx, _L().fcu_solve_csr_cg(ctx.h, n, rp, ci, va, idg, bb, xx0, float(rtol), int(max_iter),
+                                      x.ctypes.data, C.byref(info)))
+    nnz = len(col_idx)
+    secs = max(info.kernel_ms / 1e3, 1e-9)
+    flops = (2.0 * nnz + 12.0 * n) * info.iterations
+    return GpuSolveResult(x, info.iterations, info.rel_residual, (time.perf_counter() - t0) * 1e3,
+                          info.kernel_ms, flops / secs / 1e9, info.effective_bw_gbps, [f"cuda:{ctx.device}"])
+
+
+def solve_cg_gpu_or_cpu(mat: CscMatrix, b, x0=None, tol=1e-10, max_iter=1000) -> GpuSolveResult:
+    """solve_cg_gpu_or_cpu (gpu.rs:1542-1602) without the CPU branch: the solve
+    runs on the device or raises."""
+    import time
+    t0 = time.perf_counter()
+    ctx = default_context()
+    M = Matrix.from_csc(ctx, mat)
+    x, info = M.pcg(b, x0=x0, tol=tol, max_iter=max_iter)
+    M.close()
+    return GpuSolveResult(x, info.iterations, info.rel_residual, (time.perf_counter() - t0) * 1e3,
+                          info.kernel_ms, 0.0, info.effective_bw_gbps, [f"cuda:{ctx.device}"])
+
+
+@dataclass
+class PoissonSolution:
+    """poisson_solver.rs:16-23"""
+    u: np.ndarray
+    iterations: int
+    residual: float
+
+
+def _solve_poisson(mesh: Mesh, source, boundary_value, tol, max_iter, ctx, precision):
+    ctx = ctx or default_context()
+    V = FunctionSpace(ctx, mesh, FCU_SPACE_P1)
+    M = Matrix(ctx, V).assemble_stiffness()
+    q = V.quadrature_points()
+    fq = np.broadcast_to(np.asarray(source(*[q[:, d] for d in range(mesh.dim)]), np.float64), (len(q),)).copy()
+    b = V.rhs_values(fq)
+    bd = V.boundary_dofs()
+    bv = np.broadcast_to(np.asarray(boundary_value(*[mesh.coords[bd, d] for d in range(mesh.dim)]),
+                                    np.float64), (len(bd),)).copy()
+    M.apply_dirichlet(b, bd, bv)
+    x, info = M.pcg(b, tol=tol, max_iter=max_iter, precision=precision)
+    return PoissonSolution(x, info.iterations, info.residual)
+
+
+def solve_poisson_2d(mesh: Mesh, source, boundary_value, tol, max_iter, ctx=None, precision=FCU_FP64):
+    """solve_poisson_2d (poisson_solver.rs:26-59), device-resident end to end."""
+    return _solve_poisson(mesh, source, boundary_value, tol, max_iter, ctx, precision)
+
+
+def solve_poisson_3d(mesh: Mesh, source, boundary_value, tol, max_iter, ctx=None, precision=FCU_FP64):
+    """solve_poisson_3d (poisson_solver.rs:99-132)."""
+    return _solve_poisson(mesh, source, boundary_value, tol, max_iter, ctx, precision)
+
+
+@dataclass
+class ElasticitySolution:
+    """elasticity_solver.rs:13-29 (displacements, iterations, residual)."""
+    displacements: np.ndarray
+    deformed_vertices: np.ndarray
+    iterations: int
+    residual: float
+
+
+def solve_elasticity_3d(mesh: Mesh, material: ElasticMaterial, body_force, bc: VectorDirichletBC, tol, max_iter,
+                        ctx=None, precision=FCU_FP64) -> ElasticitySolution:
+    """solve_elasticity_3d (elasticity_solver.rs:31-72), assembly to solve on the device."""
+    ctx = ctx or default_context()
+    V = FunctionSpace(ctx, mesh, FCU_SPACE_P1_VEC3)
+    M = Matrix(ctx, V).assemble_elasticity(material.youngs_modulus, material.poissons_ratio)
+    f = V.body_force(body_force)
+    d, v = bc.arrays()
+    M.apply_dirichlet(f, d, v)
+    x, info = M.pcg(f, tol=tol, max_iter=max_iter, precision=precision)
+    return ElasticitySolution(x, mesh.coords + x.reshape(-1, 3), info.iterations, info.residual)

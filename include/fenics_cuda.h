@@ -1,0 +1,201 @@
+/*
+ * fenics_cuda.h — C ABI of the B200 (sm_100a) FEM assembly + Jacobi-PCG library.
+ *
+ * This is the drop-in boundary for the hot path of GlassOnTin/fenics-rs:
+ * the crates/fenics-assembly `assemble_*` / `apply_*dirichlet_bc` /
+ * `boundary_dofs_*` functions and the crates/fenics-solver `solve_cg` /
+ * `solve_csr_cg_gpu` entry points. Each declaration below names the
+ * reference function it replaces (file:line inside the reference project).
+ *
+ * Conventions
+ *  - Every call returns an int status (FCU_OK = 0); fcu_last_error(ctx)
+ *    gives the message of the last failure on that context.
+ *  - Array arguments may be host or device pointers (CUDA unified
+ *    addressing tells them apart). Host outputs are complete when the call
+ *    returns; calls whose inputs and outputs are all device memory are
+ *    asynchronous on the context's stream.
+ *  - Index arrays exchanged with the caller are int64 (Rust `usize`),
+ *    except the u32 CSR of fcu_solve_csr_cg, which mirrors gpu.rs.
+ *  - Matrices are exported in faer SparseColMat layout: column pointers,
+ *    row indices sorted inside each column, explicit zeros kept.
+ *  - Handles own their device memory. One context per host thread, or
+ *    external synchronisation.
+ */
+#ifndef FENICS_CUDA_H
+#define FENICS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define FCU_OK 0
+#define FCU_ERR_CUDA 1           /* a CUDA runtime call failed                   */
+#define FCU_ERR_BAD_ARG 2        /* invalid sizes, indices or handles            */
+#define FCU_ERR_NO_CONVERGENCE 3 /* cg.rs:139-148 "CG failed to converge"       */
+#define FCU_ERR_BREAKDOWN 4      /* cg.rs:102-107 "Breakdown in CG"             */
+#define FCU_ERR_UNSUPPORTED 5    /* mesh outside the limits of a kernel          */
+
+/* ---- space kinds ---------------------------------------------------------- */
+#define FCU_SPACE_P1 1      /* scalar P1 on triangles (dim 2) or tetrahedra (dim 3) */
+#define FCU_SPACE_P2 2      /* scalar P2 on tetrahedra: vertex dofs, then edges     */
+#define FCU_SPACE_P1_VEC3 3 /* vector P1 on tetrahedra, dof = 3*vertex + component  */
+
+/* ---- solver precision ----------------------------------------------------- */
+#define FCU_FP64 0  /* FP64 Jacobi-PCG (cg.rs:40-149 arithmetic)                 */
+#define FCU_MIXED 1 /* FP32 SpMV/axpy, FP64 dots, FP64 residual + refinement      */
+
+/* ---- analytic sources for fcu_assemble_rhs_source ------------------------- */
+#define FCU_SRC_CONSTANT 0    /* f = p[0]                                       */
+#define FCU_SRC_SIN_PRODUCT 1 /* f = p[0] * prod_d sin(p[1] * x_d)              */
+#define FCU_SRC_NODAL 2       /* f = sum_j f_j phi_j, nodal values in `values`  */
+
+typedef struct fcu_ctx_s* fcu_ctx;
+typedef struct fcu_mesh_s* fcu_mesh;
+typedef struct fcu_space_s* fcu_space;
+typedef struct fcu_matrix_s* fcu_matrix;
+
+/* Per-solve report; the fields of GpuSolveResult (gpu.rs:24-34) that are
+ * numbers, plus status and the absolute residual solve_cg returns. */
+typedef struct {
+  int64_t iterations;     /* inner PCG iterations                               */
+  int64_t outer_updates;  /* FP64 residual replacements (FCU_MIXED)             */
+  double residual;        /* absolute ||b - A x||_2 (cg.rs:121)                 */
+  double rel_residual;    /* residual / ||b||_2 (gpu.rs:1360-1363)              */
+  double kernel_ms;       /* device time of the solve (CUDA events)             */
+  double effective_bw_gbps; /* algorithmic bytes / kernel_ms                    */
+  int status;             /* FCU_OK, FCU_ERR_NO_CONVERGENCE or FCU_ERR_BREAKDOWN */
+} fcu_solve_info;
+
+/* ---- context (replaces CudaSession, gpu.rs:325-430) ----------------------- */
+int fcu_ctx_create(int device, fcu_ctx* out);
+void fcu_ctx_destroy(fcu_ctx ctx);
+const char* fcu_last_error(fcu_ctx ctx);
+int fcu_ctx_synchronize(fcu_ctx ctx);
+void* fcu_ctx_stream(fcu_ctx ctx); /* the cudaStream_t all calls run on */
+/* Number of library kernels launched on this context since creation. */
+int64_t fcu_ctx_kernel_launches(fcu_ctx ctx);
+
+/* ---- meshes (SimplicialMesh<DIM,NODES>, mesh.rs:11-20) -------------------- */
+/* coords: nv*dim doubles (Vec<[f64;DIM]>); cells: nc*(dim+1) int64 (Vec<[usize;NODES]>). */
+int fcu_mesh_create(fcu_ctx ctx, int dim, int64_t nv, const double* coords, int64_t nc,
+                    const int64_t* cells, fcu_mesh* out);
+void fcu_mesh_destroy(fcu_mesh mesh);
+/* Cells with |det J| < 1e-14 (skipped by every assembler, poisson.rs:42-45). */
+int fcu_mesh_num_degenerate(fcu_ctx ctx, fcu_mesh mesh, int64_t* count);
+
+/* boundary_dofs_2d / boundary_dofs_3d (poisson.rs:266-287): sorted, unique
+ * vertices of facets that belong to exactly one cell. out==NULL queries count. */
+int fcu_boundary_dofs(fcu_ctx ctx, fcu_mesh mesh, int64_t* out, int64_t* count);
+
+/* extract_boundary_facets (mesh.rs:79-113, 145-210). Facets are returned
+ * sorted by their sorted vertex triple (the reference's HashMap order is
+ * unspecified); 3D facets are oriented outward as in mesh.rs:166-192.
+ * verts: nf*dim; cell, local: nf each (may be NULL). out==NULL queries count. */
+int fcu_boundary_facets(fcu_ctx ctx, fcu_mesh mesh, int64_t* verts, int64_t* cell, int64_t* local,
+                        int64_t* count);
+
+/* ---- function spaces: dof map + sparsity pattern ----------------------- */
+int fcu_space_create(fcu_ctx ctx, fcu_mesh mesh, int kind, fcu_space* out);
+void fcu_space_destroy(fcu_space space);
+/* ndofs, stored entries of the raw (pre-Dirichlet) matrix in reference pattern
+ * terms, and P2 edge count (0 otherwise). Any pointer may be NULL. */
+int fcu_space_info(fcu_space space, int64_t* ndofs, int64_t* nnz, int64_t* nedges);
+/* P2: cell dof map (nc*10, P2Tetrahedron local order, lagrange.rs:286-299) and
+ * edge vertex pairs (nedges*2); either may be NULL. */
+int fcu_space_p2_dofmap(fcu_ctx ctx, fcu_space space, int64_t* cell_dofs, int64_t* edge_verts);
+/* Boundary dofs of the space: P1 = boundary_dofs_*; P2 = boundary vertices and
+ * boundary edges, sorted. out==NULL queries count. */
+int fcu_space_boundary_dofs(fcu_ctx ctx, fcu_space space, int64_t* out, int64_t* count);
+
+/* ---- matrices -------------------------------------------------------------- */
+/* Allocate a matrix on the space's pattern (values unset). */
+int fcu_matrix_create(fcu_ctx ctx, fcu_space space, fcu_matrix* out);
+/* Wrap a caller CSC (faer SparseColMat<usize,f64>) for fcu_pcg (cg.rs:40). */
+int fcu_matrix_from_csc(fcu_ctx ctx, int64_t n, const int64_t* colptr, const int64_t* rowidx,
+                        const double* vals, fcu_matrix* out);
+void fcu_matrix_destroy(fcu_matrix m);
+/* Order and stored entries (reference pattern: after Dirichlet if applied). */
+int fcu_matrix_info(fcu_matrix m, int64_t* n, int64_t* nnz);
+/* Export as faer CSC (colptr n+1, rowidx nnz, vals nnz); any may be NULL. */
+int fcu_matrix_export_csc(fcu_ctx ctx, fcu_matrix m, int64_t* colptr, int64_t* rowidx, double* vals);
+
+/* assemble_stiffness_2d / assemble_stiffness_3d (poisson.rs:23-69, 124-165)
+ * for FCU_SPACE_P1; P2 stiffness for FCU_SPACE_P2 (no reference counterpart).
+ * cell_coef (nc, may be NULL) multiplies each cell's contribution (kappa_e).
+ * Writes the FP64 values and their FP32 copy. */
+int fcu_assemble_stiffness(fcu_ctx ctx, fcu_matrix m, const double* cell_coef);
+/* assemble_elasticity_stiffness_3d (elasticity.rs:73-149) for FCU_SPACE_P1_VEC3.
+ * cell_E (nc, may be NULL) overrides Young's modulus per cell. ElasticMaterial::new
+ * rejects nu outside (-1, 0.5) (elasticity.rs:23-26): FCU_ERR_BAD_ARG here. */
+int fcu_assemble_elasticity(fcu_ctx ctx, fcu_matrix m, double E, double nu, const double* cell_E);
+
+/* apply_dirichlet_bc / apply_vector_dirichlet_bc (poisson.rs:222-263,
+ * elasticity.rs:188-227), in place on m and b: b_i -= a_ik g_k for free rows,
+ * Dirichlet rows/columns eliminated, unit diagonal (repeated dofs add up),
+ * b_k = g_k (last occurrence wins). */
+int fcu_apply_dirichlet(fcu_ctx ctx, fcu_matrix m, double* b, int64_t nbc, const int64_t* dofs,
+                        const double* vals);
+
+/* ---- right-hand sides ------------------------------------------------------ */
+/* Physical quadrature points of assemble_rhs_2d/3d (poisson.rs:77,173):
+ * nc*3 points (2D) or nc*4 points (3D), dim doubles each; for P2 the same
+ * 4-point rule. Lets a host closure f be evaluated where the reference does. */
+int fcu_quadrature_points(fcu_ctx ctx, fcu_space space, double* out);
+/* assemble_rhs_2d / assemble_rhs_3d (poisson.rs:72-121, 168-218) with f given
+ * at the quadrature points above (fq: nc*nq). P2: same rule, P2 basis. */
+int fcu_assemble_rhs_values(fcu_ctx ctx, fcu_space space, const double* fq, double* b);
+/* Same integral with f evaluated on the device (FCU_SRC_*). */
+int fcu_assemble_rhs_source(fcu_ctx ctx, fcu_space space, int source, const double* params,
+                            const double* values, double* b);
+/* assemble_elasticity_body_force_3d (elasticity.rs:153-185). */
+int fcu_assemble_body_force(fcu_ctx ctx, fcu_space space, const double* f_body3, double* b);
+/* assemble_surface_traction_3d (boundary.rs:48-108): facets nf*3 vertex ids,
+ * tq = traction at each facet's three edge midpoints (nf*3*3). b is overwritten. */
+int fcu_assemble_surface_traction(fcu_ctx ctx, fcu_space space, int64_t nf, const int64_t* facets,
+                                  const double* tq, double* b);
+
+/* ---- solvers ---------------------------------------------------------------- */
+/* solve_cg (cg.rs:40-149): Jacobi-PCG on m, x0 may be NULL (zero start), stop
+ * when ||r||/||b|| < tol after the x/r update. FCU_FP64 follows the reference
+ * arithmetic; FCU_MIXED runs FP32 SpMV/axpy with FP64 dot accumulation and
+ * FP64 residual replacement, and stops on the FP64 residual ||b - A64 x||.
+ * Returns FCU_ERR_NO_CONVERGENCE / FCU_ERR_BREAKDOWN like the reference's Err;
+ * x and info are filled in every case. */
+int fcu_pcg(fcu_ctx ctx, fcu_matrix m, const double* b, const double* x0, double* x, double tol,
+            int64_t max_iter, int precision, fcu_solve_info* info);
+
+/* solve_csr_cg_gpu (gpu.rs:1145-1442): u32 CSR, caller-supplied inverse
+ * diagonal, relative tolerance. Like the reference it returns FCU_OK when the
+ * iteration limit is reached (info.rel_residual tells), and FCU_OK with x = 0
+ * when ||b|| = 0 (gpu.rs:1169-1180). */
+int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
+                     const double* vals, const double* inv_diag, const double* b, const double* x0,
+                     double rtol, int64_t max_iter, double* x, fcu_solve_info* info);
+
+/* y = A x (cg.rs:7-23) with the FP64 values. */
+int fcu_spmv(fcu_ctx ctx, fcu_matrix m, const double* x, double* y);
+
+/* ---- adjoint sensitivities (no reference counterpart) ----------------------- */
+/* For E_e = E0 * theta_e^3: grad_e = -lambda_e^T (3 theta_e^2 E0 K_e^1) u_e, with
+ * the unit-modulus element matrix K_e^1 recomputed per cell (not stored).
+ * space: FCU_SPACE_P1_VEC3; u, lambda: 3*nv; theta, grad: nc. */
+int fcu_adjoint_gradient(fcu_ctx ctx, fcu_space space, double E0, double nu, const double* theta,
+                         const double* u, const double* lambda, double* grad);
+
+/* ---- diagnostics (no reference counterpart) -------------------------------- */
+/* Average device time of one launch of the SpMV kernel the PCG of `precision`
+ * runs on m (Ap = A p with the device p.Ap reduction), over `reps`
+ * back-to-back launches timed with CUDA events on the context stream; and
+ * the algorithmic bytes of one launch (values + column indices + row
+ * pointers + one read of p + one write of Ap). */
+int fcu_time_spmv(fcu_ctx ctx, fcu_matrix m, int precision, int reps, double* ms_per_launch,
+                  double* bytes_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FENICS_CUDA_H */
