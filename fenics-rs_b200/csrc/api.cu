@@ -253,8 +253,55 @@ T read1(fcu_ctx ctx, const T* p) {
 
 int cap_blocks(fcu_ctx ctx) { return ctx->num_sms * 16; }
 
+// Assembly overwrites every value, so a re-assembled matrix starts without
+// Dirichlet conditions (the mask is cleared, its storage kept).
+void reset_dirichlet(fcu_matrix m) {
+  if (m->bc_applied && m->dirichlet.p)
+    CUDA_CHECK(cudaMemsetAsync(m->dirichlet.p, 0, m->n, m->ctx->stream));
+  m->bc_applied = false;
+  m->n_dirichlet = 0;
+}
+
 void check_ctx(fcu_ctx ctx) {
   if (!ctx) fail(FCU_ERR_BAD_ARG, "null context");
+}
+
+void ctx_release(fcu_ctx c) {
+  if (!c || --c->refs > 0) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->temp.release();
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+void mesh_release(fcu_mesh m) {
+  if (!m || --m->refs > 0) return;
+  fcu_ctx c = m->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete m;
+  ctx_release(c);
+}
+
+void space_release(fcu_space s) {
+  if (!s || --s->refs > 0) return;
+  fcu_mesh me = s->mesh;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  delete s;
+  mesh_release(me);
+}
+
+void matrix_release(fcu_matrix m) {
+  if (!m || --m->refs > 0) return;
+  fcu_space sp = m->space;
+  fcu_ctx c = m->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete m;
+  if (sp) space_release(sp);
+  ctx_release(c);
 }
 
 }  // namespace
@@ -287,14 +334,7 @@ int fcu_ctx_create(int device, fcu_ctx* out) {
   });
 }
 
-void fcu_ctx_destroy(fcu_ctx ctx) {
-  if (!ctx) return;
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  ctx->temp.release();
-  cudaStreamDestroy(ctx->stream);
-  delete ctx;
-}
+void fcu_ctx_destroy(fcu_ctx ctx) { ctx_release(ctx); }
 
 const char* fcu_last_error(fcu_ctx ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
 
@@ -338,16 +378,12 @@ int fcu_mesh_create(fcu_ctx ctx, int dim, int64_t nv, const double* coords, int6
       if (read1(ctx, bad.p)) fail(FCU_ERR_BAD_ARG, "cell vertex index out of range");
     }
     build_mesh_validity(m.get());
+    ctx->refs++;
     *out = m.release();
   });
 }
 
-void fcu_mesh_destroy(fcu_mesh m) {
-  if (!m) return;
-  cudaSetDevice(m->ctx->device);
-  cudaStreamSynchronize(m->ctx->stream);
-  delete m;
-}
+void fcu_mesh_destroy(fcu_mesh m) { mesh_release(m); }
 
 int fcu_mesh_num_degenerate(fcu_ctx ctx, fcu_mesh mesh, int64_t* count) {
   return guarded(ctx, [&] {
@@ -404,16 +440,12 @@ int fcu_space_create(fcu_ctx ctx, fcu_mesh mesh, int kind, fcu_space* out) {
     s->kind = kind;
     build_space_pattern(s.get());
     sync(ctx);
+    mesh->refs++;
     *out = s.release();
   });
 }
 
-void fcu_space_destroy(fcu_space s) {
-  if (!s) return;
-  cudaSetDevice(s->ctx->device);
-  cudaStreamSynchronize(s->ctx->stream);
-  delete s;
-}
+void fcu_space_destroy(fcu_space s) { space_release(s); }
 
 int fcu_space_info(fcu_space s, int64_t* ndofs, int64_t* nnz, int64_t* nedges) {
   if (!s) return FCU_ERR_BAD_ARG;
@@ -489,6 +521,8 @@ int fcu_matrix_create(fcu_ctx ctx, fcu_space s, fcu_matrix* out) {
       LAUNCH_CHECK(ctx);
     }
     sync(ctx);
+    s->refs++;
+    ctx->refs++;
     *out = m.release();
   });
 }
@@ -577,16 +611,12 @@ int fcu_matrix_from_csc(fcu_ctx ctx, int64_t n, const int64_t* colptr, const int
     m->diag_pos = m->own_diag_pos.p;
     m->has_values = true;
     sync(ctx);
+    ctx->refs++;
     *out = m.release();
   });
 }
 
-void fcu_matrix_destroy(fcu_matrix m) {
-  if (!m) return;
-  cudaSetDevice(m->ctx->device);
-  cudaStreamSynchronize(m->ctx->stream);
-  delete m;
-}
+void fcu_matrix_destroy(fcu_matrix m) { matrix_release(m); }
 
 static i64 export_counts(fcu_matrix m, DBuf<i64>& colptr) {
   fcu_ctx ctx = m->ctx;
@@ -664,8 +694,8 @@ int fcu_assemble_stiffness(fcu_ctx ctx, fcu_matrix m, const double* cell_coef) {
   return guarded(ctx, [&] {
     if (!m || !m->space) fail(FCU_ERR_BAD_ARG, "matrix has no function space");
     if (m->space->kind == FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "use fcu_assemble_elasticity for vector spaces");
-    if (m->bc_applied) fail(FCU_ERR_BAD_ARG, "matrix already has Dirichlet conditions applied");
     DevIn<double> coef(ctx, cell_coef, (size_t)m->space->mesh->nc);
+    reset_dirichlet(m);
     assemble_stiffness_impl(m, coef.p);
     m->has_values = true;
     if (coef.staged.p) sync(ctx);
@@ -676,8 +706,8 @@ int fcu_assemble_elasticity(fcu_ctx ctx, fcu_matrix m, double E, double nu, cons
   return guarded(ctx, [&] {
     if (!m || !m->space || m->space->kind != FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "needs a FCU_SPACE_P1_VEC3 matrix");
     if (!(nu > -1.0 && nu < 0.5)) fail(FCU_ERR_BAD_ARG, "Poisson's ratio must be in (-1.0, 0.5) for physical stability");
-    if (m->bc_applied) fail(FCU_ERR_BAD_ARG, "matrix already has Dirichlet conditions applied");
     DevIn<double> ce(ctx, cell_E, (size_t)m->space->mesh->nc);
+    reset_dirichlet(m);
     assemble_elasticity_impl(m, E, nu, ce.p);
     m->has_values = true;
     if (ce.staged.p) sync(ctx);

@@ -23,7 +23,7 @@ constexpr int WARPS = 8;   // warps per block, scalar assembly
 constexpr int EWARPS = 6;  // warps per block, elasticity assembly (shared-memory bound)
 // Staging rows use odd strides (in doubles) so that lanes writing "their" row
 // hit distinct banks.
-constexpr int odd_stride(int k) { return (k % 2) ? k : k + 1; }
+__host__ __device__ constexpr int odd_stride(int k) { return (k % 2) ? k : k + 1; }
 constexpr unsigned FULL = 0xffffffffu;
 
 __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
@@ -106,6 +106,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
     double* __restrict__ v64, float* __restrict__ v32) {
   constexpr int KS = odd_stride(K);
   __shared__ double stage_all[WARPS][32][KS];
+  __shared__ unsigned short ent_all[WARPS][32 * K];
   __shared__ double metric_all[IS_P2 ? WARPS : 1][32][7];
   __shared__ int sa_all[IS_P2 ? WARPS : 1][32];
   __shared__ double R[IS_P2 ? 6 * 100 : 1];
@@ -120,6 +121,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
     const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
     const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
     const i64 ebase = (i64)K * cs;
+    // The row's (contribution, column) entry list, staged once per row with a
+    // coalesced copy when it fits (at most 32 contributions).
+    const bool staged = nct <= 32;
+    if (staged)
+      for (int q = lane; q < K * nct; q += 32) ent_all[wib][q] = slot_ent[ebase + q];
+    __syncwarp();
     int run = 0;  // entries consumed by earlier slot groups
     for (int g0 = 0; g0 < L; g0 += 32) {
       const int s = g0 + lane;
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
         }
         __syncwarp();
         while (e < e1) {
-          const unsigned ent = slot_ent[e];
+          const unsigned ent = staged ? ent_all[wib][e - ebase] : slot_ent[e];
           const int tl = (int)(ent >> 4);
           if (tl >= ch + 32) break;
           acc += stage[tl - ch][ent & 15];
@@ -189,6 +196,7 @@ __global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
     double mu, i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
   __shared__ double st_all[EWARPS][32][17];
   __shared__ double out_all[EWARPS][32 * 9];
+  __shared__ unsigned short ent_all[EWARPS][32 * 4];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double(*st)[17] = st_all[wib];
   double* out = out_all[wib];
@@ -197,6 +205,10 @@ __global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
     const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
     const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
     const i64 ebase = 4 * (i64)cs;
+    const bool staged = nct <= 32;
+    if (staged)
+      for (int q = lane; q < 4 * nct; q += 32) ent_all[wib][q] = slot_ent[ebase + q];
+    __syncwarp();
     int run = 0;
     for (int g0 = 0; g0 < L; g0 += 32) {
       const int s = g0 + lane;
@@ -233,7 +245,7 @@ __global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
         }
         __syncwarp();
         while (e < e1) {
-          const unsigned ent = slot_ent[e];
+          const unsigned ent = staged ? ent_all[wib][e - ebase] : slot_ent[e];
           const int tl = (int)(ent >> 4);
           if (tl >= ch + 32) break;
           const double* w = st[tl - ch];
@@ -313,7 +325,9 @@ __global__ void k_bc_lift(const int* __restrict__ row_ptr, const int* __restrict
 #pragma unroll
       for (int be = 0; be < BS; ++be) {
         const i64 c = j * BS + be;
-        if (count[c] > 0) acc -= v64[(i64)p * BS * BS + al * BS + be] * g[c];
+        // explicit roundings: no FMA contraction, same arithmetic as the
+        // reference's `new_b[row] -= val * dirichlet_val[col]`
+        if (count[c] > 0) acc = __dsub_rn(acc, __dmul_rn(v64[(i64)p * BS * BS + al * BS + be], g[c]));
       }
     }
     b[t] = acc;

@@ -73,7 +73,11 @@ struct DBuf {
 
 struct Workspace;  // solver state, defined in solver.cu
 
+// Handles are reference counted: a mesh holds its context, a space its mesh,
+// a matrix its space and context. fcu_*_destroy drops the caller's reference,
+// so handles may be destroyed in any order.
 struct fcu_ctx_s {
+  int refs = 1;
   int device = 0;
   cudaStream_t stream = nullptr;
   std::string err;
@@ -87,6 +91,7 @@ struct fcu_ctx_s {
 };
 
 struct fcu_mesh_s {
+  int refs = 1;
   fcu_ctx ctx = nullptr;
   int dim = 0, nodes = 0;
   i64 nv = 0, nc = 0;
@@ -100,6 +105,7 @@ struct fcu_mesh_s {
 // the vector space whose 3x3 blocks are stored contiguously) plus the
 // row-gather structures the assembly kernels read.
 struct fcu_space_s {
+  int refs = 1;
   fcu_ctx ctx = nullptr;
   fcu_mesh mesh = nullptr;
   int kind = 0;
@@ -125,6 +131,7 @@ struct fcu_space_s {
 };
 
 struct fcu_matrix_s {
+  int refs = 1;
   fcu_ctx ctx = nullptr;
   fcu_space space = nullptr;   // nullptr for a wrapped CSC/CSR
   i64 n = 0;                   // scalar order

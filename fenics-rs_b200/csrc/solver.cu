@@ -1,23 +1,39 @@
-// Jacobi-preconditioned CG on the device: FP64 (the arithmetic of
-// cg.rs:40-149) and mixed precision (FP32 SpMV and vector updates, FP64 dot
-// accumulation, FP64 residual replacement b - A64 x64 and FP64 solution
-// accumulation).
+// Jacobi-preconditioned CG on the device.
 //
-// Each iteration is three (FP64) or four (mixed) kernels:
-//   spmv      Ap = A p, and p.Ap reduced on the device -> alpha
-//   update    x += alpha p, r -= alpha Ap, z = D^-1 r, r.z and r.r -> beta,
-//             convergence / iteration-limit decision
-//   [reliable mixed only, and only when triggered: r = b - A64 (x64 + x32)]
-//   direction p = D^-1 r + beta p
-// Scalars never leave the device: every reduction ends in the block that
-// finishes last, which sums the per-block partials in a fixed order
-// (deterministic) and writes alpha/beta/flags to a small state record. The
-// iteration loop is captured once per matrix as a CUDA graph of CHUNK
-// iterations; kernels of a converged solve return immediately, and the host
+// FCU_FP64 follows the arithmetic of cg.rs:40-149 (up to the order of the
+// dot-product sums). FCU_MIXED runs the inner iteration on FP32 values:
+//   * the operator is applied in difference form (see bsr3_row / csr_row):
+//     off-diagonal FP32 entries act on x_j - x_i and the diagonal slot holds
+//     the FP64 row sum rounded to FP32, so constants (rigid translations) are
+//     reproduced exactly and smooth fields lose no accuracy to cancellation;
+//   * search direction p, Ap and z = D^-1 r in FP32, FP32 arithmetic in SpMV;
+//   * residual r, iterate x, alpha/beta and every dot product in FP64;
+//   * residual replacement r = b - A64 x with the FP64 matrix when the
+//     recursive residual has dropped 10x since the last replacement or claims
+//     convergence, which is then decided on the FP64 residual.
+// Plain FP32 for the whole iteration (r, x or the operator rounded entry by
+// entry) does not converge to 1e-8 on stiff elasticity systems: rounding
+// errors act on the smooth (bending) modes with a relative size of about
+// eps32 * cond(A).
+//
+// Each iteration is two kernels, one per global reduction of PCG:
+//   spmv     p = z + beta p_old (own rows written, neighbours recomputed on
+//            the fly), Ap = A p, p.Ap reduced on the device -> alpha
+//   update   x += alpha p, r -= alpha Ap, z = D^-1 r written, r.z and r.r ->
+//            beta, convergence / iteration-limit decision
+// plus, in mixed precision, the replacement kernel, which returns at once
+// unless the update kernel asked for it. p is double-buffered across
+// iterations. Every reduction ends in the block that finishes last, which sums
+// the per-block partials in a fixed order (deterministic) and writes
+// alpha / beta / flags to a small device state record. The loop is captured
+// once per matrix as a CUDA graph of CHUNK iterations, launched with
+// programmatic dependent launch so each kernel is scheduled while its
+// predecessor drains; kernels of a finished solve return at once, and the host
 // polls the state once per chunk.
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "internal.cuh"
 
@@ -26,15 +42,16 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int VBLOCK = 256;  // threads per block in solver kernels
 constexpr int MAXG = 4096;   // max blocks of a reducing kernel (partials capacity)
-constexpr int CHUNK = 16;    // iterations per graph launch
+constexpr int CHUNK = 16;    // iterations per graph launch (even: p double buffer)
 
 struct CgState {
   double rz, alpha, beta, bnorm, tol, rr, maxr, delta;
   long long iter, max_iter, updates;
-  int done, status, do_update, fold;
+  int done, status, do_update;
   int gpu_semantics;  // solve_csr_cg_gpu: no breakdown test, beta guard, Ok at limit
-  int pad;
-  unsigned ticket[4];
+  int fault;          // a bounded wait in a kernel gave up (reported as FCU_ERR_CUDA)
+  // arrival counters of the grid reductions: 32 group counters + 1 top counter
+  unsigned ticket[4][33];
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -43,13 +60,28 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may be scheduled while its predecessor drains. It waits here
+// until the predecessor has completed and its writes are visible, then
+// allows its own successor to be scheduled (which in turn waits the same way).
+__device__ __forceinline__ void grid_dep_sync() {
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 900)
+  cudaGridDependencySynchronize();
+  cudaTriggerProgrammaticLaunchCompletion();
+#endif
+}
+
 // Block-reduce NV doubles; the last block to finish reduces all partials in
 // fixed order and returns true (tot valid in every thread of that block).
+// Arrivals are counted in two levels (block b joins group b % 32; the last
+// block of a group joins the top counter) so that at most ~gridDim/32 + 32
+// same-address atomics lie on the critical path.
 template <int NV>
 __device__ bool grid_reduce(double (&v)[NV], double* __restrict__ partials, unsigned* ticket, double (&tot)[NV]) {
-  __shared__ double sh[NV][VBLOCK / 32];
+  __shared__ double sh[NV][32];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = (int)(blockDim.x >> 5);
 #pragma unroll
   for (int j = 0; j < NV; ++j) {
     double x = warp_sum(v[j]);
@@ -60,12 +92,24 @@ __device__ bool grid_reduce(double (&v)[NV], double* __restrict__ partials, unsi
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
       double s = 0.0;
-      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[j][q];
+      for (int q = 0; q < nw; ++q) s += sh[j][q];
       partials[j * MAXG + blockIdx.x] = s;
     }
+    const unsigned G = gridDim.x;
+    const unsigned grp = blockIdx.x & 31u;
+    const unsigned gsize = (G - grp + 31u) >> 5;  // blocks with this residue
+    const unsigned ngroups = G < 32u ? G : 32u;
     __threadfence();
-    unsigned t = atomicAdd(ticket, 1u);
-    last = (t == gridDim.x - 1);
+    bool is_last = false;
+    if (atomicAdd(&ticket[grp], 1u) == gsize - 1) {
+      ticket[grp] = 0u;
+      __threadfence();
+      if (atomicAdd(&ticket[32], 1u) == ngroups - 1) {
+        ticket[32] = 0u;
+        is_last = true;
+      }
+    }
+    last = is_last;
   }
   __syncthreads();
   if (!last) return false;
@@ -79,57 +123,95 @@ __device__ bool grid_reduce(double (&v)[NV], double* __restrict__ partials, unsi
     if (lane == 0) sh[j][w] = s;
     __syncthreads();
     double t2 = 0.0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t2 += sh[j][q];
+    for (int q = 0; q < nw; ++q) t2 += sh[j][q];
     tot[j] = t2;
   }
-  if (threadIdx.x == 0) *ticket = 0u;
   return true;
 }
 
 // ---------------------------------------------------------------------------
-// Row kernels. CSR: VPR lanes per row. 3x3-block CSR: 15 lanes per block
-// row, lane 3j+a handles row a of blocks j, j+5, j+10, ...
+// Row kernels. CSR: VPR lanes per row. 3x3-block CSR: a half-warp per block
+// row, lane 3j+a (j < 5) handles component row a of blocks j, j+5, j+10, with
+// the three blocks' loads issued together.
+//
+// DIFF selects the difference form used by the mixed operator: the diagonal
+// (block) slot holds the row sum S_i = sum_j A_ij of the FP64 matrix, and
+//   y_i = sum_{j != i} A_ij (x_j - x_i) + S_i x_i,
+// which equals sum_j A_ij x_j but keeps constants exact and avoids the
+// cancellation between large off-diagonal and diagonal terms, so FP32
+// storage and arithmetic lose only a first-order (smooth-field) accuracy.
+//
+// The operand is read through a gather functor gx(i) (a plain vector, or
+// the new search direction computed on the fly).
 // ---------------------------------------------------------------------------
 
 template <class T>
 struct XPlain {
   const T* x;
-  __device__ __forceinline__ T operator()(i64 c) const { return x[c]; }
-};
-struct XSum {  // x64 + x32 (mixed precision residual)
-  const double* a;
-  const float* b;
-  __device__ __forceinline__ double operator()(i64 c) const { return a[c] + (double)b[c]; }
+  __device__ __forceinline__ T operator()(i64 i) const { return x[i]; }
 };
 
-template <int VPR, class T, class TA, class GX>
-__device__ __forceinline__ TA csr_row(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
-                                      i64 row, bool valid, int sub, const GX& gx) {
-  TA s = TA(0);
+// p_new(i) = z(i) + beta * p_old(i)
+template <class T>
+struct XDirection {
+  const T* z;
+  const T* pold;
+  T beta;
+  __device__ __forceinline__ T operator()(i64 i) const { return z[i] + beta * pold[i]; }
+};
+
+template <int VPR, bool DIFF, class T, class GX>
+__device__ __forceinline__ T csr_row(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
+                                     i64 row, bool valid, int sub, const GX& gx) {
+  T s = T(0);
   if (valid) {
     const int b = rp[row], e = rp[row + 1];
-    for (int p = b + sub; p < e; p += VPR) s += (TA)val[p] * (TA)gx(ci[p]);
+    const T xi = DIFF ? gx(row) : T(0);
+    for (int p = b + sub; p < e; p += VPR) {
+      const int c = ci[p];
+      if (DIFF) s += val[p] * (c == (int)row ? xi : gx(c) - xi);
+      else s += val[p] * gx(c);
+    }
   }
 #pragma unroll
   for (int o = VPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
   return s;
 }
 
-// Returns the partial of row-component a = sub (valid for sub < 3).
-template <class T, class TA, class GX>
-__device__ __forceinline__ TA bsr3_row(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
-                                       i64 row, bool valid, int sub, const GX& gx) {
-  TA s = TA(0);
+template <bool DIFF, class T, class GX>
+__device__ __forceinline__ T bsr3_block(const T* __restrict__ v, const GX& gx, int c, i64 row, T x0, T x1, T x2) {
+  const i64 c3 = 3 * (i64)c;
+  if (!DIFF) return v[0] * gx(c3) + v[1] * gx(c3 + 1) + v[2] * gx(c3 + 2);
+  if (c == (int)row) return v[0] * x0 + v[1] * x1 + v[2] * x2;
+  return v[0] * (gx(c3) - x0) + v[1] * (gx(c3 + 1) - x1) + v[2] * (gx(c3 + 2) - x2);
+}
+
+template <bool DIFF, class T, class GX>
+__device__ __forceinline__ T bsr3_row(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val,
+                                      i64 row, bool valid, int sub, const GX& gx) {
+  T s = T(0);
   if (valid && sub < 15) {
     const int j = sub / 3, a = sub - 3 * j;
     const int b = rp[row], e = rp[row + 1];
-    for (int kb = b + j; kb < e; kb += 5) {
-      const i64 c = 3 * (i64)ci[kb];
-      const T* v = val + 9 * (i64)kb + 3 * a;
-      s += (TA)v[0] * (TA)gx(c) + (TA)v[1] * (TA)gx(c + 1) + (TA)v[2] * (TA)gx(c + 2);
+    T x0 = T(0), x1 = T(0), x2 = T(0);
+    if (DIFF) {
+      x0 = gx(3 * row);
+      x1 = gx(3 * row + 1);
+      x2 = gx(3 * row + 2);
+    }
+    for (int k0 = b + j; k0 < e; k0 += 15) {
+      const int k1 = k0 + 5, k2 = k0 + 10;
+      const bool h1 = k1 < e, h2 = k2 < e;
+      const int c0 = ci[k0];
+      const int c1 = h1 ? ci[k1] : 0;
+      const int c2 = h2 ? ci[k2] : 0;
+      T t = bsr3_block<DIFF>(val + 9 * (i64)k0 + 3 * a, gx, c0, row, x0, x1, x2);
+      if (h1) t += bsr3_block<DIFF>(val + 9 * (i64)k1 + 3 * a, gx, c1, row, x0, x1, x2);
+      if (h2) t += bsr3_block<DIFF>(val + 9 * (i64)k2 + 3 * a, gx, c2, row, x0, x1, x2);
+      s += t;
     }
   }
-  TA t;
+  T t;
   t = __shfl_down_sync(FULL, s, 3, 16);
   if (sub + 3 < 16) s += t;
   t = __shfl_down_sync(FULL, s, 6, 16);
@@ -139,9 +221,9 @@ __device__ __forceinline__ TA bsr3_row(const int* __restrict__ rp, const int* __
   return s;
 }
 
-// Iterate the rows handled by this thread group; calls emit(row_scalar_index,
-// value) once per output scalar row (from one lane).
-template <int BS, int VPR, class T, class TA, class GX, class Emit>
+// Iterate the rows handled by this warp; emit(node, component, value) once
+// per output scalar row (from one lane).
+template <int BS, int VPR, bool DIFF, class T, class GX, class Emit>
 __device__ __forceinline__ void spmv_rows(const int* __restrict__ rp, const int* __restrict__ ci,
                                           const T* __restrict__ val, i64 nrows, const GX& gx, Emit& emit) {
   constexpr int G = (BS == 3) ? 16 : VPR;  // lanes per node row
@@ -154,22 +236,66 @@ __device__ __forceinline__ void spmv_rows(const int* __restrict__ rp, const int*
     const i64 row = base + lane / G;
     const bool valid = row < nrows;
     if (BS == 3) {
-      TA s = bsr3_row<T, TA>(rp, ci, val, row, valid, sub, gx);
-      if (valid && sub < 3) emit(3 * row + sub, s);
+      T s = bsr3_row<DIFF, T>(rp, ci, val, row, valid, sub, gx);
+      if (valid && sub < 3) emit(row, sub, s);
     } else {
-      TA s = csr_row<VPR, T, TA>(rp, ci, val, row, valid, sub, gx);
-      if (valid && sub == 0) emit(row, s);
+      T s = csr_row<VPR, DIFF, T>(rp, ci, val, row, valid, sub, gx);
+      if (valid && sub == 0) emit(row, 0, s);
     }
   }
 }
 
-// --- CG step 1: Ap = A p, p.Ap -> alpha ------------------------------------
-template <class T>
+__device__ __forceinline__ void set_alpha(CgState* st, double pap) {
+  if (!st->gpu_semantics && fabs(pap) < 1e-30) {
+    st->done = 1;
+    st->status = FCU_ERR_BREAKDOWN;
+    st->iter += 1;
+  } else {
+    st->alpha = st->rz / pap;
+  }
+}
+
+// --- spmv: p = z + beta p_old ; Ap = A p ; p.Ap -> alpha -----------------------
+template <int BS, class T>
 struct EmitAp {
+  XDirection<T> dir;
+  T* pnew;
+  T* ap;
+  double dot = 0.0;
+  __device__ __forceinline__ void operator()(i64 node, int a, T s) {
+    const i64 i = node * BS + a;
+    const T pi = dir(i);
+    pnew[i] = pi;
+    ap[i] = s;
+    dot += (double)pi * (double)s;
+  }
+};
+
+// T = double: FP64 matrix and vectors. T = float: mixed operator (difference
+// form on the FP32 values with row sums in the diagonal slots).
+template <int BS, int VPR, class T>
+__global__ void __launch_bounds__(VBLOCK) k_spmv_dir(const int* __restrict__ rp, const int* __restrict__ ci,
+                                                     const T* __restrict__ val, i64 nrows, const T* __restrict__ z,
+                                                     const T* __restrict__ pold, T* __restrict__ pnew,
+                                                     T* __restrict__ ap, CgState* st, double* partials) {
+  grid_dep_sync();
+  if (st->done) return;
+  const XDirection<T> dir{z, pold, (T)st->beta};
+  EmitAp<BS, T> em{dir, pnew, ap};
+  constexpr bool DIFF = sizeof(T) == 4;
+  spmv_rows<BS, VPR, DIFF, T>(rp, ci, val, nrows, dir, em);
+  double v[1] = {em.dot}, tot[1];
+  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) set_alpha(st, tot[0]);
+}
+
+// Unfused variant: p already updated by k_direction; Ap = A p.
+template <int BS, class T>
+struct EmitApPlain {
   const T* p;
   T* ap;
   double dot = 0.0;
-  __device__ __forceinline__ void operator()(i64 i, T s) {
+  __device__ __forceinline__ void operator()(i64 node, int a, T s) {
+    const i64 i = node * BS + a;
     ap[i] = s;
     dot += (double)p[i] * (double)s;
   }
@@ -179,23 +305,248 @@ template <int BS, int VPR, class T>
 __global__ void __launch_bounds__(VBLOCK) k_spmv_ap(const int* __restrict__ rp, const int* __restrict__ ci,
                                                     const T* __restrict__ val, i64 nrows, const T* __restrict__ p,
                                                     T* __restrict__ ap, CgState* st, double* partials) {
+  grid_dep_sync();
   if (st->done) return;
-  EmitAp<T> em{p, ap};
-  spmv_rows<BS, VPR, T, T>(rp, ci, val, nrows, XPlain<T>{p}, em);
+  EmitApPlain<BS, T> em{p, ap};
+  constexpr bool DIFF = sizeof(T) == 4;
+  spmv_rows<BS, VPR, DIFF, T>(rp, ci, val, nrows, XPlain<T>{p}, em);
   double v[1] = {em.dot}, tot[1];
-  if (grid_reduce<1>(v, partials, &st->ticket[0], tot) && threadIdx.x == 0) {
-    const double pap = tot[0];
-    if (!st->gpu_semantics && fabs(pap) < 1e-30) {
+  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) set_alpha(st, tot[0]);
+}
+
+// p = z + beta p (in place), for the unfused iteration.
+template <class T>
+__global__ void __launch_bounds__(VBLOCK) k_direction(i64 n, T* __restrict__ p, const T* __restrict__ z,
+                                                      const CgState* st) {
+  grid_dep_sync();
+  if (st->done) return;
+  const T beta = (T)st->beta;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
+
+// --- 3x3-block SpMV with TMA-staged tiles --------------------------------------
+// A persistent CTA walks tiles of TR consecutive block rows. One thread streams
+// each tile's row pointers, column indices and block values into shared memory
+// with bulk asynchronous copies (cp.async.bulk, completion counted on an
+// mbarrier), two stages deep, while the CTA's warps compute the previous tile
+// from shared memory; only the operand gathers touch L2. Copies start and end
+// on 16-byte boundaries (ranges are widened outward by at most 12 bytes on each
+// side, so regions reserve 32 bytes of slack; device arrays carry 16 bytes of
+// padding past their end), and every mbarrier wait is bounded: on expiry the kernel
+// records a fault in the state record and stops.
+
+constexpr int TILE_ROWS = 32;      // block rows per tile (one half-warp each)
+constexpr int TILE_THREADS = 512;  // 16 warps: all 32 rows of a tile at once
+constexpr unsigned WAIT_LIMIT = 1u << 24;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait; false when the limit expired.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (unsigned i = 0; i < WAIT_LIMIT; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Per-stage layout: [header 64 B][row ptrs][cols][values], regions 128-aligned.
+struct TileHeader {
+  int b0;        // first block of the tile
+  int rows;      // rows in the tile
+  int col_off;   // byte offset of ci[b0] inside the staged column region
+  int val_off;   // byte offset of val[9*b0] inside the staged value region
+};
+
+__host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
+
+template <class T>
+__host__ __device__ size_t tile_stage_bytes(int cap_blocks) {
+  return align128(sizeof(TileHeader)) + align128((TILE_ROWS + 1) * 4 + 16) + align128((size_t)cap_blocks * 4 + 32) +
+         align128((size_t)cap_blocks * 9 * sizeof(T) + 32);
+}
+
+// Warp-specialised pipeline: warp 0 is the producer (one elected lane issues
+// the bulk copies for tiles NSTAGE ahead, waiting on per-stage "empty"
+// barriers), warps 1..16 are consumers (each half-warp owns one block row of
+// the tile; lane l handles blocks l, l+16, ... of it, reading the block's 9
+// values and column from shared memory and the three operand entries once,
+// keeping three partial sums that a 16-lane shuffle tree reduces). Consumers
+// wait on per-stage "full" barriers and release a stage by arriving on its
+// empty barrier.
+constexpr int SPMV_CONSUMER_WARPS = 16;
+constexpr int SPMV_THREADS = 32 * (SPMV_CONSUMER_WARPS + 1);
+constexpr int MAX_STAGES = 4;
+
+template <bool DIFF, class T, class GX, class Emit>
+__device__ __forceinline__ void bsr3_tiled_rows(const int* __restrict__ rp, const int* __restrict__ ci,
+                                                const T* __restrict__ val, i64 nrows, int cap_blocks, int nstage,
+                                                const GX& gx, Emit& emit, int* fault) {
+  extern __shared__ __align__(128) unsigned char tile_smem[];
+  __shared__ unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
+  const size_t stage_bytes = tile_stage_bytes<T>(cap_blocks);
+  const i64 ntiles = (nrows + TILE_ROWS - 1) / TILE_ROWS;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < nstage; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], SPMV_CONSUMER_WARPS);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int k = 0;
+      bool ok = true;
+      for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        const int s = k % nstage;
+        const int use = k / nstage;
+        if (use > 0 && !mbar_wait(&empty[s], (unsigned)((use - 1) & 1))) {
+          atomicExch(fault, 1);
+          ok = false;
+          break;
+        }
+        unsigned char* base = tile_smem + s * stage_bytes;
+        TileHeader* h = reinterpret_cast<TileHeader*>(base);
+        unsigned char* rps = base + align128(sizeof(TileHeader));
+        unsigned char* cs = rps + align128((TILE_ROWS + 1) * 4 + 16);
+        unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
+        const i64 r0 = t * TILE_ROWS;
+        const int rows = (int)min((i64)TILE_ROWS, nrows - r0);
+        const int b0 = rp[r0], b1 = rp[r0 + rows];
+        const unsigned rp_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);
+        const uintptr_t c_lo = reinterpret_cast<uintptr_t>(ci + b0) & ~(uintptr_t)15;
+        const uintptr_t c_hi = (reinterpret_cast<uintptr_t>(ci + b1) + 15) & ~(uintptr_t)15;
+        const uintptr_t v_lo = reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) & ~(uintptr_t)15;
+        const uintptr_t v_hi = (reinterpret_cast<uintptr_t>(val + 9 * (i64)b1) + 15) & ~(uintptr_t)15;
+        h->b0 = b0;
+        h->rows = rows;
+        h->col_off = (int)(reinterpret_cast<uintptr_t>(ci + b0) - c_lo);
+        h->val_off = (int)(reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) - v_lo);
+        const unsigned cb = (unsigned)(c_hi - c_lo), vb = (unsigned)(v_hi - v_lo);
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&full[s], rp_bytes + cb + vb);
+        bulk_load(rps, rp + r0, rp_bytes, &full[s]);
+        if (cb) bulk_load(cs, reinterpret_cast<const void*>(c_lo), cb, &full[s]);
+        if (vb) bulk_load(vs, reinterpret_cast<const void*>(v_lo), vb, &full[s]);
+      }
+      if (!ok) {
+        // let copies already issued land before the CTA exits (bounded)
+        for (int s = 0; s < nstage; ++s) mbar_wait(&full[s], 0);
+      }
+    }
+    return;
+  }
+
+  // consumers
+  const int sub = lane & 15;
+  const int row_in_tile = (warp - 1) * 2 + (lane >> 4);
+  int k = 0;
+  for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+    const int s = k % nstage;
+    const int use = k / nstage;
+    if (!mbar_wait(&full[s], (unsigned)(use & 1))) {
+      if (lane == 0) atomicExch(fault, 1);
+      break;
+    }
+    unsigned char* base = tile_smem + s * stage_bytes;
+    const TileHeader* h = reinterpret_cast<const TileHeader*>(base);
+    const int* rps = reinterpret_cast<const int*>(base + align128(sizeof(TileHeader)));
+    const unsigned char* cs = base + align128(sizeof(TileHeader)) + align128((TILE_ROWS + 1) * 4 + 16);
+    const unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
+    const int* cis = reinterpret_cast<const int*>(cs + h->col_off);
+    const T* vls = reinterpret_cast<const T*>(vs + h->val_off);
+    const int b0 = h->b0;
+    const i64 row = t * TILE_ROWS + row_in_tile;
+    const bool valid = row_in_tile < h->rows;
+    T a0 = T(0), a1 = T(0), a2 = T(0);
+    if (valid) {
+      T x0 = T(0), x1 = T(0), x2 = T(0);
+      if (DIFF) {
+        x0 = gx(3 * row);
+        x1 = gx(3 * row + 1);
+        x2 = gx(3 * row + 2);
+      }
+      const int kb1 = rps[row_in_tile + 1] - b0;
+      for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += 16) {
+        const int c = cis[kb];
+        const T* v = vls + 9 * kb;
+        const i64 c3 = 3 * (i64)c;
+        T y0, y1, y2;
+        if (DIFF && c == (int)row) {
+          y0 = x0; y1 = x1; y2 = x2;
+        } else if (DIFF) {
+          y0 = gx(c3) - x0; y1 = gx(c3 + 1) - x1; y2 = gx(c3 + 2) - x2;
+        } else {
+          y0 = gx(c3); y1 = gx(c3 + 1); y2 = gx(c3 + 2);
+        }
+        a0 += v[0] * y0 + v[1] * y1 + v[2] * y2;
+        a1 += v[3] * y0 + v[4] * y1 + v[5] * y2;
+        a2 += v[6] * y0 + v[7] * y1 + v[8] * y2;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(FULL, a0, o);
+      a1 += __shfl_xor_sync(FULL, a1, o);
+      a2 += __shfl_xor_sync(FULL, a2, o);
+    }
+    if (valid && sub < 3) emit(row, sub, sub == 0 ? a0 : (sub == 1 ? a1 : a2));
+  }
+}
+
+template <int DIFF, class T>
+__global__ void __launch_bounds__(SPMV_THREADS) k_spmv_tiled(const int* __restrict__ rp, const int* __restrict__ ci,
+                                                            const T* __restrict__ val, i64 nrows, int cap_blocks,
+                                                            int nstage, const T* __restrict__ p, T* __restrict__ ap,
+                                                            CgState* st, double* partials) {
+  grid_dep_sync();
+  if (st->done) return;
+  EmitApPlain<3, T> em{p, ap};
+  bsr3_tiled_rows<DIFF != 0, T>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, &st->fault);
+  double v[1] = {em.dot}, tot[1];
+  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) {
+    if (st->fault) {
       st->done = 1;
-      st->status = FCU_ERR_BREAKDOWN;
-      st->iter += 1;
+      st->status = FCU_ERR_CUDA;
     } else {
-      st->alpha = st->rz / pap;
+      set_alpha(st, tot[0]);
     }
   }
 }
 
-// --- FP64 update ------------------------------------------------------------
+// --- update -----------------------------------------------------------------
 __device__ __forceinline__ void decide_after_update(CgState* st, double rz_new, double rr) {
   st->iter += 1;
   st->rr = rr;
@@ -212,60 +563,93 @@ __device__ __forceinline__ void decide_after_update(CgState* st, double rz_new, 
   st->rz = rz_new;
 }
 
-__global__ void __launch_bounds__(VBLOCK) k_cg_update(i64 n, double* __restrict__ x, double* __restrict__ r,
-                                                      const double* __restrict__ p, const double* __restrict__ ap,
-                                                      const double* __restrict__ invd, CgState* st,
-                                                      double* partials) {
+// x += alpha p ; r -= alpha Ap ; z = D^-1 r (stored as T) ; (r.z, r.r).
+// x, r and D^-1 are FP64 in both precisions.
+template <class T>
+__global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x, double* __restrict__ r,
+                                                   const T* __restrict__ p, const T* __restrict__ ap,
+                                                   const double* __restrict__ invd, T* __restrict__ z, CgState* st,
+                                                   double* partials) {
+  grid_dep_sync();
   if (st->done) return;
   const double alpha = st->alpha;
   double rz = 0.0, rr = 0.0;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-    x[i] += alpha * p[i];
-    const double ri = r[i] - alpha * ap[i];
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+#pragma unroll 2
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += stride) {
+    x[i] += alpha * (double)p[i];
+    const double ri = r[i] - alpha * (double)ap[i];
     r[i] = ri;
-    const double z = ri * invd[i];
-    rz += ri * z;
+    const double zi = ri * invd[i];
+    z[i] = (T)zi;
+    rz += ri * zi;
     rr += ri * ri;
   }
   double v[2] = {rz, rr}, tot[2];
-  if (grid_reduce<2>(v, partials, &st->ticket[1], tot) && threadIdx.x == 0) decide_after_update(st, tot[0], tot[1]);
+  if (grid_reduce<2>(v, partials, st->ticket[1], tot) && threadIdx.x == 0) {
+    if (sizeof(T) == 8) {
+      decide_after_update(st, tot[0], tot[1]);
+    } else {
+      // mixed: replace the residual when it has dropped by `delta` since the
+      // last replacement or claims convergence; otherwise continue.
+      st->iter += 1;
+      st->rr = tot[1];
+      const double res = sqrt(tot[1]);
+      const double rel = st->bnorm > 0.0 ? res / st->bnorm : res;
+      st->do_update = (rel < st->tol || res < st->delta * st->maxr) ? 1 : 0;
+      if (!st->do_update) {
+        if (st->iter >= st->max_iter) {
+          st->done = 1;
+          st->status = FCU_ERR_NO_CONVERGENCE;
+          return;
+        }
+        st->beta = tot[0] / st->rz;
+        st->rz = tot[0];
+      }
+    }
+  }
 }
 
-template <class T>
-__global__ void __launch_bounds__(VBLOCK) k_cg_direction(i64 n, T* __restrict__ p, const T* __restrict__ r,
-                                                         const T* __restrict__ invd, const CgState* st) {
-  if (st->done) return;
-  const T beta = (T)st->beta;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
-    p[i] = r[i] * invd[i] + beta * p[i];
-}
-
-// --- initialisation ---------------------------------------------------------
-struct EmitRes {  // r = b - A x (FP64), rr, bb
+// --- residual: r = b - A64 x, z = D^-1 r (init, and the mixed replacement) ----
+template <int BS, class T>
+struct EmitRes {
   const double* b;
+  const double* invd;
   double* r;
-  double rr = 0.0;
-  __device__ __forceinline__ void operator()(i64 i, double s) {
+  T* z;
+  double rr = 0.0, rz = 0.0;
+  __device__ __forceinline__ void operator()(i64 node, int a, double s) {
+    const i64 i = node * BS + a;
     const double v = b[i] - s;
     r[i] = v;
+    const double zi = v * invd[i];
+    z[i] = (T)zi;
     rr += v * v;
+    rz += v * zi;
   }
 };
 
-template <int BS, int VPR>
+template <int BS, int VPR, class T>
 __global__ void __launch_bounds__(VBLOCK) k_init_residual(const int* __restrict__ rp, const int* __restrict__ ci,
                                                           const double* __restrict__ val, i64 nrows,
                                                           const double* __restrict__ x, const double* __restrict__ b,
-                                                          double* __restrict__ r, i64 n, CgState* st,
+                                                          const double* __restrict__ invd, double* __restrict__ r,
+                                                          T* __restrict__ z, T* __restrict__ pold, i64 n, CgState* st,
                                                           double* partials) {
-  EmitRes em{b, r};
-  spmv_rows<BS, VPR, double, double>(rp, ci, val, nrows, XPlain<double>{x}, em);
+  grid_dep_sync();
+  EmitRes<BS, T> em{b, invd, r, z};
+  spmv_rows<BS, VPR, false, double>(rp, ci, val, nrows, XPlain<double>{x}, em);
   double bb = 0.0;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) bb += b[i] * b[i];
-  double v[2] = {em.rr, bb}, tot[2];
-  if (grid_reduce<2>(v, partials, &st->ticket[2], tot) && threadIdx.x == 0) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    bb += b[i] * b[i];
+    pold[i] = T(0);
+  }
+  double v[3] = {em.rr, bb, em.rz}, tot[3];
+  if (grid_reduce<3>(v, partials, st->ticket[2], tot) && threadIdx.x == 0) {
     st->bnorm = sqrt(tot[1]);
     st->rr = tot[0];
+    st->rz = tot[2];
+    st->beta = 0.0;  // first direction p = z
     const double r0 = sqrt(tot[0]);
     st->maxr = r0;
     // cg.rs:87-90
@@ -276,108 +660,18 @@ __global__ void __launch_bounds__(VBLOCK) k_init_residual(const int* __restrict_
   }
 }
 
-// inv_diag (cg.rs:52-64): 1/a_kk when |a_kk| > 1e-15, else 1.
-template <int BS>
-__global__ void k_inv_diag(const int* __restrict__ diag_pos, const double* __restrict__ val, i64 nn,
-                           double* __restrict__ invd, float* __restrict__ invd32) {
-  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nn * BS; t += (i64)gridDim.x * blockDim.x) {
-    const i64 node = t / BS;
-    const int a = (int)(t - node * BS);
-    const double d = val[(i64)diag_pos[node] * BS * BS + a * BS + a];
-    const double iv = fabs(d) > 1e-15 ? 1.0 / d : 1.0;
-    invd[t] = iv;
-    invd32[t] = (float)iv;
-  }
-}
-
-// z = D^-1 r, p = z, rz (FP64) ; or the FP32 copies for the mixed path.
-__global__ void __launch_bounds__(VBLOCK) k_init_direction(i64 n, const double* __restrict__ r,
-                                                           const double* __restrict__ invd, double* __restrict__ p,
-                                                           float* __restrict__ r32, const float* __restrict__ invd32,
-                                                           float* __restrict__ p32, CgState* st, double* partials) {
-  double rz = 0.0;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-    if (r32) {
-      const float rf = (float)r[i];
-      r32[i] = rf;
-      const float z = rf * invd32[i];
-      p32[i] = z;
-      rz += (double)rf * (double)z;
-    } else {
-      const double z = r[i] * invd[i];
-      p[i] = z;
-      rz += r[i] * z;
-    }
-  }
-  double v[1] = {rz}, tot[1];
-  if (grid_reduce<1>(v, partials, &st->ticket[3], tot) && threadIdx.x == 0) st->rz = tot[0];
-}
-
-// --- mixed precision --------------------------------------------------------
-__global__ void __launch_bounds__(VBLOCK) k_mx_update(i64 n, float* __restrict__ x32, float* __restrict__ r32,
-                                                      const float* __restrict__ p32, const float* __restrict__ ap32,
-                                                      const float* __restrict__ invd32, CgState* st,
-                                                      double* partials) {
-  if (st->done) return;
-  const float alpha = (float)st->alpha;
-  double rz = 0.0, rr = 0.0;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-    x32[i] += alpha * p32[i];
-    const float ri = r32[i] - alpha * ap32[i];
-    r32[i] = ri;
-    const float z = ri * invd32[i];
-    rz += (double)ri * (double)z;
-    rr += (double)ri * (double)ri;
-  }
-  double v[2] = {rz, rr}, tot[2];
-  if (grid_reduce<2>(v, partials, &st->ticket[1], tot) && threadIdx.x == 0) {
-    st->iter += 1;
-    st->fold = 0;
-    const double res = sqrt(tot[1]);
-    const double rel = st->bnorm > 0.0 ? res / st->bnorm : res;
-    st->rr = tot[1];
-    // Replace the recursively updated residual by the true FP64 one when it
-    // has dropped by `delta` since the last replacement, or claims convergence.
-    st->do_update = (rel < st->tol || res < st->delta * st->maxr) ? 1 : 0;
-    if (!st->do_update) {
-      if (st->iter >= st->max_iter) {
-        st->done = 1;
-        st->status = FCU_ERR_NO_CONVERGENCE;
-        return;
-      }
-      st->beta = tot[0] / st->rz;
-      st->rz = tot[0];
-    }
-  }
-}
-
-struct EmitReliable {  // r = b - A64 (x64 + x32): r32 = (float) r, rr, rz
-  const double* b;
-  float* r32;
-  const float* invd32;
-  double rr = 0.0, rz = 0.0;
-  __device__ __forceinline__ void operator()(i64 i, double s) {
-    const double v = b[i] - s;
-    rr += v * v;
-    const float rf = (float)v;
-    r32[i] = rf;
-    rz += (double)rf * (double)(rf * invd32[i]);
-  }
-};
-
 template <int BS, int VPR>
-__global__ void __launch_bounds__(VBLOCK) k_mx_reliable(const int* __restrict__ rp, const int* __restrict__ ci,
-                                                        const double* __restrict__ val, i64 nrows,
-                                                        const double* __restrict__ x64, const float* __restrict__ x32,
-                                                        const double* __restrict__ b, float* __restrict__ r32,
-                                                        const float* __restrict__ invd32, CgState* st,
-                                                        double* partials) {
+__global__ void __launch_bounds__(VBLOCK) k_mx_replace(const int* __restrict__ rp, const int* __restrict__ ci,
+                                                       const double* __restrict__ val, i64 nrows,
+                                                       const double* __restrict__ x, const double* __restrict__ b,
+                                                       const double* __restrict__ invd, double* __restrict__ r,
+                                                       float* __restrict__ z, CgState* st, double* partials) {
+  grid_dep_sync();
   if (st->done || !st->do_update) return;
-  EmitReliable em{b, r32, invd32};
-  spmv_rows<BS, VPR, double, double>(rp, ci, val, nrows, XSum{x64, x32}, em);
+  EmitRes<BS, float> em{b, invd, r, z};
+  spmv_rows<BS, VPR, false, double>(rp, ci, val, nrows, XPlain<double>{x}, em);
   double v[2] = {em.rz, em.rr}, tot[2];
-  if (grid_reduce<2>(v, partials, &st->ticket[2], tot) && threadIdx.x == 0) {
-    st->fold = 1;
+  if (grid_reduce<2>(v, partials, st->ticket[2], tot) && threadIdx.x == 0) {
     st->updates += 1;
     st->rr = tot[1];
     const double res = sqrt(tot[1]);
@@ -390,39 +684,46 @@ __global__ void __launch_bounds__(VBLOCK) k_mx_reliable(const int* __restrict__ 
   }
 }
 
-__global__ void __launch_bounds__(VBLOCK) k_mx_direction(i64 n, float* __restrict__ p32, const float* __restrict__ r32,
-                                                         const float* __restrict__ invd32, double* __restrict__ x64,
-                                                         float* __restrict__ x32, const CgState* st) {
-  const bool fold = st->fold != 0;
-  const bool done = st->done != 0;
-  if (!fold && done) return;
-  const float beta = (float)st->beta;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-    if (fold) {
-      x64[i] += (double)x32[i];
-      x32[i] = 0.0f;
-    }
-    if (!done) p32[i] = r32[i] * invd32[i] + beta * p32[i];
+// inv_diag (cg.rs:52-64): 1/a_kk when |a_kk| > 1e-15, else 1.
+template <int BS>
+__global__ void k_inv_diag(const int* __restrict__ diag_pos, const double* __restrict__ val, i64 nn,
+                           double* __restrict__ invd) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nn * BS; t += (i64)gridDim.x * blockDim.x) {
+    const i64 node = t / BS;
+    const int a = (int)(t - node * BS);
+    const int dp = diag_pos[node];
+    const double d = dp >= 0 ? val[(i64)dp * BS * BS + a * BS + a] : 0.0;
+    invd[t] = fabs(d) > 1e-15 ? 1.0 / d : 1.0;
   }
 }
 
-__global__ void k_fold(i64 n, double* __restrict__ x64, float* __restrict__ x32) {
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-    x64[i] += (double)x32[i];
-    x32[i] = 0.0f;
+// Mixed operator: write into each diagonal (block) slot of the FP32 values
+// the row sums of the FP64 matrix, S_i[a][b] = sum_j A_ij[a][b].
+template <int BS>
+__global__ void k_build_rowsum32(const int* __restrict__ rp, const int* __restrict__ diag_pos,
+                                 const double* __restrict__ v64, i64 nn, float* __restrict__ v32) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nn * BS * BS; t += (i64)gridDim.x * blockDim.x) {
+    const i64 node = t / (BS * BS);
+    const int e = (int)(t - node * BS * BS);
+    double d = 0.0;
+    for (int p = rp[node]; p < rp[node + 1]; ++p) d += v64[(i64)p * BS * BS + e];
+    const int dp = diag_pos[node];
+    if (dp >= 0) v32[(i64)dp * BS * BS + e] = (float)d;
   }
 }
 
 // --- plain SpMV (fcu_spmv) --------------------------------------------------
+template <int BS>
 struct EmitStore {
   double* y;
-  __device__ __forceinline__ void operator()(i64 i, double s) { y[i] = s; }
+  __device__ __forceinline__ void operator()(i64 node, int a, double s) { y[node * BS + a] = s; }
 };
 template <int BS, int VPR>
 __global__ void k_spmv_plain(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ val,
                              i64 nrows, const double* __restrict__ x, double* __restrict__ y) {
-  EmitStore em{y};
-  spmv_rows<BS, VPR, double, double>(rp, ci, val, nrows, XPlain<double>{x}, em);
+  grid_dep_sync();
+  EmitStore<BS> em{y};
+  spmv_rows<BS, VPR, false, double>(rp, ci, val, nrows, XPlain<double>{x}, em);
 }
 
 }  // namespace
@@ -433,14 +734,14 @@ __global__ void k_spmv_plain(const int* __restrict__ rp, const int* __restrict__
 
 struct Workspace {
   i64 n = 0;
-  DBuf<double> x, r, p, ap, b, invd, partials;
-  DBuf<float> x32, r32, p32, ap32, invd32;
+  DBuf<double> x, r, b, invd, partials;
+  DBuf<double> z64, pa64, pb64, ap64;  // FP64 path: z, p (two buffers), Ap
+  DBuf<float> z32, pa32, pb32, ap32;   // mixed path
   DBuf<CgState> st;
   CgState* host_st = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int vpr = 0;  // chosen lanes per row (CSR)
   int grid = 0;
-  bool invd_ready = false;
   ~Workspace() {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
@@ -452,9 +753,20 @@ fcu_matrix_s::~fcu_matrix_s() { delete ws; }
 
 namespace {
 
+// Blocks per SM for the solver kernels (grid-stride loops); FCU_SOLVER_BPSM
+// overrides the default for tuning.
+int blocks_per_sm() {
+  static int v = [] {
+    const char* e = getenv("FCU_SOLVER_BPSM");
+    int x = e ? atoi(e) : 8;
+    return (x >= 1 && x <= 16) ? x : 8;
+  }();
+  return v;
+}
+
 int solver_grid(fcu_ctx ctx, i64 n) {
   i64 want = (n + VBLOCK - 1) / VBLOCK;
-  i64 cap = (i64)ctx->num_sms * 4;
+  i64 cap = (i64)ctx->num_sms * blocks_per_sm();
   return (int)std::max<i64>(1, std::min(want, cap));
 }
 
@@ -474,8 +786,7 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     Workspace* w = m->ws;
     w->n = m->n;
     const i64 n = m->n;
-    w->x.alloc(n); w->r.alloc(n); w->p.alloc(n); w->ap.alloc(n); w->b.alloc(n); w->invd.alloc(n);
-    w->invd32.alloc(n);
+    w->x.alloc(n); w->r.alloc(n); w->b.alloc(n); w->invd.alloc(n);
     w->partials.alloc(3 * MAXG);
     w->st.alloc(1);
     CUDA_CHECK(cudaMemsetAsync(w->st.p, 0, sizeof(CgState), ctx->stream));
@@ -484,66 +795,174 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     w->grid = solver_grid(ctx, n);
   }
   Workspace* w = m->ws;
-  if (mixed && !w->x32.p) {
-    const i64 n = m->n;
-    w->x32.alloc(n); w->r32.alloc(n); w->p32.alloc(n); w->ap32.alloc(n);
+  if (!mixed && !w->z64.p) {
+    w->z64.alloc(m->n); w->pa64.alloc(m->n); w->pb64.alloc(m->n); w->ap64.alloc(m->n);
+  }
+  if (mixed && !w->z32.p) {
+    w->z32.alloc(m->n); w->pa32.alloc(m->n); w->pb32.alloc(m->n); w->ap32.alloc(m->n);
   }
   return w;
 }
 
-// Dispatch a node-row kernel on (BS, VPR).
-#define DISPATCH_ROWS(BS_, VPR_, KERNEL, GRID, ...)                                  \
-  do {                                                                               \
-    if ((BS_) == 3) KERNEL<3, 16><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__);    \
-    else if ((VPR_) == 4) KERNEL<1, 4><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__); \
-    else if ((VPR_) == 8) KERNEL<1, 8><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__); \
-    else if ((VPR_) == 16) KERNEL<1, 16><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__); \
-    else KERNEL<1, 32><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__);               \
-    LAUNCH_CHECK(ctx);                                                               \
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while its predecessor drains, and waits in grid_dep_sync().
+template <class... KArgs, class... Args>
+void launch_pdl(fcu_ctx ctx, void (*kern)(KArgs...), int grid, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(VBLOCK);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+  ctx->launches++;
+}
+
+template <class... KArgs, class... Args>
+void launch_pdl_cfg(fcu_ctx ctx, void (*kern)(KArgs...), int grid, int block, size_t smem, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+  ctx->launches++;
+}
+
+// Tiled 3x3-block SpMV launch: shared memory for two stages sized by the
+// longest block row; grid = resident CTAs (persistent), at most one per tile.
+template <int DIFF, class T>
+void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
+  fcu_ctx ctx = m->ctx;
+  const int max_row = m->space ? m->space->max_row : 32;
+  const int cap = TILE_ROWS * max_row;
+  const int nstage = 3;
+  const size_t smem = nstage * tile_stage_bytes<T>(cap);
+  auto kern = k_spmv_tiled<DIFF, T>;
+  static int configured_dev[2][2] = {{-1, -1}, {-1, -1}};
+  static size_t configured_smem[2][2] = {{0, 0}, {0, 0}};
+  int& cd = configured_dev[DIFF][sizeof(T) == 8];
+  size_t& cs = configured_smem[DIFF][sizeof(T) == 8];
+  if (cd != ctx->device || cs < smem) {
+    CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cd = ctx->device;
+    cs = smem;
+  }
+  int per_sm = 0;
+  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SPMV_THREADS, smem));
+  if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "block rows too long for the tiled SpMV");
+  const i64 ntiles = (m->nnodes + TILE_ROWS - 1) / TILE_ROWS;
+  const int grid = (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)per_sm * ctx->num_sms));
+  launch_pdl_cfg(ctx, kern, grid, SPMV_THREADS, smem, m->row_ptr, m->col_idx, val, m->nnodes, cap, nstage, p, ap,
+                 w->st.p, w->partials.p);
+}
+
+bool use_tiled_spmv() {
+  static int v = [] {
+    const char* e = getenv("FCU_TILED_SPMV");
+    return e ? atoi(e) : 1;
+  }();
+  return v != 0;
+}
+
+// Dispatch a node-row kernel: KERNEL(BS, VPR) names the instantiation.
+#define DISPATCH_ROWS(BS_, VPR_, GRID, KERNEL, ...)                           \
+  do {                                                                        \
+    if ((BS_) == 3) launch_pdl(ctx, KERNEL(3, 16), GRID, __VA_ARGS__);        \
+    else if ((VPR_) == 4) launch_pdl(ctx, KERNEL(1, 4), GRID, __VA_ARGS__);   \
+    else if ((VPR_) == 8) launch_pdl(ctx, KERNEL(1, 8), GRID, __VA_ARGS__);   \
+    else if ((VPR_) == 16) launch_pdl(ctx, KERNEL(1, 16), GRID, __VA_ARGS__); \
+    else launch_pdl(ctx, KERNEL(1, 32), GRID, __VA_ARGS__);                   \
   } while (0)
 
-#define DISPATCH_AP(T, BS_, VPR_, GRID, ...)                                                 \
-  do {                                                                                       \
-    if ((BS_) == 3) k_spmv_ap<3, 16, T><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__);      \
-    else if ((VPR_) == 4) k_spmv_ap<1, 4, T><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__); \
-    else if ((VPR_) == 8) k_spmv_ap<1, 8, T><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__); \
-    else if ((VPR_) == 16) k_spmv_ap<1, 16, T><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__); \
-    else k_spmv_ap<1, 32, T><<<GRID, VBLOCK, 0, ctx->stream>>>(__VA_ARGS__);                 \
-    LAUNCH_CHECK(ctx);                                                                       \
-  } while (0)
+#define K_SPMV_AP64(B, V) k_spmv_ap<B, V, double>
+#define K_SPMV_AP32(B, V) k_spmv_ap<B, V, float>
+#define K_SPMV_DIR64(B, V) k_spmv_dir<B, V, double>
+#define K_SPMV_DIR32(B, V) k_spmv_dir<B, V, float>
+#define K_INIT64(B, V) k_init_residual<B, V, double>
+#define K_INIT32(B, V) k_init_residual<B, V, float>
+#define K_REPLACE(B, V) k_mx_replace<B, V>
+#define K_PLAIN(B, V) k_spmv_plain<B, V>
 
-void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed) {
+// Fuse the direction update into the SpMV (1) or run it as its own kernel
+// (0); FCU_FUSE_DIRECTION overrides the default.
+bool fuse_direction() {
+  static int v = [] {
+    const char* e = getenv("FCU_FUSE_DIRECTION");
+    return e ? atoi(e) : 0;
+  }();
+  return v != 0;
+}
+
+// One PCG iteration; `parity` selects which p buffer is old / new.
+void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
   fcu_ctx ctx = m->ctx;
   const int g = w->grid;
   const i64 n = m->n, nr = m->nnodes;
+  if (!fuse_direction()) {
+    // direction (p = z + beta p, in place on buffer a) then SpMV
+    if (!mixed) {
+      launch_pdl(ctx, k_direction<double>, g, n, w->pa64.p, w->z64.p, w->st.p);
+      if (m->bs == 3 && use_tiled_spmv())
+        launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+      else
+        DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, nr, w->pa64.p, w->ap64.p,
+                      w->st.p, w->partials.p);
+      launch_pdl(ctx, k_update<double>, g, n, w->x.p, w->r.p, w->pa64.p, w->ap64.p, w->invd.p, w->z64.p, w->st.p,
+                 w->partials.p);
+    } else {
+      launch_pdl(ctx, k_direction<float>, g, n, w->pa32.p, w->z32.p, w->st.p);
+      if (m->bs == 3 && use_tiled_spmv())
+        launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+      else
+        DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, nr, w->pa32.p, w->ap32.p,
+                      w->st.p, w->partials.p);
+      launch_pdl(ctx, k_update<float>, g, n, w->x.p, w->r.p, w->pa32.p, w->ap32.p, w->invd.p, w->z32.p, w->st.p,
+                 w->partials.p);
+      DISPATCH_ROWS(m->bs, w->vpr, g, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
+                    w->r.p, w->z32.p, w->st.p, w->partials.p);
+    }
+    return;
+  }
   if (!mixed) {
-    DISPATCH_AP(double, m->bs, w->vpr, g, m->row_ptr, m->col_idx, m->val64.p, nr, w->p.p, w->ap.p, w->st.p,
-                w->partials.p);
-    k_cg_update<<<g, VBLOCK, 0, ctx->stream>>>(n, w->x.p, w->r.p, w->p.p, w->ap.p, w->invd.p, w->st.p, w->partials.p);
-    LAUNCH_CHECK(ctx);
-    k_cg_direction<double><<<g, VBLOCK, 0, ctx->stream>>>(n, w->p.p, w->r.p, w->invd.p, w->st.p);
-    LAUNCH_CHECK(ctx);
+    double* pold = parity ? w->pb64.p : w->pa64.p;
+    double* pnew = parity ? w->pa64.p : w->pb64.p;
+    DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_DIR64, m->row_ptr, m->col_idx, m->val64.p, nr, w->z64.p, pold, pnew,
+                  w->ap64.p, w->st.p, w->partials.p);
+    launch_pdl(ctx, k_update<double>, g, n, w->x.p, w->r.p, pnew, w->ap64.p, w->invd.p, w->z64.p, w->st.p,
+               w->partials.p);
   } else {
-    DISPATCH_AP(float, m->bs, w->vpr, g, m->row_ptr, m->col_idx, m->val32.p, nr, w->p32.p, w->ap32.p, w->st.p,
-                w->partials.p);
-    k_mx_update<<<g, VBLOCK, 0, ctx->stream>>>(n, w->x32.p, w->r32.p, w->p32.p, w->ap32.p, w->invd32.p, w->st.p,
-                                               w->partials.p);
-    LAUNCH_CHECK(ctx);
-    DISPATCH_ROWS(m->bs, w->vpr, k_mx_reliable, g, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->x32.p, w->b.p,
-                  w->r32.p, w->invd32.p, w->st.p, w->partials.p);
-    k_mx_direction<<<g, VBLOCK, 0, ctx->stream>>>(n, w->p32.p, w->r32.p, w->invd32.p, w->x.p, w->x32.p, w->st.p);
-    LAUNCH_CHECK(ctx);
+    float* pold = parity ? w->pb32.p : w->pa32.p;
+    float* pnew = parity ? w->pa32.p : w->pb32.p;
+    DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_DIR32, m->row_ptr, m->col_idx, m->val32.p, nr, w->z32.p, pold, pnew,
+                  w->ap32.p, w->st.p, w->partials.p);
+    launch_pdl(ctx, k_update<float>, g, n, w->x.p, w->r.p, pnew, w->ap32.p, w->invd.p, w->z32.p, w->st.p,
+               w->partials.p);
+    DISPATCH_ROWS(m->bs, w->vpr, g, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
+                  w->r.p, w->z32.p, w->st.p, w->partials.p);
   }
 }
+
+int launches_per_iteration(bool mixed) { return (mixed ? 3 : 2) + (fuse_direction() ? 0 : 1); }
 
 cudaGraphExec_t get_graph(fcu_matrix m, Workspace* w, bool mixed) {
   fcu_ctx ctx = m->ctx;
   cudaGraphExec_t& ge = w->graph[mixed ? 1 : 0];
   if (ge) return ge;
   cudaGraph_t g;
+  const i64 launches0 = ctx->launches;
   CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   try {
-    for (int it = 0; it < CHUNK; ++it) enqueue_iteration(m, w, mixed);
+    for (int it = 0; it < CHUNK; ++it) enqueue_iteration(m, w, mixed, it & 1);
   } catch (...) {
     cudaStreamEndCapture(ctx->stream, &g);
     throw;
@@ -552,31 +971,48 @@ cudaGraphExec_t get_graph(fcu_matrix m, Workspace* w, bool mixed) {
   CUDA_CHECK(cudaGraphInstantiate(&ge, g, 0));
   cudaGraphDestroy(g);
   // launches inside the graph are counted per replay in run_pcg
-  ctx->launches -= (i64)CHUNK * (mixed ? 4 : 3);
+  ctx->launches = launches0;
   return ge;
 }
 
 }  // namespace
 
-// Algorithmic bytes of one iteration (see DESIGN.md-free statement in bench):
-// matrix values + indices + row pointers, x gather + y write, and 11 vector
-// passes (x, p, r, Ap, D^-1 reads; x, r writes; r, D^-1, p reads + p write).
+// Algorithmic bytes of one PCG iteration (per launch pair):
+//   spmv:   matrix values + column indices + row pointers, z and p_old read
+//           once, p_new and Ap written once
+//   update: x, r read and written; p, Ap, D^-1 read; z written
+// FP64: 8-byte values and vectors. Mixed: 4-byte values, p, Ap, z; x, r and
+// D^-1 stay 8-byte.
 double pcg_bytes_per_iter(fcu_matrix m, bool mixed) {
-  const double w = mixed ? 4.0 : 8.0;
   const double bs2 = (double)m->bs * m->bs;
+  const double n = (double)m->n;
+  const double w = mixed ? 4.0 : 8.0;
   const double mat = (double)m->nnzb * (bs2 * w + 4.0) + 4.0 * (double)(m->nnodes + 1);
-  return mat + 2.0 * m->n * w + 11.0 * m->n * w;
+  const double spmv_vec = 4.0 * n * w;
+  const double update = n * (8 + 8 + 8 + 8) + n * (w + w + 8) + n * w;
+  return mat + spmv_vec + update;
 }
 
-void ensure_inv_diag(fcu_matrix m) {
-  Workspace* w = ensure_ws(m, false);
+void ensure_inv_diag(fcu_matrix m, Workspace* w) {
   fcu_ctx ctx = m->ctx;
   if (m->bs == 3)
     k_inv_diag<3><<<grid_for(m->n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(m->diag_pos, m->val64.p, m->nnodes,
-                                                                                  w->invd.p, w->invd32.p);
+                                                                                  w->invd.p);
   else
     k_inv_diag<1><<<grid_for(m->n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(m->diag_pos, m->val64.p, m->nnodes,
-                                                                                  w->invd.p, w->invd32.p);
+                                                                                  w->invd.p);
+  LAUNCH_CHECK(ctx);
+}
+
+void build_rowsum32(fcu_matrix m) {
+  fcu_ctx ctx = m->ctx;
+  const i64 t = m->nnodes * m->bs * m->bs;
+  if (m->bs == 3)
+    k_build_rowsum32<3><<<grid_for(t, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(m->row_ptr, m->diag_pos,
+                                                                                     m->val64.p, m->nnodes, m->val32.p);
+  else
+    k_build_rowsum32<1><<<grid_for(t, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(m->row_ptr, m->diag_pos,
+                                                                                     m->val64.p, m->nnodes, m->val32.p);
   LAUNCH_CHECK(ctx);
 }
 
@@ -586,40 +1022,40 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
             int precision, bool gpu_semantics, const double* inv_diag_dev, fcu_solve_info* info) {
   fcu_ctx ctx = m->ctx;
   const bool mixed = precision == FCU_MIXED;
+  if (mixed && !m->val32.p) fail(FCU_ERR_BAD_ARG, "matrix has no FP32 copy");
   Workspace* w = ensure_ws(m, mixed);
   const i64 n = m->n, nr = m->nnodes;
   const int g = w->grid;
-  if (inv_diag_dev) {
-    CUDA_CHECK(cudaMemcpyAsync(w->invd.p, inv_diag_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    // FP32 copy (mixed path) from the FP64 one
-    if (mixed) fail(FCU_ERR_BAD_ARG, "caller-supplied inverse diagonal is FP64-only");
-  } else {
-    ensure_inv_diag(m);
-  }
   cudaEvent_t e0, e1;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
   CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+  if (inv_diag_dev) CUDA_CHECK(cudaMemcpyAsync(w->invd.p, inv_diag_dev, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                               ctx->stream));
+  else ensure_inv_diag(m, w);
+  if (mixed) build_rowsum32(m);
 
   CgState init{};
   init.tol = tol;
   init.max_iter = max_iter;
   init.gpu_semantics = gpu_semantics ? 1 : 0;
   init.delta = 0.1;
-  CUDA_CHECK(cudaMemcpyAsync(w->st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
+  *w->host_st = init;
+  CUDA_CHECK(cudaMemcpyAsync(w->st.p, w->host_st, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
   CUDA_CHECK(cudaMemcpyAsync(w->b.p, b_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   if (x0_dev) CUDA_CHECK(cudaMemcpyAsync(w->x.p, x0_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   else CUDA_CHECK(cudaMemsetAsync(w->x.p, 0, n * sizeof(double), ctx->stream));
-  if (mixed) CUDA_CHECK(cudaMemsetAsync(w->x32.p, 0, n * sizeof(float), ctx->stream));
-  // r = b - A x0 ; bnorm ; initial test
-  DISPATCH_ROWS(m->bs, w->vpr, k_init_residual, g, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->r.p, n,
-                w->st.p, w->partials.p);
-  k_init_direction<<<g, VBLOCK, 0, ctx->stream>>>(n, w->r.p, w->invd.p, w->p.p, mixed ? w->r32.p : nullptr,
-                                                  w->invd32.p, mixed ? w->p32.p : nullptr, w->st.p, w->partials.p);
-  LAUNCH_CHECK(ctx);
+  // r = b - A x0 ; z = D^-1 r ; ||b|| ; r.z ; p_old = 0 ; initial test (cg.rs:79-90)
+  if (mixed)
+    DISPATCH_ROWS(m->bs, w->vpr, g, K_INIT32, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
+                  w->r.p, w->z32.p, w->pa32.p, n, w->st.p, w->partials.p);
+  else
+    DISPATCH_ROWS(m->bs, w->vpr, g, K_INIT64, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
+                  w->r.p, w->z64.p, w->pa64.p, n, w->st.p, w->partials.p);
   CUDA_CHECK(cudaMemcpyAsync(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-  if (gpu_semantics && w->host_st->bnorm == 0.0) {
+  bool zero_rhs = gpu_semantics && w->host_st->bnorm == 0.0;
+  if (zero_rhs) {
     // gpu.rs:1169-1180: zero right-hand side -> zero solution, Ok
     CUDA_CHECK(cudaMemsetAsync(x_dev, 0, n * sizeof(double), ctx->stream));
     w->host_st->done = 1;
@@ -627,10 +1063,9 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
     w->host_st->iter = 0;
   } else if (!w->host_st->done && max_iter > 0) {
     cudaGraphExec_t ge = get_graph(m, w, mixed);
-    const int per = mixed ? 4 : 3;
     for (i64 launched = 0; launched < max_iter + CHUNK; launched += CHUNK) {
       CUDA_CHECK(cudaGraphLaunch(ge, ctx->stream));
-      ctx->launches += (i64)CHUNK * per;
+      ctx->launches += (i64)CHUNK * launches_per_iteration(mixed);
       CUDA_CHECK(cudaMemcpyAsync(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
       if (w->host_st->done) break;
@@ -638,12 +1073,7 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
   } else if (!w->host_st->done) {
     w->host_st->status = gpu_semantics ? FCU_OK : FCU_ERR_NO_CONVERGENCE;
   }
-  if (mixed) {
-    k_fold<<<g, VBLOCK, 0, ctx->stream>>>(n, w->x.p, w->x32.p);
-    LAUNCH_CHECK(ctx);
-  }
-  if (!(gpu_semantics && w->host_st->bnorm == 0.0))
-    CUDA_CHECK(cudaMemcpyAsync(x_dev, w->x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (!zero_rhs) CUDA_CHECK(cudaMemcpyAsync(x_dev, w->x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
   CUDA_CHECK(cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -668,7 +1098,7 @@ void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev) {
   fcu_ctx ctx = m->ctx;
   const int vpr = pick_vpr(m);
   const int g = solver_grid(ctx, m->n);
-  DISPATCH_ROWS(m->bs, vpr, k_spmv_plain, g, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, x_dev, y_dev);
+  DISPATCH_ROWS(m->bs, vpr, g, K_PLAIN, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, x_dev, y_dev);
 }
 
 // Average time of the PCG SpMV kernel over `reps` launches (diagnostics).
@@ -676,24 +1106,39 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
   fcu_ctx ctx = m->ctx;
   const bool mixed = precision == FCU_MIXED;
   Workspace* w = ensure_ws(m, mixed);
-  const i64 nr = m->nnodes;
-  const int g = w->grid;
+  if (mixed) build_rowsum32(m);
   CgState init{};
   init.rz = 1.0;
-  CUDA_CHECK(cudaMemcpyAsync(w->st.p, &init, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
-  if (mixed) CUDA_CHECK(cudaMemsetAsync(w->p32.p, 0, m->n * sizeof(float), ctx->stream));
-  else CUDA_CHECK(cudaMemsetAsync(w->p.p, 0, m->n * sizeof(double), ctx->stream));
+  init.beta = 0.5;
+  init.gpu_semantics = 1;  // no breakdown exit: every launch does the full product
+  *w->host_st = init;
+  CUDA_CHECK(cudaMemcpyAsync(w->st.p, w->host_st, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
+  const i64 n = m->n;
+  // any non-zero vectors (1/64 in every entry)
+  if (mixed) {
+    CUDA_CHECK(cudaMemsetAsync(w->z32.p, 0x3c, n * sizeof(float), ctx->stream));
+    CUDA_CHECK(cudaMemsetAsync(w->pa32.p, 0x3c, n * sizeof(float), ctx->stream));
+  } else {
+    CUDA_CHECK(cudaMemsetAsync(w->z64.p, 0x3f, n * sizeof(double), ctx->stream));
+    CUDA_CHECK(cudaMemsetAsync(w->pa64.p, 0x3f, n * sizeof(double), ctx->stream));
+  }
+  const int g = w->grid;
   cudaEvent_t e0, e1;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
   CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
   for (int r = 0; r < reps; ++r) {
-    if (mixed)
-      DISPATCH_AP(float, m->bs, w->vpr, g, m->row_ptr, m->col_idx, m->val32.p, nr, w->p32.p, w->ap32.p, w->st.p,
-                  w->partials.p);
-    else
-      DISPATCH_AP(double, m->bs, w->vpr, g, m->row_ptr, m->col_idx, m->val64.p, nr, w->p.p, w->ap.p, w->st.p,
-                  w->partials.p);
+    if (mixed) {
+      if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+      else
+        DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, m->nnodes, w->pa32.p,
+                      w->ap32.p, w->st.p, w->partials.p);
+    } else {
+      if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+      else
+        DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->pa64.p,
+                      w->ap64.p, w->st.p, w->partials.p);
+    }
   }
   CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
   CUDA_CHECK(cudaEventSynchronize(e1));
@@ -702,7 +1147,7 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *ms = reps > 0 ? (double)t / reps : 0.0;
-  const double wv = mixed ? 4.0 : 8.0;
   const double bs2 = (double)m->bs * m->bs;
-  *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
+  const double wv = mixed ? 4.0 : 8.0;
+  *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)n * wv;
 }

@@ -425,9 +425,11 @@ def test_cantilever_bending_device(fcu, ctx):
     om = O.box_beam(1.0, 0.1, 0.1, 20, 3, 3)
     dofs = O.clamp_dofs(om)
     bc = fcu.VectorDirichletBC([(int(d), 0.0) for d in dofs])
-    for prec in (fcu.FCU_FP64, fcu.FCU_MIXED):
+    # The FP32 inner iteration converges more slowly on this ill-conditioned
+    # beam, so the mixed solve gets a larger iteration budget.
+    for prec, budget in ((fcu.FCU_FP64, 2000), (fcu.FCU_MIXED, 20000)):
         sol = fcu.solve_elasticity_3d(_fmesh(fcu, om), fcu.ElasticMaterial(1e6, 0.3), [0.0, 0.0, -1000.0], bc,
-                                      1e-9, 2000, ctx, precision=prec)
+                                      1e-9, budget, ctx, precision=prec)
         tip = np.abs(om.coords[:, 0] - 1.0) < 1e-6
         uz = sol.displacements[3 * np.nonzero(tip)[0] + 2].mean()
         assert abs(uz - (-0.0890)) / 0.0890 < 0.06
