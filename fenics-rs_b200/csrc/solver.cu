@@ -740,8 +740,10 @@ struct Workspace {
   DBuf<CgState> st;
   CgState* host_st = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  int vpr = 0;  // chosen lanes per row (CSR)
-  int grid = 0;
+  int vpr = 0;    // chosen lanes per row (CSR)
+  int grid = 0;   // row kernels
+  int vgrid = 0;  // element-wise vector kernels
+  int rgrid = 0;  // residual replacement (rarely does work; small grid keeps its no-op cheap)
   ~Workspace() {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
@@ -770,6 +772,17 @@ int solver_grid(fcu_ctx ctx, i64 n) {
   return (int)std::max<i64>(1, std::min(want, cap));
 }
 
+// Blocks per SM for the element-wise vector kernels (update, direction);
+// FCU_VEC_BPSM overrides the default.
+int vec_blocks_per_sm() {
+  static int v = [] {
+    const char* e = getenv("FCU_VEC_BPSM");
+    int x = e ? atoi(e) : 8;
+    return (x >= 1 && x <= 16) ? x : 8;
+  }();
+  return v;
+}
+
 int pick_vpr(fcu_matrix m) {
   if (m->bs == 3) return 16;
   double avg = m->nnodes ? (double)m->nnzb / (double)m->nnodes : 1.0;
@@ -793,6 +806,8 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     CUDA_CHECK(cudaMallocHost(&w->host_st, sizeof(CgState)));
     w->vpr = pick_vpr(m);
     w->grid = solver_grid(ctx, n);
+    w->vgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms * vec_blocks_per_sm()));
+    w->rgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms));
   }
   Workspace* w = m->ws;
   if (!mixed && !w->z64.p) {
@@ -911,25 +926,25 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
   if (!fuse_direction()) {
     // direction (p = z + beta p, in place on buffer a) then SpMV
     if (!mixed) {
-      launch_pdl(ctx, k_direction<double>, g, n, w->pa64.p, w->z64.p, w->st.p);
+      launch_pdl(ctx, k_direction<double>, w->vgrid, n, w->pa64.p, w->z64.p, w->st.p);
       if (m->bs == 3 && use_tiled_spmv())
         launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
       else
         DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, nr, w->pa64.p, w->ap64.p,
                       w->st.p, w->partials.p);
-      launch_pdl(ctx, k_update<double>, g, n, w->x.p, w->r.p, w->pa64.p, w->ap64.p, w->invd.p, w->z64.p, w->st.p,
-                 w->partials.p);
+      launch_pdl(ctx, k_update<double>, w->vgrid, n, w->x.p, w->r.p, w->pa64.p, w->ap64.p, w->invd.p, w->z64.p,
+                 w->st.p, w->partials.p);
     } else {
-      launch_pdl(ctx, k_direction<float>, g, n, w->pa32.p, w->z32.p, w->st.p);
+      launch_pdl(ctx, k_direction<float>, w->vgrid, n, w->pa32.p, w->z32.p, w->st.p);
       if (m->bs == 3 && use_tiled_spmv())
         launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
       else
         DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, nr, w->pa32.p, w->ap32.p,
                       w->st.p, w->partials.p);
-      launch_pdl(ctx, k_update<float>, g, n, w->x.p, w->r.p, w->pa32.p, w->ap32.p, w->invd.p, w->z32.p, w->st.p,
-                 w->partials.p);
-      DISPATCH_ROWS(m->bs, w->vpr, g, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
-                    w->r.p, w->z32.p, w->st.p, w->partials.p);
+      launch_pdl(ctx, k_update<float>, w->vgrid, n, w->x.p, w->r.p, w->pa32.p, w->ap32.p, w->invd.p, w->z32.p,
+                 w->st.p, w->partials.p);
+      DISPATCH_ROWS(m->bs, w->vpr, w->rgrid, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p,
+                    w->invd.p, w->r.p, w->z32.p, w->st.p, w->partials.p);
     }
     return;
   }
@@ -1151,3 +1166,4 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
   const double wv = mixed ? 4.0 : 8.0;
   *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)n * wv;
 }
+
