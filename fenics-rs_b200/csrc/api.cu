@@ -26,6 +26,9 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
             int precision, bool gpu_semantics, const double* inv_diag_dev, fcu_solve_info* info);
 void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev);
 void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes);
+int run_pcg_noalloc(i64 n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
+                    const double* inv_diag, const double* b, const double* x0, double rtol, i64 max_iter, double* x,
+                    fcu_solve_info* info, void* stream);
 
 namespace {
 
@@ -872,6 +875,18 @@ int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint
     status = run_pcg(m.get(), bd.p, x0d.p, xo.p, rtol, max_iter, FCU_FP64, true, idd.p, info);
     xo.finish(ctx);
     sync(ctx);
+  });
+  return rc != FCU_OK ? rc : status;
+}
+
+// Allocation-free variant of fcu_solve_csr_cg for callers that cannot
+// allocate device memory at solve time; errors go to fcu_last_error(NULL).
+int fcu_solve_csr_cg_noalloc(int64_t n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
+                             const double* inv_diag, const double* b, const double* x0, double rtol,
+                             int64_t max_iter, double* x, fcu_solve_info* info, void* stream) {
+  int status = FCU_OK;
+  int rc = guarded(nullptr, [&] {
+    status = run_pcg_noalloc(n, row_ptr, col_idx, vals, inv_diag, b, x0, rtol, max_iter, x, info, stream);
   });
   return rc != FCU_OK ? rc : status;
 }

@@ -32,8 +32,11 @@
 // polls the state once per chunk.
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <string>
 
 #include "internal.cuh"
 
@@ -1167,3 +1170,236 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
   *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)n * wv;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free CSR PCG (fcu_solve_csr_cg_noalloc).
+//
+// Some callers cannot allocate device memory when they solve. One example is
+// an application whose own pool allocator reserves the device's memory up
+// front and leaves nothing for a library to cudaMalloc. Another is a
+// time-stepping loop that solves many small systems: cudaMalloc and cudaFree
+// synchronise the whole device, which would stall that application's other
+// streams every step. For them this variant runs the same kernels as
+// fcu_solve_csr_cg (FP64, gpu.rs semantics) but keeps all its work vectors,
+// reduction partials and solver state in one fixed module-scope device
+// array. A call allocates no device memory: no cudaMalloc, cudaMallocHost or
+// cudaFree, no graph instantiation, no library routine that allocates.
+//
+// Limits and rules:
+//  - at most NOALLOC_MAX_N rows (the array holds four vectors of that
+//    length, about 4 MiB in all);
+//  - every array argument is device memory of the current device (nothing
+//    is staged, since staging would allocate);
+//  - the array is shared by all calls on a device, so calls that overlap in
+//    time on one device (from several host threads) race and corrupt each
+//    other's results. Callers must not overlap them;
+//  - the first call on a device looks up the array's device address with
+//    cudaGetSymbolAddress, which may load this module onto that device. Make
+//    that first call before any stream capture begins on the device;
+//  - the solver state (grid-reduction arrival counters included) must start
+//    at zero. Each call writes a fresh state block over the array's header
+//    on the caller's stream before its first kernel. The vectors need no
+//    initial value: the initial residual kernel writes r, z and p before
+//    anything reads them.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr i64 NOALLOC_MAX_N = 131072;
+
+struct NoAllocHeader {
+  CgState st;
+  int bad;  // set by the index check
+};
+static_assert(sizeof(NoAllocHeader) <= 1024, "header region");
+
+constexpr size_t NA_HEADER_WORDS = 1024 / sizeof(double);
+constexpr size_t NA_PARTIAL_WORDS = 3 * MAXG;
+constexpr size_t NA_VEC_WORDS = (size_t)NOALLOC_MAX_N;
+constexpr size_t NA_WORDS = NA_HEADER_WORDS + NA_PARTIAL_WORDS + 4 * NA_VEC_WORDS;
+
+}  // namespace
+
+// The scratch array. On the host this name only stands for the symbol; its
+// device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) double g_noalloc_scratch[NA_WORDS];
+
+namespace {
+
+constexpr int NA_MAX_DEVICES = 64;
+std::atomic<double*> g_noalloc_addr[NA_MAX_DEVICES];
+
+// Device address of the scratch array on the current device (looked up on
+// the first call per device; the lookup is idempotent, so concurrent first
+// calls agree).
+double* noalloc_scratch(int dev) {
+  if (dev < 0 || dev >= NA_MAX_DEVICES) fail(FCU_ERR_UNSUPPORTED, "device ordinal too large for the no-alloc solver");
+  double* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (p) return p;
+  void* a = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+  if (e != cudaSuccess) fail(FCU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  if (!a) fail(FCU_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+  p = static_cast<double*>(a);
+  g_noalloc_addr[dev].store(p, std::memory_order_release);
+  return p;
+}
+
+// Same acceptance rule as the u32 -> i32 conversion of fcu_solve_csr_cg:
+// row pointers at most nnz, column indices below n.
+__global__ void k_noalloc_check(const uint32_t* __restrict__ rp, i64 n, const uint32_t* __restrict__ ci, i64 nnz,
+                                int* __restrict__ bad) {
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t <= n; t += stride)
+    if ((i64)rp[t] > nnz) atomicExch(bad, 1);
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nnz; t += stride)
+    if ((i64)ci[t] >= n) atomicExch(bad, 1);
+}
+
+void require_device_ptr(const void* p, int dev, const char* what) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    fail(FCU_ERR_BAD_ARG, std::string(what) + ": not a device pointer (the no-alloc solver stages nothing)");
+  }
+  const bool dev_mem = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (!dev_mem) fail(FCU_ERR_BAD_ARG, std::string(what) + ": not a device pointer (the no-alloc solver stages nothing)");
+  if (a.type == cudaMemoryTypeDevice && a.device != dev)
+    fail(FCU_ERR_BAD_ARG, std::string(what) + ": memory of another device");
+}
+
+template <int VPR>
+void noalloc_chunk(cudaStream_t s, int g, int vg, const int* rp, const int* ci, const double* val, i64 n, double* x,
+                   double* r, double* z, double* p, double* ap, const double* invd, CgState* st, double* partials) {
+  for (int it = 0; it < CHUNK; ++it) {
+    k_direction<double><<<vg, VBLOCK, 0, s>>>(n, p, z, st);
+    k_spmv_ap<1, VPR, double><<<g, VBLOCK, 0, s>>>(rp, ci, val, n, p, ap, st, partials);
+    k_update<double><<<vg, VBLOCK, 0, s>>>(n, x, r, p, ap, invd, z, st, partials);
+  }
+  CUDA_CHECK(cudaGetLastError());
+}
+
+template <int VPR>
+void noalloc_init(cudaStream_t s, int g, const int* rp, const int* ci, const double* val, i64 n, const double* x,
+                  const double* b, const double* invd, double* r, double* z, double* p, CgState* st,
+                  double* partials) {
+  k_init_residual<1, VPR, double><<<g, VBLOCK, 0, s>>>(rp, ci, val, n, x, b, invd, r, z, p, n, st, partials);
+  CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace
+
+int run_pcg_noalloc(i64 n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
+                    const double* inv_diag, const double* b, const double* x0, double rtol, i64 max_iter, double* x,
+                    fcu_solve_info* info, void* stream) {
+  const auto t0 = std::chrono::steady_clock::now();
+  if (n <= 0) fail(FCU_ERR_BAD_ARG, "n must be positive");
+  if (n > NOALLOC_MAX_N)
+    fail(FCU_ERR_BAD_ARG, "n = " + std::to_string(n) + " exceeds the no-alloc solver's capacity of " +
+                              std::to_string(NOALLOC_MAX_N) + " rows");
+  if (max_iter < 0) fail(FCU_ERR_BAD_ARG, "max_iter must be non-negative");
+  if (!row_ptr || !inv_diag || !b || !x) fail(FCU_ERR_BAD_ARG, "null CSR argument");
+  int dev = 0;
+  CUDA_CHECK(cudaGetDevice(&dev));
+  require_device_ptr(row_ptr, dev, "row_ptr");
+  require_device_ptr(inv_diag, dev, "inv_diag");
+  require_device_ptr(b, dev, "b");
+  require_device_ptr(x, dev, "x");
+  if (x0) require_device_ptr(x0, dev, "x0");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  uint32_t nnz32 = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&nnz32, row_ptr + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CUDA_CHECK(cudaStreamSynchronize(s));
+  const i64 nnz = nnz32;
+  if (nnz >= (1ll << 31)) fail(FCU_ERR_UNSUPPORTED, "nnz exceeds 32-bit indexing");
+  if (nnz > 0) {
+    if (!col_idx || !vals) fail(FCU_ERR_BAD_ARG, "null CSR arrays");
+    require_device_ptr(col_idx, dev, "col_idx");
+    require_device_ptr(vals, dev, "vals");
+  }
+
+  double* base = noalloc_scratch(dev);
+  NoAllocHeader* hdr = reinterpret_cast<NoAllocHeader*>(base);
+  double* partials = base + NA_HEADER_WORDS;
+  double* r = partials + NA_PARTIAL_WORDS;
+  double* z = r + NA_VEC_WORDS;
+  double* p = z + NA_VEC_WORDS;
+  double* ap = p + NA_VEC_WORDS;
+
+  NoAllocHeader init{};
+  init.st.tol = rtol;
+  init.st.max_iter = max_iter;
+  init.st.gpu_semantics = 1;
+  init.st.delta = 0.1;
+  CUDA_CHECK(cudaMemcpyAsync(hdr, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+
+  int num_sms = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  const i64 want = (n + VBLOCK - 1) / VBLOCK;
+  const int g = (int)std::max<i64>(1, std::min<i64>(want, (i64)num_sms * blocks_per_sm()));
+  const int vg = (int)std::max<i64>(1, std::min<i64>(want, (i64)num_sms * vec_blocks_per_sm()));
+  if (g > MAXG || vg > MAXG) fail(FCU_ERR_UNSUPPORTED, "grid exceeds the reduction capacity");
+
+  const int check_grid = (int)std::max<i64>(1, std::min<i64>((std::max(n + 1, nnz) + 255) / 256, (i64)num_sms * 8));
+  k_noalloc_check<<<check_grid, 256, 0, s>>>(row_ptr, n, col_idx, nnz, &hdr->bad);
+  CUDA_CHECK(cudaGetLastError());
+  int bad = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&bad, &hdr->bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_CHECK(cudaStreamSynchronize(s));
+  if (bad) fail(FCU_ERR_BAD_ARG, "CSR index out of range");
+  // Every index is now known to be below 2^31, so the u32 arrays read as i32.
+  const int* rp = reinterpret_cast<const int*>(row_ptr);
+  const int* ci = reinterpret_cast<const int*>(col_idx);
+
+  // CSR lanes per row by average row length (as for library matrices).
+  const double avg = (double)nnz / (double)n;
+  const int vpr = avg <= 6 ? 4 : avg <= 14 ? 8 : avg <= 40 ? 16 : 32;
+
+  if (x0 && x0 != x) CUDA_CHECK(cudaMemcpyAsync(x, x0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  else if (!x0) CUDA_CHECK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+  CgState* st = &hdr->st;
+  switch (vpr) {
+    case 4: noalloc_init<4>(s, g, rp, ci, vals, n, x, b, inv_diag, r, z, p, st, partials); break;
+    case 8: noalloc_init<8>(s, g, rp, ci, vals, n, x, b, inv_diag, r, z, p, st, partials); break;
+    case 16: noalloc_init<16>(s, g, rp, ci, vals, n, x, b, inv_diag, r, z, p, st, partials); break;
+    default: noalloc_init<32>(s, g, rp, ci, vals, n, x, b, inv_diag, r, z, p, st, partials); break;
+  }
+  CgState hs{};
+  CUDA_CHECK(cudaMemcpyAsync(&hs, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+  CUDA_CHECK(cudaStreamSynchronize(s));
+  const bool zero_rhs = hs.bnorm == 0.0;
+  if (zero_rhs) {
+    // gpu.rs:1169-1180: zero right-hand side -> zero solution, Ok
+    CUDA_CHECK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    hs.done = 1;
+    hs.status = FCU_OK;
+    hs.iter = 0;
+  } else if (!hs.done && max_iter > 0) {
+    for (i64 launched = 0; launched < max_iter + CHUNK; launched += CHUNK) {
+      switch (vpr) {
+        case 4: noalloc_chunk<4>(s, g, vg, rp, ci, vals, n, x, r, z, p, ap, inv_diag, st, partials); break;
+        case 8: noalloc_chunk<8>(s, g, vg, rp, ci, vals, n, x, r, z, p, ap, inv_diag, st, partials); break;
+        case 16: noalloc_chunk<16>(s, g, vg, rp, ci, vals, n, x, r, z, p, ap, inv_diag, st, partials); break;
+        default: noalloc_chunk<32>(s, g, vg, rp, ci, vals, n, x, r, z, p, ap, inv_diag, st, partials); break;
+      }
+      CUDA_CHECK(cudaMemcpyAsync(&hs, st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+      CUDA_CHECK(cudaStreamSynchronize(s));
+      if (hs.done) break;
+    }
+  } else if (!hs.done) {
+    hs.status = FCU_OK;  // zero iterations allowed: Ok at the limit (gpu.rs semantics)
+  }
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (info) {
+    info->iterations = hs.iter;
+    info->outer_updates = hs.updates;
+    info->residual = std::sqrt(std::max(hs.rr, 0.0));
+    info->rel_residual = hs.bnorm > 0.0 ? info->residual / hs.bnorm : info->residual;
+    info->kernel_ms = ms;
+    // same algorithmic count as the library solver: matrix + SpMV vectors + update vectors
+    const double bytes_iter = (double)nnz * 12.0 + 4.0 * (double)(n + 1) + 4.0 * n * 8.0 + 64.0 * n;
+    info->effective_bw_gbps = ms > 0 ? bytes_iter * (double)hs.iter / (ms * 1e-3) / 1e9 : 0.0;
+    info->status = hs.done ? hs.status : FCU_OK;
+  }
+  return hs.done ? hs.status : FCU_OK;
+}

@@ -18,6 +18,8 @@ FCU_ERR_NO_CONVERGENCE = 3
 FCU_ERR_BREAKDOWN = 4
 FCU_ERR_UNSUPPORTED = 5
 
+FCU_NOALLOC_MAX_N = 131072  # row capacity of fcu_solve_csr_cg_noalloc
+
 FCU_SPACE_P1 = 1
 FCU_SPACE_P2 = 2
 FCU_SPACE_P1_VEC3 = 3
@@ -80,6 +82,7 @@ SIGNATURES = {
     "fcu_assemble_surface_traction": (cint, [vp, vp, i64, vp, vp, vp]),
     "fcu_pcg": (cint, [vp, vp, vp, vp, vp, dbl, i64, cint, C.POINTER(SolveInfo)]),
     "fcu_solve_csr_cg": (cint, [vp, i64, vp, vp, vp, vp, vp, vp, dbl, i64, vp, C.POINTER(SolveInfo)]),
+    "fcu_solve_csr_cg_noalloc": (cint, [i64, vp, vp, vp, vp, vp, vp, dbl, i64, vp, C.POINTER(SolveInfo), vp]),
     "fcu_spmv": (cint, [vp, vp, vp, vp]),
     "fcu_adjoint_gradient": (cint, [vp, vp, dbl, dbl, vp, vp, vp, vp]),
     "fcu_time_spmv": (cint, [vp, vp, cint, cint, C.POINTER(dbl), C.POINTER(dbl)]),

@@ -176,6 +176,31 @@ int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint
                      const double* vals, const double* inv_diag, const double* b, const double* x0,
                      double rtol, int64_t max_iter, double* x, fcu_solve_info* info);
 
+/* Allocation-free variant of fcu_solve_csr_cg. No counterpart in the
+ * reference: it serves callers that cannot allocate device memory when they
+ * solve (an application whose pool allocator owns the device's memory, or a
+ * time-stepping loop where cudaMalloc/cudaFree would synchronise the device).
+ * It takes no context and allocates nothing: its work vectors and state live
+ * in one fixed module-scope device array.
+ *  - n <= FCU_NOALLOC_MAX_N, else FCU_ERR_BAD_ARG;
+ *  - every array is device memory of the calling thread's current device
+ *    (host pointers are rejected with FCU_ERR_BAD_ARG; nothing is staged);
+ *    x is used as the iterate in place and may equal x0;
+ *  - runs on `stream` (a cudaStream_t; NULL = legacy default stream) and
+ *    synchronises it before returning;
+ *  - the array is shared by every call on a device: calls that overlap in
+ *    time on one device race. Callers must not overlap them;
+ *  - the first call on a device looks up the array's address (and may load
+ *    the module there); make it before any stream capture begins;
+ *  - each call resets the solver state itself (it must start at zero);
+ *  - info->kernel_ms is the host wall time of the call;
+ *  - errors: fcu_last_error(NULL). Results and semantics as fcu_solve_csr_cg. */
+#define FCU_NOALLOC_MAX_N 131072
+int fcu_solve_csr_cg_noalloc(int64_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
+                             const double* vals, const double* inv_diag, const double* b,
+                             const double* x0, double rtol, int64_t max_iter, double* x,
+                             fcu_solve_info* info, void* stream);
+
 /* y = A x (cg.rs:7-23) with the FP64 values. */
 int fcu_spmv(fcu_ctx ctx, fcu_matrix m, const double* x, double* y);
 
