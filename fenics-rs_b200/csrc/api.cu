@@ -8,6 +8,8 @@
 #include <cstring>
 #include <memory>
 
+#include <vector>
+
 #include "internal.cuh"
 
 // implemented in assemble.cu / rhs.cu / solver.cu
@@ -26,6 +28,10 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
             int precision, bool gpu_semantics, const double* inv_diag_dev, fcu_solve_info* info);
 void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev);
 void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes);
+int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
+                   i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
+                   fcu_solve_info* info);
+void batch_config(fcu_matrix m, int precision, int* vpr, int* threads);
 int run_pcg_noalloc(i64 n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
                     const double* inv_diag, const double* b, const double* x0, double rtol, i64 max_iter, double* x,
                     fcu_solve_info* info, void* stream);
@@ -831,6 +837,38 @@ int fcu_pcg(fcu_ctx ctx, fcu_matrix m, const double* b, const double* x0, double
   else if (status == FCU_ERR_BREAKDOWN)
     ctx->err = "Breakdown in CG: curvature p^T A p is near zero";
   return status;
+}
+
+int fcu_batch_pcg(fcu_ctx ctx, fcu_matrix m, int64_t nb, const int64_t* offsets, const double* b, double* x,
+                  double tol, int64_t max_iter, int precision, int64_t* iterations, double* rel_residual,
+                  int* status, fcu_solve_info* info) {
+  int st = FCU_OK;
+  int rc = guarded(ctx, [&] {
+    if (!m || !offsets || !b || !x) fail(FCU_ERR_BAD_ARG, "null argument");
+    if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
+    if (nb <= 0) fail(FCU_ERR_BAD_ARG, "need at least one instance");
+    std::vector<i64> offs(nb + 1);
+    if (is_device_ptr(offsets)) download(ctx, offs.data(), offsets, nb + 1);
+    else std::copy(offsets, offsets + nb + 1, offs.begin());
+    DevIn<double> bd(ctx, b, m->n);
+    DevOut<double> xo(x, m->n);
+    st = batch_pcg_impl(m, nb, offs.data(), bd.p, xo.p, tol, max_iter, precision, iterations, rel_residual, status,
+                        info);
+    xo.finish(ctx);
+    sync(ctx);
+  });
+  if (rc != FCU_OK) return rc;
+  if (st == FCU_ERR_NO_CONVERGENCE)
+    ctx->err = "CG failed to converge within " + std::to_string(max_iter) + " iterations for some instances";
+  else if (st == FCU_ERR_BREAKDOWN)
+    ctx->err = "Breakdown in CG: curvature p^T A p is near zero for some instances";
+  return st;
+}
+
+int fcu_batch_config(fcu_matrix m, int precision, int* lanes_per_row, int* threads_per_cta) {
+  if (!m || !lanes_per_row || !threads_per_cta) return FCU_ERR_BAD_ARG;
+  batch_config(m, precision, lanes_per_row, threads_per_cta);
+  return FCU_OK;
 }
 
 int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,

@@ -1,0 +1,580 @@
+// Batched Jacobi-PCG over many independent systems (no reference
+// counterpart; the batch of the scope table's multi-mesh case).
+//
+// The systems are the diagonal blocks of one block-diagonal matrix: meshes
+// of uneven sizes are concatenated into one mesh (vertex ranges disjoint), so
+// the library's pattern, assembly, load-vector and Dirichlet kernels build
+// the whole batch in one pass each, and block i is rows [off[i], off[i+1]).
+//
+// One persistent launch solves the batch. Each CTA takes the next instance
+// from a queue ordered by estimated cost (largest first) and runs that
+// instance's whole PCG alone: every reduction is CTA-local (shared memory,
+// fixed order), so instances converge, stop and report independently and no
+// grid-wide synchronisation exists. The arithmetic per instance is that of
+// the library's single-system PCG (cg.rs:40-149 for FP64; for mixed, FP32
+// difference-form operator with FP64 r, x and dots and FP64 residual
+// replacement). The launch is captured in a CUDA graph together with the
+// queue reset, and the graph is replayed on later solves. Lanes per row and
+// threads per CTA are picked by timing the candidates on the batch itself
+// (first solve of a matrix and precision), unless FCU_BATCH_VPR /
+// FCU_BATCH_THREADS fix them.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+#include "internal.cuh"
+
+void build_rowsum32(fcu_matrix m);
+
+namespace {
+
+constexpr unsigned BFULL = 0xffffffffu;
+
+__device__ __forceinline__ double bwarp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(BFULL, v, o);
+  return v;
+}
+
+// Sum NV doubles over the CTA in a fixed order; every thread gets the totals.
+template <int NV, int BT>
+__device__ __forceinline__ void cta_sum(double (&v)[NV]) {
+  __shared__ double sh[NV][BT / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    const double x = bwarp_sum(v[j]);
+    if (lane == 0) sh[j][w] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double t = 0.0;
+#pragma unroll 4
+    for (int q = 0; q < BT / 32; ++q) t += sh[j][q];
+    v[j] = t;
+  }
+  __syncthreads();
+}
+
+// One CSR row with VPR lanes (all lanes of the warp call it). DIFF: the
+// mixed operator y_i = sum_{j != i} a_ij (x_j - x_i) + S_i x_i, with S_i in
+// the diagonal slot; otherwise y_i = sum_j a_ij x_j.
+template <int VPR, bool DIFF, class T>
+__device__ __forceinline__ T batch_row(const int* __restrict__ rp, const int* __restrict__ ci,
+                                       const T* __restrict__ val, i64 row, bool valid, int sub,
+                                       const T* __restrict__ xv) {
+  T s = T(0);
+  if (valid) {
+    const int b = rp[row], e = rp[row + 1];
+    const T xi = DIFF ? xv[row] : T(0);
+    for (int q = b + sub; q < e; q += VPR) {
+      const int c = ci[q];
+      if (DIFF) s += val[q] * (c == (int)row ? xi : xv[c] - xi);
+      else s += val[q] * xv[c];
+    }
+  }
+#pragma unroll
+  for (int o = VPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(BFULL, s, o);
+  return s;
+}
+
+struct BatchArgs {
+  const int* rp;
+  const int* ci;
+  const double* val64;
+  const float* val32;
+  const i64* off;    // nb + 1 row offsets
+  const int* order;  // instances, largest first
+  int nb;
+  const double* b;
+  double* x;
+  double* r;
+  const double* invd;
+  void* z;   // T
+  void* p;   // T
+  void* ap;  // T
+  double tol;
+  i64 max_iter;
+  double delta;
+  unsigned* counter;  // queue head (zeroed before every launch)
+  i64* iters;
+  i64* updates;
+  double* relres;
+  int* status;
+};
+
+template <int VPR, int BT, class T>
+__global__ void __launch_bounds__(BT, 1024 / BT) k_batch_pcg(BatchArgs a) {
+  constexpr bool MIXED = sizeof(T) == 4;
+  constexpr int G = BT / VPR;  // row groups per CTA
+  __shared__ int s_q;
+  T* z = static_cast<T*>(a.z);
+  T* p = static_cast<T*>(a.p);
+  T* ap = static_cast<T*>(a.ap);
+  const T* val = MIXED ? reinterpret_cast<const T*>(a.val32) : reinterpret_cast<const T*>(a.val64);
+  const int tid = threadIdx.x;
+  const int g = tid / VPR, sub = tid % VPR;
+
+  for (;;) {
+    if (tid == 0) s_q = (int)atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const int q = s_q;
+    __syncthreads();
+    if (q >= a.nb) break;
+    const int inst = a.order[q];
+    const i64 r0 = a.off[inst], r1 = a.off[inst + 1];
+
+    // x0 = 0: r = b, z = D^-1 r, p = 0; r.z, r.r, b.b (cg.rs:79-90)
+    double v3[3] = {0.0, 0.0, 0.0};
+    for (i64 i = r0 + tid; i < r1; i += BT) {
+      a.x[i] = 0.0;
+      const double ri = a.b[i];
+      a.r[i] = ri;
+      const double zi = ri * a.invd[i];
+      z[i] = (T)zi;
+      p[i] = T(0);
+      v3[0] += ri * zi;
+      v3[1] += ri * ri;
+      v3[2] += ri * ri;
+    }
+    cta_sum<3, BT>(v3);
+    double rz = v3[0], rr = v3[1];
+    const double bnorm = sqrt(v3[2]);
+    double maxr = sqrt(rr);
+    double beta = 0.0;
+    i64 iter = 0, updates = 0;
+    int status = FCU_ERR_NO_CONVERGENCE;
+    bool done = false;
+    {
+      const double r0n = sqrt(rr);
+      if (r0n < a.tol || (bnorm > 0.0 && r0n / bnorm < a.tol)) {
+        status = FCU_OK;
+        done = true;
+      }
+    }
+    while (!done && iter < a.max_iter) {
+      // direction
+      {
+        const T bt = (T)beta;
+        for (i64 i = r0 + tid; i < r1; i += BT) p[i] = z[i] + bt * p[i];
+      }
+      __syncthreads();
+      // Ap, p.Ap
+      double v1[1] = {0.0};
+      for (i64 base = r0; base < r1; base += G) {
+        const i64 row = base + g;
+        const bool valid = row < r1;
+        const T s = batch_row<VPR, MIXED, T>(a.rp, a.ci, val, row, valid, sub, p);
+        if (valid && sub == 0) {
+          ap[row] = s;
+          v1[0] += (double)p[row] * (double)s;
+        }
+      }
+      cta_sum<1, BT>(v1);
+      if (fabs(v1[0]) < 1e-30) {  // cg.rs:102-107
+        iter += 1;
+        status = FCU_ERR_BREAKDOWN;
+        break;
+      }
+      const double alpha = rz / v1[0];
+      // x += alpha p, r -= alpha Ap, z = D^-1 r
+      double v2[2] = {0.0, 0.0};
+      for (i64 i = r0 + tid; i < r1; i += BT) {
+        a.x[i] += alpha * (double)p[i];
+        const double ri = a.r[i] - alpha * (double)ap[i];
+        a.r[i] = ri;
+        const double zi = ri * a.invd[i];
+        z[i] = (T)zi;
+        v2[0] += ri * zi;
+        v2[1] += ri * ri;
+      }
+      cta_sum<2, BT>(v2);
+      iter += 1;
+      rr = v2[1];
+      const double res = sqrt(v2[1]);
+      const double rel = bnorm > 0.0 ? res / bnorm : res;
+      if (!MIXED) {
+        if (rel < a.tol) {
+          status = FCU_OK;
+          done = true;
+          break;
+        }
+        beta = v2[0] / rz;
+        rz = v2[0];
+        continue;
+      }
+      if (!(rel < a.tol || res < a.delta * maxr)) {
+        beta = v2[0] / rz;
+        rz = v2[0];
+        continue;
+      }
+      // residual replacement with the FP64 matrix: r = b - A64 x, z = D^-1 r
+      double v4[2] = {0.0, 0.0};
+      for (i64 base = r0; base < r1; base += G) {
+        const i64 row = base + g;
+        const bool valid = row < r1;
+        const double s = batch_row<VPR, false, double>(a.rp, a.ci, a.val64, row, valid, sub, a.x);
+        if (valid && sub == 0) {
+          const double ri = a.b[row] - s;
+          a.r[row] = ri;
+          const double zi = ri * a.invd[row];
+          z[row] = (T)zi;
+          v4[0] += ri * zi;
+          v4[1] += ri * ri;
+        }
+      }
+      cta_sum<2, BT>(v4);
+      updates += 1;
+      rr = v4[1];
+      const double res2 = sqrt(v4[1]);
+      const double rel2 = bnorm > 0.0 ? res2 / bnorm : res2;
+      if (rel2 < a.tol) {
+        status = FCU_OK;
+        done = true;
+        break;
+      }
+      maxr = res2;
+      beta = v4[0] / rz;
+      rz = v4[0];
+    }
+    if (tid == 0) {
+      a.iters[inst] = iter;
+      a.updates[inst] = updates;
+      a.relres[inst] = bnorm > 0.0 ? sqrt(rr) / bnorm : sqrt(rr);
+      a.status[inst] = status;
+    }
+    __syncthreads();
+  }
+}
+
+// D^-1 from the diagonal slots (cg.rs:52-64: 1 when |a_kk| <= 1e-15).
+__global__ void k_batch_invd(const int* __restrict__ diag_pos, const double* __restrict__ val, i64 n,
+                             double* __restrict__ invd) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const int dp = diag_pos[i];
+    const double d = dp >= 0 ? val[dp] : 0.0;
+    invd[i] = fabs(d) > 1e-15 ? 1.0 / d : 1.0;
+  }
+}
+
+// Every row of block i must only reference columns of block i.
+__global__ void k_batch_check(const int* __restrict__ rp, const int* __restrict__ ci, const i64* __restrict__ off,
+                              int nb, int* __restrict__ bad) {
+  const int inst = blockIdx.x;
+  if (inst >= nb) return;
+  const i64 r0 = off[inst], r1 = off[inst + 1];
+  for (i64 row = r0 + threadIdx.x; row < r1; row += blockDim.x)
+    for (int q = rp[row]; q < rp[row + 1]; ++q)
+      if (ci[q] < r0 || ci[q] >= r1) atomicExch(bad, 1);
+}
+
+struct BatchConfig {
+  int vpr = 4;
+  int threads = 512;
+};
+
+using BatchKernel = void (*)(BatchArgs);
+
+template <class T>
+BatchKernel batch_kernel(int vpr, int threads) {
+#define FCU_BATCH_CASE(V, B) \
+  if (vpr == V && threads == B) return k_batch_pcg<V, B, T>;
+  FCU_BATCH_CASE(2, 256) FCU_BATCH_CASE(2, 512) FCU_BATCH_CASE(2, 1024)
+  FCU_BATCH_CASE(4, 256) FCU_BATCH_CASE(4, 512) FCU_BATCH_CASE(4, 1024)
+  FCU_BATCH_CASE(8, 256) FCU_BATCH_CASE(8, 512) FCU_BATCH_CASE(8, 1024)
+#undef FCU_BATCH_CASE
+  return nullptr;
+}
+
+}  // namespace
+
+// Per-matrix state of the batched solver: the instance layout, work buffers,
+// the tuned configuration and the instantiated graph, per precision.
+struct BatchWorkspace {
+  int nb = 0;
+  std::vector<i64> off;  // host copy of the offsets
+  DBuf<i64> off_d;
+  DBuf<int> order;
+  DBuf<double> b, x, r, invd;
+  DBuf<double> z64, p64, ap64;
+  DBuf<float> z32, p32, ap32;
+  DBuf<unsigned> counter;
+  DBuf<i64> iters, updates;
+  DBuf<double> relres;
+  DBuf<int> status;
+  BatchConfig cfg[2];
+  bool tuned[2] = {false, false};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_key[2] = {-1, -1};  // vpr * 4096 + threads of the captured launch
+  double tol_g[2] = {0.0, 0.0};
+  i64 iters_g[2] = {0, 0};
+  ~BatchWorkspace() {
+    for (auto& g : graph)
+      if (g) cudaGraphExecDestroy(g);
+  }
+};
+
+void destroy_batch_ws(BatchWorkspace* w) { delete w; }
+
+namespace {
+
+int env_int(const char* name, int dflt) {
+  const char* e = getenv(name);
+  return e ? atoi(e) : dflt;
+}
+
+BatchArgs make_args(fcu_matrix m, BatchWorkspace* w, bool mixed, double tol, i64 max_iter) {
+  BatchArgs a;
+  a.rp = m->row_ptr;
+  a.ci = m->col_idx;
+  a.val64 = m->val64.p;
+  a.val32 = m->val32.p;
+  a.off = w->off_d.p;
+  a.order = w->order.p;
+  a.nb = w->nb;
+  a.b = w->b.p;
+  a.x = w->x.p;
+  a.r = w->r.p;
+  a.invd = w->invd.p;
+  a.z = mixed ? (void*)w->z32.p : (void*)w->z64.p;
+  a.p = mixed ? (void*)w->p32.p : (void*)w->p64.p;
+  a.ap = mixed ? (void*)w->ap32.p : (void*)w->ap64.p;
+  a.tol = tol;
+  a.max_iter = max_iter;
+  a.delta = 0.1;
+  a.counter = w->counter.p;
+  a.iters = w->iters.p;
+  a.updates = w->updates.p;
+  a.relres = w->relres.p;
+  a.status = w->status.p;
+  return a;
+}
+
+BatchKernel pick_kernel(bool mixed, const BatchConfig& c) {
+  return mixed ? batch_kernel<float>(c.vpr, c.threads) : batch_kernel<double>(c.vpr, c.threads);
+}
+
+// Persistent grid: as many CTAs as fit on the device at once.
+int batch_grid(fcu_ctx ctx, BatchKernel k, int threads, int nb) {
+  int per_sm = 0;
+  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0));
+  if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "batched PCG kernel does not fit an SM");
+  return std::max(1, std::min(nb, per_sm * ctx->num_sms));
+}
+
+void launch_batch(fcu_ctx ctx, BatchWorkspace* w, BatchKernel k, const BatchConfig& c, const BatchArgs& a) {
+  CUDA_CHECK(cudaMemsetAsync(w->counter.p, 0, sizeof(unsigned), ctx->stream));
+  const int grid = batch_grid(ctx, k, c.threads, w->nb);
+  k<<<grid, c.threads, 0, ctx->stream>>>(a);
+  LAUNCH_CHECK(ctx);
+}
+
+// Time each candidate on the batch itself with a short iteration cap and
+// keep the fastest.
+BatchConfig autotune(fcu_matrix m, BatchWorkspace* w, bool mixed, double tol) {
+  BatchConfig fixed;
+  fixed.vpr = env_int("FCU_BATCH_VPR", 0);
+  fixed.threads = env_int("FCU_BATCH_THREADS", 0);
+  if (fixed.vpr && fixed.threads && pick_kernel(mixed, fixed)) return fixed;
+  fcu_ctx ctx = m->ctx;
+  const int vprs[3] = {2, 4, 8};
+  const int thr[3] = {256, 512, 1024};
+  BatchConfig best;
+  float best_ms = 1e30f;
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  const BatchArgs a = make_args(m, w, mixed, tol, 24);
+  for (int v : vprs)
+    for (int t : thr) {
+      BatchConfig c;
+      c.vpr = v;
+      c.threads = t;
+      BatchKernel k = pick_kernel(mixed, c);
+      if (!k) continue;
+      launch_batch(ctx, w, k, c, a);  // warm
+      CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+      launch_batch(ctx, w, k, c, a);
+      CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+      CUDA_CHECK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
+}  // namespace
+
+// Batched PCG driver; b, x and the per-instance outputs are device or host
+// buffers handled by the caller (api.cu) through staging.
+int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
+                   i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
+                   fcu_solve_info* info) {
+  fcu_ctx ctx = m->ctx;
+  const bool mixed = precision == FCU_MIXED;
+  if (m->bs != 1) fail(FCU_ERR_UNSUPPORTED, "batched PCG takes scalar (CSR) matrices");
+  if (!m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+  if (mixed && !m->val32.p) fail(FCU_ERR_BAD_ARG, "matrix has no FP32 copy");
+  if (nb <= 0 || nb > (1 << 30)) fail(FCU_ERR_BAD_ARG, "bad instance count");
+  if (offsets_host[0] != 0 || offsets_host[nb] != m->n) fail(FCU_ERR_BAD_ARG, "offsets must span the matrix rows");
+  for (i64 i = 0; i < nb; ++i)
+    if (offsets_host[i + 1] < offsets_host[i]) fail(FCU_ERR_BAD_ARG, "offsets must not decrease");
+  if (max_iter < 0) fail(FCU_ERR_BAD_ARG, "max_iter must be non-negative");
+
+  BatchWorkspace*& w = m->bws;
+  const bool same = w && w->nb == nb && std::equal(w->off.begin(), w->off.end(), offsets_host);
+  if (!same) {
+    delete w;
+    w = new BatchWorkspace();
+    w->nb = (int)nb;
+    w->off.assign(offsets_host, offsets_host + nb + 1);
+    upload(ctx, w->off_d, w->off.data(), nb + 1);
+    DBuf<int> bad;
+    bad.alloc(1);
+    CUDA_CHECK(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+    k_batch_check<<<(unsigned)nb, 256, 0, ctx->stream>>>(m->row_ptr, m->col_idx, w->off_d.p, (int)nb, bad.p);
+    LAUNCH_CHECK(ctx);
+    int hbad = 0;
+    download(ctx, &hbad, bad.p, 1);
+    if (hbad) fail(FCU_ERR_BAD_ARG, "matrix is not block diagonal over the given offsets");
+    // queue order: estimated cost (stored entries x sqrt(rows), the 2D
+    // iteration growth), largest first
+    std::vector<int> hrp(nb + 1);
+    std::vector<int> rpv(m->n + 1);
+    download(ctx, rpv.data(), m->row_ptr, m->n + 1);
+    std::vector<double> cost(nb);
+    for (i64 i = 0; i < nb; ++i) {
+      const double rows = (double)(offsets_host[i + 1] - offsets_host[i]);
+      const double nnz = (double)(rpv[offsets_host[i + 1]] - rpv[offsets_host[i]]);
+      cost[i] = (nnz + rows) * std::sqrt(std::max(rows, 1.0));
+    }
+    std::vector<int> ord(nb);
+    for (i64 i = 0; i < nb; ++i) ord[i] = (int)i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    upload(ctx, w->order, ord.data(), nb);
+    const i64 n = m->n;
+    w->b.alloc(n);
+    w->x.alloc(n);
+    w->r.alloc(n);
+    w->invd.alloc(n);
+    w->counter.alloc(1);
+    w->iters.alloc(nb);
+    w->updates.alloc(nb);
+    w->relres.alloc(nb);
+    w->status.alloc(nb);
+  }
+  const i64 n = m->n;
+  if (mixed && !w->z32.p) {
+    w->z32.alloc(n);
+    w->p32.alloc(n);
+    w->ap32.alloc(n);
+  }
+  if (!mixed && !w->z64.p) {
+    w->z64.alloc(n);
+    w->p64.alloc(n);
+    w->ap64.alloc(n);
+  }
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+  k_batch_invd<<<grid_for(n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(m->diag_pos, m->val64.p, n, w->invd.p);
+  LAUNCH_CHECK(ctx);
+  if (mixed) build_rowsum32(m);
+  CUDA_CHECK(cudaMemcpyAsync(w->b.p, b_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  const int k = mixed ? 1 : 0;
+  if (!w->tuned[k]) {
+    w->cfg[k] = autotune(m, w, mixed, tol);
+    w->tuned[k] = true;
+  }
+  const BatchConfig c = w->cfg[k];
+  BatchKernel kern = pick_kernel(mixed, c);
+  const int key = c.vpr * 4096 + c.threads;
+  if (!w->graph[k] || w->graph_key[k] != key || w->tol_g[k] != tol || w->iters_g[k] != max_iter) {
+    if (w->graph[k]) {
+      cudaGraphExecDestroy(w->graph[k]);
+      w->graph[k] = nullptr;
+    }
+    const BatchArgs a = make_args(m, w, mixed, tol, max_iter);
+    cudaGraph_t g;
+    CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      launch_batch(ctx, w, kern, c, a);
+    } catch (...) {
+      cudaStreamEndCapture(ctx->stream, &g);
+      throw;
+    }
+    CUDA_CHECK(cudaStreamEndCapture(ctx->stream, &g));
+    CUDA_CHECK(cudaGraphInstantiate(&w->graph[k], g, 0));
+    cudaGraphDestroy(g);
+    w->graph_key[k] = key;
+    w->tol_g[k] = tol;
+    w->iters_g[k] = max_iter;
+  }
+  CUDA_CHECK(cudaGraphLaunch(w->graph[k], ctx->stream));
+  ctx->launches += 1;
+  CUDA_CHECK(cudaMemcpyAsync(x_dev, w->x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+  CUDA_CHECK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::vector<i64> it(nb), up(nb);
+  std::vector<double> rel(nb);
+  std::vector<int> st(nb);
+  download(ctx, it.data(), w->iters.p, nb);
+  download(ctx, up.data(), w->updates.p, nb);
+  download(ctx, rel.data(), w->relres.p, nb);
+  download(ctx, st.data(), w->status.p, nb);
+  if (iters_host) std::copy(it.begin(), it.end(), iters_host);
+  if (relres_host) std::copy(rel.begin(), rel.end(), relres_host);
+  if (status_host) std::copy(st.begin(), st.end(), status_host);
+  int worst = FCU_OK;
+  i64 max_it = 0, sum_it = 0, sum_up = 0;
+  double max_rel = 0.0;
+  double bytes = 0.0;
+  const double w8 = mixed ? 4.0 : 8.0;
+  for (i64 i = 0; i < nb; ++i) {
+    if (st[i] != FCU_OK && worst == FCU_OK) worst = st[i];
+    max_it = std::max(max_it, it[i]);
+    sum_it += it[i];
+    sum_up += up[i];
+    max_rel = std::max(max_rel, rel[i]);
+    // per iteration: values + columns + row pointers, then the vector passes
+    // (direction 3w, SpMV p and Ap 2w, update 40 + 3w bytes per row)
+    const double rows = (double)(offsets_host[i + 1] - offsets_host[i]);
+    bytes += (double)it[i] * (rows * (8.0 * w8 + 44.0));
+  }
+  if (info) {
+    info->iterations = max_it;
+    info->outer_updates = sum_up;
+    info->residual = 0.0;
+    info->rel_residual = max_rel;
+    info->kernel_ms = ms;
+    info->effective_bw_gbps = ms > 0 ? bytes / (ms * 1e-3) / 1e9 : 0.0;
+    info->status = worst;
+  }
+  (void)sum_it;
+  return worst;
+}
+
+void batch_config(fcu_matrix m, int precision, int* vpr, int* threads) {
+  const int k = precision == FCU_MIXED ? 1 : 0;
+  if (!m->bws || !m->bws->tuned[k]) {
+    *vpr = 0;
+    *threads = 0;
+    return;
+  }
+  *vpr = m->bws->cfg[k].vpr;
+  *threads = m->bws->cfg[k].threads;
+}

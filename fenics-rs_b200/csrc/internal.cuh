@@ -71,7 +71,9 @@ struct DBuf {
 // Handles
 // ---------------------------------------------------------------------------
 
-struct Workspace;  // solver state, defined in solver.cu
+struct Workspace;       // solver state, defined in solver.cu
+struct BatchWorkspace;  // batched solver state, defined in batch.cu
+void destroy_batch_ws(BatchWorkspace* w);
 
 // Handles are reference counted: a mesh holds its context, a space its mesh,
 // a matrix its space and context. fcu_*_destroy drops the caller's reference,
@@ -155,6 +157,7 @@ struct fcu_matrix_s {
   DBuf<i64> csc_colptr, csc_rowidx; // wrapped CSC: the caller's layout, for export
   DBuf<int> csr_of;                 // wrapped CSC: CSC position -> CSR slot
   Workspace* ws = nullptr;
+  BatchWorkspace* bws = nullptr;
   ~fcu_matrix_s();
 };
 

@@ -754,7 +754,10 @@ struct Workspace {
   }
 };
 
-fcu_matrix_s::~fcu_matrix_s() { delete ws; }
+fcu_matrix_s::~fcu_matrix_s() {
+  delete ws;
+  destroy_batch_ws(bws);
+}
 
 namespace {
 

@@ -197,6 +197,23 @@ def unit_square(nx: int, ny: int) -> Mesh:
     return Mesh(coords, cells)
 
 
+def concat_meshes(meshes) -> tuple[Mesh, np.ndarray]:
+    """One mesh holding several meshes side by side (vertex ranges disjoint,
+    cells renumbered), and the vertex offsets of each: the layout of a batch,
+    whose scalar P1 matrix is block diagonal over these offsets."""
+    meshes = list(meshes)
+    if not meshes:
+        raise ValueError("no meshes")
+    dims = {m.dim for m in meshes}
+    if len(dims) != 1:
+        raise ValueError("meshes of one dimension expected")
+    nvs = np.array([m.nv for m in meshes], np.int64)
+    offs = np.concatenate([[0], np.cumsum(nvs)])
+    coords = np.concatenate([m.coords for m in meshes])
+    cells = np.concatenate([m.cells + o for m, o in zip(meshes, offs[:-1])])
+    return Mesh(coords, cells), offs
+
+
 def box_beam(length, width, height, nx, ny, nz) -> Mesh:
     """generators.rs:58-111: x fastest, Kuhn split of each hexahedron into 6 tets."""
     if nx <= 0 or ny <= 0 or nz <= 0:
@@ -437,6 +454,31 @@ class Matrix:
         if raise_on_error:
             _check(self.ctx, rc)
         return x, info
+
+    def batch_pcg(self, offsets, b, x=None, tol=1e-8, max_iter=10000, precision=FCU_MIXED, raise_on_error=True):
+        """Batched Jacobi-PCG over the diagonal blocks [offsets[i], offsets[i+1])
+        of this matrix, each solved from zero to its own tolerance in one
+        persistent launch. Returns (x, iterations, rel_residual, status, SolveInfo)."""
+        offs = np.ascontiguousarray(offsets, dtype=np.int64)
+        nb = len(offs) - 1
+        x = np.empty(self.n) if x is None else x
+        pb, kb = _ptr(b, np.float64)
+        px, kx = _ptr(x)
+        it = np.zeros(nb, np.int64)
+        rel = np.zeros(nb)
+        st = np.zeros(nb, np.int32)
+        info = SolveInfo()
+        rc = _L().fcu_batch_pcg(self.ctx.h, self.h, nb, offs.ctypes.data, pb, px, float(tol), int(max_iter),
+                                precision, it.ctypes.data, rel.ctypes.data, st.ctypes.data, C.byref(info))
+        if raise_on_error:
+            _check(self.ctx, rc)
+        return x, it, rel, st, info
+
+    def batch_config(self, precision=FCU_MIXED):
+        """(lanes per row, threads per CTA) the batched solver tuned for this matrix."""
+        v, t = C.c_int(), C.c_int()
+        _L().fcu_batch_config(self.h, precision, C.byref(v), C.byref(t))
+        return v.value, t.value
 
 
 # ---------------------------------------------------------------------------
@@ -702,6 +744,42 @@ def solve_poisson_2d(mesh: Mesh, source, boundary_value, tol, max_iter, ctx=None
 def solve_poisson_3d(mesh: Mesh, source, boundary_value, tol, max_iter, ctx=None, precision=FCU_FP64):
     """solve_poisson_3d (poisson_solver.rs:99-132)."""
     return _solve_poisson(mesh, source, boundary_value, tol, max_iter, ctx, precision)
+
+
+@dataclass
+class BatchSolution:
+    """Per-instance results of a batched solve."""
+    solutions: list
+    iterations: np.ndarray
+    rel_residuals: np.ndarray
+    statuses: np.ndarray
+    info: SolveInfo
+    offsets: np.ndarray
+
+
+def solve_poisson_batch(meshes, kappas=None, nodal_sources=None, tol=1e-8, max_iter=100000, ctx=None,
+                        precision=FCU_MIXED, raise_on_error=True) -> BatchSolution:
+    """Independent P1 Poisson problems -div(kappa_e grad u) = f, u = 0 on each
+    mesh's boundary, assembled as one block-diagonal system and solved by the
+    batched PCG (each instance to its own relative tolerance). kappas: per-cell
+    coefficients per mesh (None = 1); nodal_sources: nodal f per mesh, loaded as
+    the integral of (sum_j f_j phi_j) phi_i (None = 1)."""
+    ctx = ctx or default_context()
+    meshes = list(meshes)
+    mesh, offs = concat_meshes(meshes)
+    V = FunctionSpace(ctx, mesh, FCU_SPACE_P1)
+    kappa = None if kappas is None else np.concatenate([np.asarray(k, np.float64) for k in kappas])
+    M = Matrix(ctx, V).assemble_stiffness(kappa)
+    f = np.ones(mesh.nv) if nodal_sources is None else np.concatenate([np.asarray(v, np.float64)
+                                                                      for v in nodal_sources])
+    b = V.rhs_source(FCU_SRC_NODAL, nodal=f)
+    bd = V.boundary_dofs()
+    M.apply_dirichlet(b, bd, np.zeros(len(bd)))
+    x, it, rel, st, info = M.batch_pcg(offs, b, tol=tol, max_iter=max_iter, precision=precision,
+                                       raise_on_error=raise_on_error)
+    M.close()
+    V.close()
+    return BatchSolution([x[offs[i]:offs[i + 1]] for i in range(len(meshes))], it, rel, st, info, offs)
 
 
 @dataclass

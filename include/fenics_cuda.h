@@ -176,6 +176,25 @@ int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint
                      const double* vals, const double* inv_diag, const double* b, const double* x0,
                      double rtol, int64_t max_iter, double* x, fcu_solve_info* info);
 
+/* Batched Jacobi-PCG over independent systems (no reference counterpart; the
+ * multi-mesh batch). m is a scalar matrix that is block diagonal over the
+ * row ranges [offsets[i], offsets[i+1]), i < nb (offsets: nb + 1 values,
+ * offsets[0] = 0, offsets[nb] = n) - e.g. assembled on a mesh that
+ * concatenates the instances' meshes. Every block is solved from x0 = 0 with
+ * its own alpha, beta and stopping test ||r_i|| / ||b_i|| < tol, as
+ * fcu_pcg would solve it alone (precision FCU_FP64 or FCU_MIXED), in one
+ * persistent launch (captured in a CUDA graph, replayed on later calls).
+ * Per-instance iterations, relative residuals and statuses go to the
+ * optional host arrays (nb each). Returns FCU_OK when every instance
+ * converged, else the first failing status. info: max iterations, total
+ * replacements, max relative residual, device time. */
+int fcu_batch_pcg(fcu_ctx ctx, fcu_matrix m, int64_t nb, const int64_t* offsets, const double* b, double* x,
+                  double tol, int64_t max_iter, int precision, int64_t* iterations, double* rel_residual,
+                  int* status, fcu_solve_info* info);
+/* Lanes per row and threads per CTA the batched solver chose for m and
+ * `precision` (0, 0 before its first solve). */
+int fcu_batch_config(fcu_matrix m, int precision, int* lanes_per_row, int* threads_per_cta);
+
 /* Allocation-free variant of fcu_solve_csr_cg. No counterpart in the
  * reference: it serves callers that cannot allocate device memory when they
  * solve (an application whose pool allocator owns the device's memory, or a

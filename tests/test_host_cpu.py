@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 import oracle as O
 
@@ -50,3 +51,20 @@ def test_vector_bc_arrays(fcu):
     bc = fcu.VectorDirichletBC([(3, 0.0), (4, 1.5)])
     d, v = bc.arrays()
     assert d.tolist() == [3, 4] and v.tolist() == [0.0, 1.5]
+
+
+def test_concat_meshes_layout(fcu):
+    """A batch's concatenated mesh: disjoint vertex ranges, renumbered cells,
+    and a boundary that is the union of the instances' boundaries."""
+    parts = [O.unit_square(n, n) for n in (3, 5, 2)]
+    mesh, offs = fcu.concat_meshes([fcu.Mesh(p.coords, p.cells) for p in parts])
+    assert offs.tolist() == [0, 16, 52, 61]
+    assert mesh.nv == 61 and mesh.nc == sum(p.cells.shape[0] for p in parts)
+    for p, o, c0 in zip(parts, offs[:-1], np.cumsum([0] + [q.cells.shape[0] for q in parts])[:-1]):
+        assert np.array_equal(mesh.coords[o:o + p.coords.shape[0]], p.coords)
+        assert np.array_equal(mesh.cells[c0:c0 + p.cells.shape[0]], p.cells + o)
+    om = O.Mesh(mesh.coords, mesh.cells)
+    want = np.concatenate([O.boundary_dofs_2d(p) + o for p, o in zip(parts, offs[:-1])])
+    assert np.array_equal(O.boundary_dofs_2d(om), want)
+    with pytest.raises(ValueError):
+        fcu.concat_meshes([])
