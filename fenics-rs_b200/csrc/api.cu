@@ -31,7 +31,7 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
 int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
                    i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
                    fcu_solve_info* info);
-void batch_config(fcu_matrix m, int precision, int* vpr, int* threads);
+void batch_config(fcu_matrix m, int precision, int* vpr, int* threads, int* cluster);
 int run_pcg_noalloc(i64 n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
                     const double* inv_diag, const double* b, const double* x0, double rtol, i64 max_iter, double* x,
                     fcu_solve_info* info, void* stream);
@@ -865,9 +865,9 @@ int fcu_batch_pcg(fcu_ctx ctx, fcu_matrix m, int64_t nb, const int64_t* offsets,
   return st;
 }
 
-int fcu_batch_config(fcu_matrix m, int precision, int* lanes_per_row, int* threads_per_cta) {
-  if (!m || !lanes_per_row || !threads_per_cta) return FCU_ERR_BAD_ARG;
-  batch_config(m, precision, lanes_per_row, threads_per_cta);
+int fcu_batch_config(fcu_matrix m, int precision, int* lanes_per_row, int* threads_per_cta, int* ctas_per_cluster) {
+  if (!m || !lanes_per_row || !threads_per_cta || !ctas_per_cluster) return FCU_ERR_BAD_ARG;
+  batch_config(m, precision, lanes_per_row, threads_per_cta, ctas_per_cluster);
   return FCU_OK;
 }
 

@@ -24,7 +24,11 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "internal.cuh"
+
+namespace cg = cooperative_groups;
 
 void build_rowsum32(fcu_matrix m);
 
@@ -38,9 +42,16 @@ __device__ __forceinline__ double bwarp_sum(double v) {
   return v;
 }
 
-// Sum NV doubles over the CTA in a fixed order; every thread gets the totals.
+// Sum NV doubles over the cluster that owns the instance; every thread of
+// every CTA of the cluster gets the totals. Each CTA reduces its threads in a
+// fixed order and publishes its sum in a shared-memory slot; after the
+// cluster barrier (release/acquire at cluster scope, so it also orders the
+// CTAs' global-memory writes) every thread adds the slots in rank order. The
+// slots alternate between two buffers: a CTA rewrites a buffer only after the
+// next barrier, which every CTA reaches after reading it.
 template <int NV, int BT>
-__device__ __forceinline__ void cta_sum(double (&v)[NV]) {
+__device__ __forceinline__ void cluster_sum(double (&v)[NV], double (*slots)[4], int& parity,
+                                            cg::cluster_group& cl) {
   __shared__ double sh[NV][BT / 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -49,17 +60,27 @@ __device__ __forceinline__ void cta_sum(double (&v)[NV]) {
     if (lane == 0) sh[j][w] = x;
   }
   __syncthreads();
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int j = 0; j < NV; ++j) {
-    double t = 0.0;
-#pragma unroll 4
-    for (int q = 0; q < BT / 32; ++q) t += sh[j][q];
-    v[j] = t;
+    for (int j = 0; j < NV; ++j) {
+      double t = 0.0;
+      for (int q = 0; q < BT / 32; ++q) t += sh[j][q];
+      slots[parity][j] = t;
+    }
   }
-  __syncthreads();
+  cl.sync();
+  const unsigned nr = cl.num_blocks();
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = 0.0;
+  for (unsigned k = 0; k < nr; ++k) {
+    const double* rs = cl.map_shared_rank(&slots[parity][0], k);
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] += rs[j];
+  }
+  parity ^= 1;
 }
 
-// One CSR row with VPR lanes (all lanes of the warp call it). DIFF: the
+// One CSR row with VPR >= 2 lanes (all lanes of the warp call it). DIFF: the
 // mixed operator y_i = sum_{j != i} a_ij (x_j - x_i) + S_i x_i, with S_i in
 // the diagonal slot; otherwise y_i = sum_j a_ij x_j.
 template <int VPR, bool DIFF, class T>
@@ -78,6 +99,38 @@ __device__ __forceinline__ T batch_row(const int* __restrict__ rp, const int* __
   }
 #pragma unroll
   for (int o = VPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(BFULL, s, o);
+  return s;
+}
+
+// One CSR row per thread (VPR = 1): a block of entries (eight for FP32,
+// four for FP64, to stay within the register budget) is loaded, values and
+// columns, then all its operand entries, before the arithmetic. Entries are
+// summed in CSR order; unused slots read row 0's operand with weight 0.
+template <bool DIFF, class T>
+__device__ __forceinline__ T batch_row1(const int* __restrict__ rp, const int* __restrict__ ci,
+                                        const T* __restrict__ val, i64 row, const T* __restrict__ xv) {
+  constexpr int E = sizeof(T) == 4 ? 8 : 4;
+  const int a0 = rp[row], a1 = rp[row + 1];
+  const T xa = DIFF ? xv[row] : T(0);
+  T s = T(0);
+  for (int k0 = a0; k0 < a1; k0 += E) {
+    const int na = a1 - k0;
+    int c[E];
+    T wv[E], g[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const bool h = k < na;
+      c[k] = h ? ci[k0 + k] : 0;
+      wv[k] = h ? val[k0 + k] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < E; ++k) g[k] = xv[c[k]];
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      if (DIFF) s += wv[k] * (c[k] == (int)row ? xa : g[k] - xa);
+      else s += wv[k] * g[k];
+    }
+  }
   return s;
 }
 
@@ -106,30 +159,61 @@ struct BatchArgs {
   int* status;
 };
 
+// Operator rows [c0, c1) of this CTA: y = A v; emit(row, y) once per row.
+template <int VPR, int BT, bool DIFF, class T, class Emit>
+__device__ __forceinline__ void batch_spmv(const int* __restrict__ rp, const int* __restrict__ ci,
+                                           const T* __restrict__ val, i64 c0, i64 c1, const T* __restrict__ v,
+                                           Emit emit) {
+  const int tid = threadIdx.x;
+  if (VPR == 1) {
+    for (i64 row = c0 + tid; row < c1; row += BT) emit(row, batch_row1<DIFF, T>(rp, ci, val, row, v));
+  } else {
+    constexpr int G = BT / VPR;
+    const int g = tid / VPR, sub = tid % VPR;
+    for (i64 base = c0; base < c1; base += G) {
+      const i64 row = base + g;
+      const bool valid = row < c1;
+      const T s = batch_row<VPR, DIFF, T>(rp, ci, val, row, valid, sub, v);
+      if (valid && sub == 0) emit(row, s);
+    }
+  }
+}
+
+// A cluster of CTAs (1 to 8; the launch's cluster size) solves one instance
+// at a time: CTA rank k owns rows [r0 + k len / CL, r0 + (k + 1) len / CL)
+// for every phase, and the phases are separated by cluster barriers.
 template <int VPR, int BT, class T>
 __global__ void __launch_bounds__(BT, 1024 / BT) k_batch_pcg(BatchArgs a) {
   constexpr bool MIXED = sizeof(T) == 4;
-  constexpr int G = BT / VPR;  // row groups per CTA
   __shared__ int s_q;
-  T* z = static_cast<T*>(a.z);
-  T* p = static_cast<T*>(a.p);
-  T* ap = static_cast<T*>(a.ap);
-  const T* val = MIXED ? reinterpret_cast<const T*>(a.val32) : reinterpret_cast<const T*>(a.val64);
+  __shared__ double slots[2][4];
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned ncl = cl.num_blocks(), rank = cl.block_rank();
+  int parity = 0;
+  // the parameter block's address is never taken (no local copy of it)
+  T* const z = static_cast<T*>(a.z);
+  T* const p = static_cast<T*>(a.p);
+  T* const ap = static_cast<T*>(a.ap);
   const int tid = threadIdx.x;
-  const int g = tid / VPR, sub = tid % VPR;
 
   for (;;) {
-    if (tid == 0) s_q = (int)atomicAdd(a.counter, 1u);
-    __syncthreads();
-    const int q = s_q;
-    __syncthreads();
+    if (rank == 0 && tid == 0) s_q = (int)atomicAdd(a.counter, 1u);
+    cl.sync();
+    const int q = *cl.map_shared_rank(&s_q, 0);
+    cl.sync();
     if (q >= a.nb) break;
     const int inst = a.order[q];
     const i64 r0 = a.off[inst], r1 = a.off[inst + 1];
+    // rank k owns len / ncl rows, one more for the first len % ncl ranks
+    // (32-bit arithmetic: rows are int32-indexed)
+    const unsigned len = (unsigned)(r1 - r0);
+    const unsigned share = len / ncl, extra = len % ncl;
+    const i64 c0 = r0 + (i64)(share * rank + min(rank, extra));
+    const i64 c1 = c0 + (i64)(share + (rank < extra ? 1u : 0u));
 
     // x0 = 0: r = b, z = D^-1 r, p = 0; r.z, r.r, b.b (cg.rs:79-90)
     double v3[3] = {0.0, 0.0, 0.0};
-    for (i64 i = r0 + tid; i < r1; i += BT) {
+    for (i64 i = c0 + tid; i < c1; i += BT) {
       a.x[i] = 0.0;
       const double ri = a.b[i];
       a.r[i] = ri;
@@ -138,42 +222,41 @@ __global__ void __launch_bounds__(BT, 1024 / BT) k_batch_pcg(BatchArgs a) {
       p[i] = T(0);
       v3[0] += ri * zi;
       v3[1] += ri * ri;
-      v3[2] += ri * ri;
     }
-    cta_sum<3, BT>(v3);
+    v3[2] = v3[1];
+    cluster_sum<3, BT>(v3, slots, parity, cl);
     double rz = v3[0], rr = v3[1];
     const double bnorm = sqrt(v3[2]);
     double maxr = sqrt(rr);
     double beta = 0.0;
     i64 iter = 0, updates = 0;
     int status = FCU_ERR_NO_CONVERGENCE;
-    bool done = false;
     {
       const double r0n = sqrt(rr);
-      if (r0n < a.tol || (bnorm > 0.0 && r0n / bnorm < a.tol)) {
-        status = FCU_OK;
-        done = true;
-      }
+      if (r0n < a.tol || (bnorm > 0.0 && r0n / bnorm < a.tol)) status = FCU_OK;
     }
-    while (!done && iter < a.max_iter) {
+    while (status != FCU_OK && iter < a.max_iter) {
       // direction
       {
         const T bt = (T)beta;
-        for (i64 i = r0 + tid; i < r1; i += BT) p[i] = z[i] + bt * p[i];
-      }
-      __syncthreads();
-      // Ap, p.Ap
-      double v1[1] = {0.0};
-      for (i64 base = r0; base < r1; base += G) {
-        const i64 row = base + g;
-        const bool valid = row < r1;
-        const T s = batch_row<VPR, MIXED, T>(a.rp, a.ci, val, row, valid, sub, p);
-        if (valid && sub == 0) {
-          ap[row] = s;
-          v1[0] += (double)p[row] * (double)s;
+        for (i64 i = c0 + tid; i < c1; i += 4 * BT) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const i64 k = i + u * BT;
+            if (k < c1) p[k] = z[k] + bt * p[k];
+          }
         }
       }
-      cta_sum<1, BT>(v1);
+      cl.sync();
+      // Ap, p.Ap
+      double v1[1] = {0.0};
+      batch_spmv<VPR, BT, MIXED, T>(a.rp, a.ci, MIXED ? reinterpret_cast<const T*>(a.val32)
+                                                      : reinterpret_cast<const T*>(a.val64),
+                                    c0, c1, p, [&v1, ap, p](i64 row, T s) {
+                                      ap[row] = s;
+                                      v1[0] += (double)p[row] * (double)s;
+                                    });
+      cluster_sum<1, BT>(v1, slots, parity, cl);
       if (fabs(v1[0]) < 1e-30) {  // cg.rs:102-107
         iter += 1;
         status = FCU_ERR_BREAKDOWN;
@@ -182,16 +265,35 @@ __global__ void __launch_bounds__(BT, 1024 / BT) k_batch_pcg(BatchArgs a) {
       const double alpha = rz / v1[0];
       // x += alpha p, r -= alpha Ap, z = D^-1 r
       double v2[2] = {0.0, 0.0};
-      for (i64 i = r0 + tid; i < r1; i += BT) {
-        a.x[i] += alpha * (double)p[i];
-        const double ri = a.r[i] - alpha * (double)ap[i];
-        a.r[i] = ri;
-        const double zi = ri * a.invd[i];
-        z[i] = (T)zi;
-        v2[0] += ri * zi;
-        v2[1] += ri * ri;
+      for (i64 i = c0 + tid; i < c1; i += 2 * BT) {
+        double xi[2], ri[2], di[2];
+        T pi[2], api[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const i64 k = i + u * BT;
+          if (k < c1) {
+            xi[u] = a.x[k];
+            ri[u] = a.r[k];
+            di[u] = a.invd[k];
+            pi[u] = p[k];
+            api[u] = ap[k];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const i64 k = i + u * BT;
+          if (k < c1) {
+            a.x[k] = xi[u] + alpha * (double)pi[u];
+            const double rn = ri[u] - alpha * (double)api[u];
+            a.r[k] = rn;
+            const double zi = rn * di[u];
+            z[k] = (T)zi;
+            v2[0] += rn * zi;
+            v2[1] += rn * rn;
+          }
+        }
       }
-      cta_sum<2, BT>(v2);
+      cluster_sum<2, BT>(v2, slots, parity, cl);
       iter += 1;
       rr = v2[1];
       const double res = sqrt(v2[1]);
@@ -199,7 +301,6 @@ __global__ void __launch_bounds__(BT, 1024 / BT) k_batch_pcg(BatchArgs a) {
       if (!MIXED) {
         if (rel < a.tol) {
           status = FCU_OK;
-          done = true;
           break;
         }
         beta = v2[0] / rz;
@@ -212,41 +313,36 @@ __global__ void __launch_bounds__(BT, 1024 / BT) k_batch_pcg(BatchArgs a) {
         continue;
       }
       // residual replacement with the FP64 matrix: r = b - A64 x, z = D^-1 r
+      // (x of the whole instance is complete since the cluster sum above)
       double v4[2] = {0.0, 0.0};
-      for (i64 base = r0; base < r1; base += G) {
-        const i64 row = base + g;
-        const bool valid = row < r1;
-        const double s = batch_row<VPR, false, double>(a.rp, a.ci, a.val64, row, valid, sub, a.x);
-        if (valid && sub == 0) {
-          const double ri = a.b[row] - s;
-          a.r[row] = ri;
-          const double zi = ri * a.invd[row];
-          z[row] = (T)zi;
-          v4[0] += ri * zi;
-          v4[1] += ri * ri;
-        }
-      }
-      cta_sum<2, BT>(v4);
+      batch_spmv<VPR, BT, false, double>(a.rp, a.ci, a.val64, c0, c1, a.x,
+                                         [&v4, z, rv = a.r, bv = a.b, dv = a.invd](i64 row, double s) {
+                                           const double rn = bv[row] - s;
+                                           rv[row] = rn;
+                                           const double zi = rn * dv[row];
+                                           z[row] = (T)zi;
+                                           v4[0] += rn * zi;
+                                           v4[1] += rn * rn;
+                                         });
+      cluster_sum<2, BT>(v4, slots, parity, cl);
       updates += 1;
       rr = v4[1];
       const double res2 = sqrt(v4[1]);
       const double rel2 = bnorm > 0.0 ? res2 / bnorm : res2;
       if (rel2 < a.tol) {
         status = FCU_OK;
-        done = true;
         break;
       }
       maxr = res2;
       beta = v4[0] / rz;
       rz = v4[0];
     }
-    if (tid == 0) {
+    if (rank == 0 && tid == 0) {
       a.iters[inst] = iter;
       a.updates[inst] = updates;
       a.relres[inst] = bnorm > 0.0 ? sqrt(rr) / bnorm : sqrt(rr);
       a.status[inst] = status;
     }
-    __syncthreads();
   }
 }
 
@@ -272,8 +368,9 @@ __global__ void k_batch_check(const int* __restrict__ rp, const int* __restrict_
 }
 
 struct BatchConfig {
-  int vpr = 4;
-  int threads = 512;
+  int vpr = 1;
+  int threads = 1024;
+  int cluster = 1;
 };
 
 using BatchKernel = void (*)(BatchArgs);
@@ -282,9 +379,9 @@ template <class T>
 BatchKernel batch_kernel(int vpr, int threads) {
 #define FCU_BATCH_CASE(V, B) \
   if (vpr == V && threads == B) return k_batch_pcg<V, B, T>;
-  FCU_BATCH_CASE(2, 256) FCU_BATCH_CASE(2, 512) FCU_BATCH_CASE(2, 1024)
-  FCU_BATCH_CASE(4, 256) FCU_BATCH_CASE(4, 512) FCU_BATCH_CASE(4, 1024)
-  FCU_BATCH_CASE(8, 256) FCU_BATCH_CASE(8, 512) FCU_BATCH_CASE(8, 1024)
+  FCU_BATCH_CASE(1, 512) FCU_BATCH_CASE(1, 1024)
+  FCU_BATCH_CASE(2, 512) FCU_BATCH_CASE(2, 1024)
+  FCU_BATCH_CASE(4, 512) FCU_BATCH_CASE(4, 1024)
 #undef FCU_BATCH_CASE
   return nullptr;
 }
@@ -308,7 +405,7 @@ struct BatchWorkspace {
   BatchConfig cfg[2];
   bool tuned[2] = {false, false};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  int graph_key[2] = {-1, -1};  // vpr * 4096 + threads of the captured launch
+  int graph_key[2] = {-1, -1};  // configuration of the captured launch
   double tol_g[2] = {0.0, 0.0};
   i64 iters_g[2] = {0, 0};
   ~BatchWorkspace() {
@@ -357,31 +454,59 @@ BatchKernel pick_kernel(bool mixed, const BatchConfig& c) {
   return mixed ? batch_kernel<float>(c.vpr, c.threads) : batch_kernel<double>(c.vpr, c.threads);
 }
 
-// Persistent grid: as many CTAs as fit on the device at once.
-int batch_grid(fcu_ctx ctx, BatchKernel k, int threads, int nb) {
-  int per_sm = 0;
-  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0));
-  if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "batched PCG kernel does not fit an SM");
-  return std::max(1, std::min(nb, per_sm * ctx->num_sms));
+// Persistent grid: as many clusters as fit on the device at once (at most
+// one per instance). 0 when the configuration cannot be placed.
+int batch_grid(fcu_ctx ctx, BatchKernel k, const BatchConfig& c, int nb) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(c.cluster * std::max(1, std::min(nb, ctx->num_sms))));
+  cfg.blockDim = dim3((unsigned)c.threads);
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)c.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int nclusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&nclusters, k, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return c.cluster * std::min(nb, nclusters);
 }
 
-void launch_batch(fcu_ctx ctx, BatchWorkspace* w, BatchKernel k, const BatchConfig& c, const BatchArgs& a) {
+void launch_batch(fcu_ctx ctx, BatchWorkspace* w, BatchKernel k, const BatchConfig& c, int grid,
+                  const BatchArgs& a) {
   CUDA_CHECK(cudaMemsetAsync(w->counter.p, 0, sizeof(unsigned), ctx->stream));
-  const int grid = batch_grid(ctx, k, c.threads, w->nb);
-  k<<<grid, c.threads, 0, ctx->stream>>>(a);
-  LAUNCH_CHECK(ctx);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)c.threads);
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)c.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CUDA_CHECK(cudaLaunchKernelEx(&cfg, k, a));
 }
 
-// Time each candidate on the batch itself with a short iteration cap and
-// keep the fastest.
+// Time each candidate (lanes per row x threads per CTA x CTAs per cluster) on
+// the batch itself with a short iteration cap and keep the fastest.
 BatchConfig autotune(fcu_matrix m, BatchWorkspace* w, bool mixed, double tol) {
   BatchConfig fixed;
   fixed.vpr = env_int("FCU_BATCH_VPR", 0);
   fixed.threads = env_int("FCU_BATCH_THREADS", 0);
-  if (fixed.vpr && fixed.threads && pick_kernel(mixed, fixed)) return fixed;
+  fixed.cluster = env_int("FCU_BATCH_CLUSTER", 0);
+  if (fixed.vpr && fixed.threads && fixed.cluster && pick_kernel(mixed, fixed) &&
+      batch_grid(m->ctx, pick_kernel(mixed, fixed), fixed, w->nb) > 0)
+    return fixed;
   fcu_ctx ctx = m->ctx;
-  const int vprs[3] = {2, 4, 8};
-  const int thr[3] = {256, 512, 1024};
+  const int vprs[3] = {1, 2, 4};
+  const int thr[2] = {512, 1024};
+  const int cls[4] = {1, 2, 4, 8};
   BatchConfig best;
   float best_ms = 1e30f;
   cudaEvent_t e0, e1;
@@ -389,26 +514,31 @@ BatchConfig autotune(fcu_matrix m, BatchWorkspace* w, bool mixed, double tol) {
   CUDA_CHECK(cudaEventCreate(&e1));
   const BatchArgs a = make_args(m, w, mixed, tol, 24);
   for (int v : vprs)
-    for (int t : thr) {
-      BatchConfig c;
-      c.vpr = v;
-      c.threads = t;
-      BatchKernel k = pick_kernel(mixed, c);
-      if (!k) continue;
-      launch_batch(ctx, w, k, c, a);  // warm
-      CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
-      launch_batch(ctx, w, k, c, a);
-      CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
-      CUDA_CHECK(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best_ms) {
-        best_ms = ms;
-        best = c;
+    for (int t : thr)
+      for (int cs : cls) {
+        BatchConfig c;
+        c.vpr = v;
+        c.threads = t;
+        c.cluster = cs;
+        BatchKernel k = pick_kernel(mixed, c);
+        if (!k) continue;
+        const int grid = batch_grid(ctx, k, c, w->nb);
+        if (grid <= 0) continue;
+        launch_batch(ctx, w, k, c, grid, a);  // warm
+        CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+        launch_batch(ctx, w, k, c, grid, a);
+        CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+        CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
       }
-    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (best_ms >= 1e30f) fail(FCU_ERR_UNSUPPORTED, "no batched PCG configuration fits this device");
   return best;
 }
 
@@ -498,7 +628,7 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
   }
   const BatchConfig c = w->cfg[k];
   BatchKernel kern = pick_kernel(mixed, c);
-  const int key = c.vpr * 4096 + c.threads;
+  const int key = (c.vpr * 4096 + c.threads) * 16 + c.cluster;
   if (!w->graph[k] || w->graph_key[k] != key || w->tol_g[k] != tol || w->iters_g[k] != max_iter) {
     if (w->graph[k]) {
       cudaGraphExecDestroy(w->graph[k]);
@@ -507,8 +637,10 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
     const BatchArgs a = make_args(m, w, mixed, tol, max_iter);
     cudaGraph_t g;
     CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int grid = batch_grid(ctx, kern, c, w->nb);
+    if (grid <= 0) fail(FCU_ERR_UNSUPPORTED, "batched PCG configuration does not fit this device");
     try {
-      launch_batch(ctx, w, kern, c, a);
+      launch_batch(ctx, w, kern, c, grid, a);
     } catch (...) {
       cudaStreamEndCapture(ctx->stream, &g);
       throw;
@@ -568,13 +700,13 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
   return worst;
 }
 
-void batch_config(fcu_matrix m, int precision, int* vpr, int* threads) {
+void batch_config(fcu_matrix m, int precision, int* vpr, int* threads, int* cluster) {
   const int k = precision == FCU_MIXED ? 1 : 0;
   if (!m->bws || !m->bws->tuned[k]) {
-    *vpr = 0;
-    *threads = 0;
+    *vpr = *threads = *cluster = 0;
     return;
   }
   *vpr = m->bws->cfg[k].vpr;
   *threads = m->bws->cfg[k].threads;
+  *cluster = m->bws->cfg[k].cluster;
 }

@@ -475,10 +475,11 @@ class Matrix:
         return x, it, rel, st, info
 
     def batch_config(self, precision=FCU_MIXED):
-        """(lanes per row, threads per CTA) the batched solver tuned for this matrix."""
-        v, t = C.c_int(), C.c_int()
-        _L().fcu_batch_config(self.h, precision, C.byref(v), C.byref(t))
-        return v.value, t.value
+        """(lanes per row, threads per CTA, CTAs per instance) the batched solver
+        tuned for this matrix."""
+        v, t, c = C.c_int(), C.c_int(), C.c_int()
+        _L().fcu_batch_config(self.h, precision, C.byref(v), C.byref(t), C.byref(c))
+        return v.value, t.value, c.value
 
 
 # ---------------------------------------------------------------------------

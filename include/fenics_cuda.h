@@ -183,7 +183,8 @@ int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint
  * concatenates the instances' meshes. Every block is solved from x0 = 0 with
  * its own alpha, beta and stopping test ||r_i|| / ||b_i|| < tol, as
  * fcu_pcg would solve it alone (precision FCU_FP64 or FCU_MIXED), in one
- * persistent launch (captured in a CUDA graph, replayed on later calls).
+ * persistent launch (captured in a CUDA graph, replayed on later calls):
+ * each instance is taken by a cluster of 1-8 CTAs, largest instances first.
  * Per-instance iterations, relative residuals and statuses go to the
  * optional host arrays (nb each). Returns FCU_OK when every instance
  * converged, else the first failing status. info: max iterations, total
@@ -191,9 +192,11 @@ int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint
 int fcu_batch_pcg(fcu_ctx ctx, fcu_matrix m, int64_t nb, const int64_t* offsets, const double* b, double* x,
                   double tol, int64_t max_iter, int precision, int64_t* iterations, double* rel_residual,
                   int* status, fcu_solve_info* info);
-/* Lanes per row and threads per CTA the batched solver chose for m and
- * `precision` (0, 0 before its first solve). */
-int fcu_batch_config(fcu_matrix m, int precision, int* lanes_per_row, int* threads_per_cta);
+/* Lanes per row, threads per CTA and CTAs per instance (thread-block
+ * cluster) that the batched solver's tuning chose for m and `precision`
+ * (all 0 before its first solve). */
+int fcu_batch_config(fcu_matrix m, int precision, int* lanes_per_row, int* threads_per_cta,
+                     int* ctas_per_cluster);
 
 /* Allocation-free variant of fcu_solve_csr_cg. No counterpart in the
  * reference: it serves callers that cannot allocate device memory when they

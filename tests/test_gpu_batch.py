@@ -94,8 +94,8 @@ def test_batch_replay_is_bit_identical_and_tuned(fcu, ctx):
         x2, it2, _, st2, _ = M.batch_pcg(offs, b, tol=1e-9, precision=prec)
         assert np.array_equal(x1, x2) and np.array_equal(it1, it2)
         assert np.all(st1 == 0)
-        v, t = M.batch_config(prec)
-        assert v in (2, 4, 8) and t in (256, 512, 1024)
+        v, t, c = M.batch_config(prec)
+        assert v in (1, 2, 4) and t in (512, 1024) and c in (1, 2, 4, 8)
     M.close()
     V.close()
 
