@@ -11,7 +11,12 @@ Dirichlet elimination + mixed PCG to 1e-8, inputs resident in HBM. The
 metric is dofs / step time (DOF/s). Inputs are synthetic (generated meshes).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
-                    [--config c2|c2p|c1|c3|c4|c5]
+                    [--config c2|c2p] [--no-cpu-baseline] [--no-extra]
+
+After the headline measurement, rank 0 of a 1-GPU run also measures the
+other configurations (2D Poisson 64^2, elasticity at 1.57M dofs, P2 Poisson
+with random coefficient, adjoint sensitivities, the 256-problem batch) and
+reports them under "workloads".
 
 --impl reference times the CPU restatement of the reference path (the
 reference itself is Rust and cannot be built here) on the host cores.
@@ -325,6 +330,8 @@ def run_cuda(args, cfg):
                         "build, assembly, body force, Dirichlet, mixed PCG, solution download"},
         "setup_s": t_setup,
     }
+    if rank == 0 and world == 1 and not args.no_extra:
+        res["workloads"] = run_workloads(ctx, stream, peak)
     if rank == 0 and not args.no_cpu_baseline:
         res["cpu_baseline"] = cpu_reference_run(cfg, it_f)
     if dist:
@@ -332,6 +339,199 @@ def run_cuda(args, cfg):
         tdist.destroy_process_group()
     ctx.close()
     return res if rank == 0 else None
+
+
+def _events_ms(stream, fn):
+    """Device time of fn() on `stream` (CUDA events on both sides)."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def _best_ms(stream, fn, k=2):
+    """Best of k device-timed runs (host stalls on a shared host only add time)."""
+    best, out = None, None
+    for _ in range(k):
+        ms, out = _events_ms(stream, fn)
+        best = ms if best is None else min(best, ms)
+    return best, out
+
+
+def run_workloads(ctx, stream, peak):
+    """The scope table's other configurations, each measured on this GPU:
+    C1 (the reference's own CPU-runnable case), C2' (the 1.5M-dof elasticity),
+    C3 (P2 Poisson with a random per-cell coefficient), C4 (adjoint
+    sensitivities) and C5 (the batch of 256 uneven Poisson problems). One
+    warm-up and one timed run each; inputs resident in HBM."""
+    import fenics_cuda as fcu
+    out = {}
+
+    # C1: 2D P1 Poisson 64x64, f = 2 pi^2 sin(pi x) sin(pi y), u = 0, FP64 PCG to 1e-10
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def d64(a):
+        return torch.as_tensor(np.ascontiguousarray(a), device=dev)
+
+    mesh = fcu.unit_square(64, 64)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
+    M = fcu.Matrix(ctx, V)
+    bd = d64(V.boundary_dofs().astype(np.int64))
+    z = torch.zeros(len(bd), dtype=torch.float64, device=dev)
+    b = torch.empty(V.ndofs, dtype=torch.float64, device=dev)
+    x = torch.empty_like(b)
+
+    def c1():
+        M.assemble_stiffness(None)
+        V.rhs_source(fcu.FCU_SRC_SIN_PRODUCT, params=(2 * math.pi ** 2, math.pi), out=b)
+        M.apply_dirichlet(b, bd, z)
+        return M.pcg(b, x=x, tol=1e-10, max_iter=10000, precision=fcu.FCU_FP64)
+    c1()
+    ms, (x, info) = _best_ms(stream, c1)
+    out["c1"] = {"workload": "2D P1 Poisson, unit square 64x64 x 2 triangles (8,192 cells, 4,225 dofs), "
+                             "f = 2 pi^2 sin(pi x) sin(pi y), u = 0 on the boundary, FP64 PCG to 1e-10",
+                 "ms": ms, "dof_per_s": V.ndofs / (ms * 1e-3), "iterations": int(info.iterations),
+                 "u_center": float(x[32 * 65 + 32]), "note": "launch-bound at this size"}
+    del x
+    M.close(); V.close()
+
+    # C2': 3D vector-P1 elasticity 200x50x50 (1,568,403 dofs), mixed vs FP64
+    mesh = fcu.box_beam(4.0, 1.0, 1.0, 200, 50, 50)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+    M = fcu.Matrix(ctx, V)
+    cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+    dofs = d64((3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64))
+    zz = torch.zeros(len(dofs), dtype=torch.float64, device=dev)
+    fb = np.array([0.0, 0.0, -7.8e4])
+    b = torch.empty(V.ndofs, dtype=torch.float64, device=dev)
+    x = torch.empty_like(b)
+    c2p = {"workload": CONFIGS["c2p"]["workload"], "ndofs": V.ndofs}
+    for name, prec in (("mixed", fcu.FCU_MIXED), ("fp64", fcu.FCU_FP64)):
+        def step():
+            M.assemble_elasticity(210e9, 0.3)
+            V.body_force(fb, out=b)
+            M.apply_dirichlet(b, dofs, zz)
+            return M.pcg(b, x=x, tol=1e-8, max_iter=100000, precision=prec)
+        step()
+        ms, (_, info) = _best_ms(stream, step)
+        c2p[name] = {"ms": ms, "solve_ms": info.kernel_ms, "dof_per_s": V.ndofs / (ms * 1e-3),
+                     "iterations": int(info.iterations),
+                     "rel_residual": info.rel_residual}
+    c2p["speedup_mixed_vs_fp64"] = c2p["fp64"]["ms"] / c2p["mixed"]["ms"]
+    out["c2p"] = c2p
+    M.close(); V.close()
+
+    # C3: P2 Poisson on the unit cube 64^3 x 6 tets, kappa = exp(g), g ~ N(0,1) per cell, f = 1, u = 0
+    mesh = fcu.unit_cube(64, 64, 64)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P2)
+    M = fcu.Matrix(ctx, V)
+    kappa = d64(np.exp(np.random.default_rng(3).standard_normal(mesh.nc)))
+    bd = d64(V.boundary_dofs().astype(np.int64))
+    z = torch.zeros(len(bd), dtype=torch.float64, device=dev)
+    b = torch.empty(V.ndofs, dtype=torch.float64, device=dev)
+    x = torch.empty_like(b)
+    c3 = {"workload": "3D P2 Poisson, unit cube 64^3 hexes x 6 tets (1,572,864 tets, 2,146,689 dofs), "
+                      "kappa = exp(g), g ~ N(0,1) i.i.d. per cell (seed 3), f = 1, u = 0 on the boundary, "
+                      "mixed-precision refined PCG to 1e-8 vs FP64 PCG", "ndofs": V.ndofs, "nnz": M.nnz}
+    M.assemble_stiffness(kappa)
+    ms_asm, _ = _best_ms(stream, lambda: M.assemble_stiffness(kappa), k=3)
+    asm_bytes = mesh.nc * (10 * 4 + 8) + mesh.nv * 24 + M.nnz * (8 + 4)
+    c3["assembly"] = {"ms": ms_asm, "gbs": asm_bytes / (ms_asm * 1e-3) / 1e9, "bytes": asm_bytes,
+                      "frac_of_hbm": asm_bytes / (ms_asm * 1e-3) / 1e9 / peak}
+    for name, prec in (("mixed", fcu.FCU_MIXED), ("fp64", fcu.FCU_FP64)):
+        def step():
+            M.assemble_stiffness(kappa)
+            V.rhs_source(fcu.FCU_SRC_CONSTANT, params=(1.0,), out=b)
+            M.apply_dirichlet(b, bd, z)
+            return M.pcg(b, x=x, tol=1e-8, max_iter=100000, precision=prec)
+        step()
+        ms, (_, info) = _best_ms(stream, step)
+        c3[name] = {"ms": ms, "solve_ms": info.kernel_ms, "dof_per_s": V.ndofs / (ms * 1e-3),
+                    "iterations": int(info.iterations),
+                    "rel_residual": info.rel_residual, "replacements": int(info.outer_updates)}
+        sms, sbytes = M.time_spmv(prec, reps=20)
+        c3[name]["spmv"] = {"ms": sms, "gbs": sbytes / (sms * 1e-3) / 1e9,
+                            "frac_of_hbm": sbytes / (sms * 1e-3) / 1e9 / peak}
+    c3["speedup_mixed_vs_fp64"] = c3["fp64"]["ms"] / c3["mixed"]["ms"]
+    out["c3"] = c3
+    M.close(); V.close()
+
+    # C4: adjoint sensitivities, box [0,3]x[0,1]x[0,1] 96x32x32 x 6 tets, E_e = theta_e^3, nu = 0.3
+    L = 3.0
+    mesh = fcu.box_beam(L, 1.0, 1.0, 96, 32, 32)
+    theta = np.random.default_rng(4).uniform(0.01, 1.0, mesh.nc)
+    facets = fcu.facets_on_plane(mesh, 0, L, ctx)
+    cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+    dofs = (3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64)
+    Vt = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+    f = fcu.traction_load(Vt, facets, (0.0, 0.0, -1.0))
+    Vt.close()
+    verts, cells, _ = fcu.extract_boundary_facets(mesh, ctx)
+    tipc = cells[np.all(np.abs(mesh.coords[verts][..., 0] - L) < 1e-9, axis=1)]
+    tipv = np.unique(mesh.cells[tipc])
+    cz = np.zeros(3 * mesh.nv)
+    cz[3 * tipv + 2] = 1.0 / len(tipv)
+    c4 = {"workload": "adjoint sensitivities, 3D vector-P1 elasticity on [0,3]x[0,1]x[0,1], 96x32x32 hexes x 6 "
+                      "tets (589,824 tets, 316,899 dofs), theta ~ U[0.01,1] per cell (seed 4), E = theta^3, "
+                      "nu = 0.3, clamped x = 0, unit downward traction on x = 3; objectives compliance and mean "
+                      "u_z over the vertices of the cells touching x = 3; mixed PCG to 1e-8"}
+    for name, obj in (("compliance", "compliance"), ("tip_uz", cz)):
+        adj = fcu.ElasticityAdjoint(mesh, 0.3, f, dofs, objective=obj, ctx=ctx, tol=1e-8,
+                                    precision=fcu.FCU_MIXED)
+        adj.forward(theta)
+        adj.backward()
+        ms_f, J = _best_ms(stream, lambda: adj.forward(theta))
+        ms_b, g = _best_ms(stream, lambda: adj.backward())
+        c4[name] = {"J": J, "forward_ms": ms_f, "forward_solve_ms": adj.info.kernel_ms, "backward_ms": ms_b,
+                    "forward_iterations": int(adj.info.iterations), "grad_norm": float(np.linalg.norm(g)),
+                    "inputs": "host arrays (theta, load) staged per call"}
+        if name == "compliance":
+            th_d, u_d = d64(theta), d64(adj.u)
+            gd = torch.empty(mesh.nc, dtype=torch.float64, device=dev)
+            ms_g, _ = _best_ms(stream, lambda: adj.V.adjoint_gradient(1.0, 0.3, th_d, u_d, u_d, out=gd), k=3)
+            gbytes = mesh.nc * (16 + 8 + 8) + mesh.nv * (24 + 2 * 24)
+            c4["gradient_kernel"] = {"ms": ms_g, "gbs": gbytes / (ms_g * 1e-3) / 1e9, "bytes": gbytes,
+                                     "frac_of_hbm": gbytes / (ms_g * 1e-3) / 1e9 / peak}
+        else:
+            c4[name]["adjoint_iterations"] = int(adj.adjoint_info.iterations)
+        adj.close()
+    out["c4"] = c4
+
+    # C5: 256 independent 2D P1 Poisson problems on N x N unit squares, N ~ U{32..256}
+    rng = np.random.default_rng(2024)
+    ns = rng.integers(32, 257, size=256)
+    meshes = [fcu.unit_square(int(n), int(n)) for n in ns]
+    kap = np.concatenate([np.exp(rng.standard_normal(m.nc)) for m in meshes])
+    fs = np.concatenate([rng.uniform(-1.0, 1.0, m.nv) for m in meshes])
+    mesh, offs = fcu.concat_meshes(meshes)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
+    M = fcu.Matrix(ctx, V).assemble_stiffness(kap)
+    b = V.rhs_source(fcu.FCU_SRC_NODAL, nodal=fs)
+    bd = V.boundary_dofs()
+    M.apply_dirichlet(b, bd, np.zeros(len(bd)))
+    c5 = {"workload": "256 independent 2D P1 Poisson problems, instance i on an N_i x N_i right-diagonal unit "
+                      "square, N_i ~ U{32..256} (seed 2024), kappa = exp(N(0,1)) per cell, nodal f ~ U[-1,1], "
+                      "u = 0 on each boundary, one persistent graph-captured launch, PCG to 1e-8 per instance",
+          "instances": 256, "ndofs": V.ndofs, "nnz": M.nnz}
+    for name, prec in (("mixed", fcu.FCU_MIXED), ("fp64", fcu.FCU_FP64)):
+        M.batch_pcg(offs, b, tol=1e-8, max_iter=100000, precision=prec)  # tunes, captures the graph
+        ms, (x, it, rel, st, info) = _best_ms(
+            stream, lambda: M.batch_pcg(offs, b, tol=1e-8, max_iter=100000, precision=prec))
+        c5[name] = {"ms": info.kernel_ms, "ms_call": ms, "dof_per_s": V.ndofs / (info.kernel_ms * 1e-3),
+                    "iterations_max": int(it.max()), "iterations_mean": float(it.mean()),
+                    "unconverged": int((st != 0).sum()), "rel_residual_max": float(rel.max()),
+                    "effective_gbs": info.effective_bw_gbps, "frac_of_hbm": info.effective_bw_gbps / peak,
+                    "tuned": dict(zip(("lanes_per_row", "threads_per_cta", "ctas_per_instance"),
+                                      M.batch_config(prec)))}
+    c5["speedup_mixed_vs_fp64"] = c5["fp64"]["ms"] / c5["mixed"]["ms"]
+    out["c5"] = c5
+    M.close(); V.close()
+    return out
 
 
 def run_reference(args, cfg):
@@ -365,6 +565,7 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the C1/C2'/C3/C4/C5 workload measurements")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     res = run_reference(args, cfg) if args.impl == "reference" else run_cuda(args, cfg)

@@ -40,8 +40,16 @@ namespace {
 
 thread_local std::string g_create_err;
 
+// Sets the allocation stream for the duration of a call.
+struct AllocStreamScope {
+  cudaStream_t prev;
+  explicit AllocStreamScope(cudaStream_t s) : prev(fcu_alloc_stream()) { fcu_alloc_stream() = s; }
+  ~AllocStreamScope() { fcu_alloc_stream() = prev; }
+};
+
 template <class F>
 int guarded(fcu_ctx ctx, F&& f) {
+  AllocStreamScope scope(ctx ? ctx->stream : nullptr);
   try {
     if (ctx) CUDA_CHECK(cudaSetDevice(ctx->device));
     f();
@@ -338,6 +346,14 @@ int fcu_ctx_create(int device, fcu_ctx* out) {
     if (e != cudaSuccess) {
       delete c;
       fail(FCU_ERR_CUDA, cudaGetErrorString(e));
+    }
+    // Library buffers come from the device's default memory pool, stream
+    // ordered; keep freed blocks cached in the pool rather than returning
+    // them to the driver at every synchronisation.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     *out = c;
   });

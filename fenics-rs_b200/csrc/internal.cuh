@@ -36,16 +36,24 @@ struct FcuError {
 // Device buffer (RAII, stream-ordered allocation on the context stream)
 // ---------------------------------------------------------------------------
 
+// The stream library allocations are ordered on: the calling context's
+// stream for the duration of a C-ABI call (set by the call wrapper).
+inline cudaStream_t& fcu_alloc_stream() {
+  static thread_local cudaStream_t s = nullptr;
+  return s;
+}
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;  // stream the allocation and its release are ordered on
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
-  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
   DBuf& operator=(DBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) { release(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
     return *this;
   }
   ~DBuf() { release(); }
@@ -53,14 +61,18 @@ struct DBuf {
     if (count == n && p) return;
     release();
     if (count) {
+      s = fcu_alloc_stream();
       // 16 extra bytes so vector loads that round a range outward stay inside.
-      cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T) + 16);
-      if (e != cudaSuccess) { p = nullptr; fail(FCU_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
+      cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T) + 16, s);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        fail(FCU_ERR_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+      }
     }
     n = count;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
     n = 0;
   }

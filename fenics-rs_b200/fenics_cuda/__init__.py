@@ -747,6 +747,81 @@ def solve_poisson_3d(mesh: Mesh, source, boundary_value, tol, max_iter, ctx=None
     return _solve_poisson(mesh, source, boundary_value, tol, max_iter, ctx, precision)
 
 
+def facets_on_plane(mesh: Mesh, axis: int, value: float, ctx: Context | None = None, eps: float = 1e-9):
+    """Boundary facets (vertex triples, outward) whose vertices all lie on the
+    plane x[axis] = value, from extract_boundary_facets."""
+    verts, _, _ = extract_boundary_facets(mesh, ctx)
+    on = np.all(np.abs(mesh.coords[verts][..., axis] - value) < eps, axis=1)
+    return verts[on]
+
+
+def traction_load(V, facets, traction) -> np.ndarray:
+    """assemble_surface_traction_3d (boundary.rs:48-108) for a constant traction."""
+    t = np.asarray(traction, np.float64)
+    tq = np.broadcast_to(t, (len(facets), 3, 3)).copy()
+    return V.surface_traction(np.ascontiguousarray(facets, np.int64), tq)
+
+
+class ElasticityAdjoint:
+    """Forward/backward pair for an objective J(u(theta)) of linear elasticity
+    with per-cell modulus E_e = E0 * theta_e^3: K(theta) u = f with the clamped
+    dofs eliminated. It plays the role of a torch.autograd.Function:
+
+      forward(theta)  assembles K(theta), solves for u and returns J;
+      backward(dJ)    returns dJ * dJ/dtheta, where dJ/dtheta_e =
+                      -lambda_e^T (3 theta_e^2 E0 K_e^1) u_e, K lambda = dJ/du
+                      solved by the same PCG on the same operator (for the
+                      compliance J = f^T u, lambda = u and no second solve),
+                      and the unit-modulus element matrices K_e^1 are
+                      recomputed per cell by the gradient kernel.
+
+    objective: "compliance", or a vector c for J = c^T u (e.g. a mean of
+    displacement components)."""
+
+    def __init__(self, mesh: Mesh, nu, load, clamp_dofs, objective="compliance", ctx=None, E0=1.0, tol=1e-10,
+                 max_iter=100000, precision=FCU_FP64):
+        self.ctx = ctx or default_context()
+        self.mesh, self.nu, self.E0 = mesh, float(nu), float(E0)
+        self.V = FunctionSpace(self.ctx, mesh, FCU_SPACE_P1_VEC3)
+        self.M = Matrix(self.ctx, self.V)
+        self.f = np.ascontiguousarray(load, np.float64)
+        self.dofs = np.ascontiguousarray(clamp_dofs, np.int64)
+        self.objective = objective
+        self.tol, self.max_iter, self.precision = tol, max_iter, precision
+        self.theta = self.u = None
+        self.info = self.adjoint_info = None
+
+    def _solve(self, rhs):
+        b = rhs.copy()
+        b[self.dofs] = 0.0   # the eliminated system's right-hand side (g = 0)
+        x, info = self.M.pcg(b, tol=self.tol, max_iter=self.max_iter, precision=self.precision)
+        return x, info
+
+    def forward(self, theta) -> float:
+        self.theta = np.ascontiguousarray(theta, np.float64)
+        if self.theta.shape != (self.mesh.nc,):
+            raise ValueError("one theta per cell expected")
+        self.M.assemble_elasticity(self.E0, self.nu, self.E0 * self.theta ** 3)
+        b = self.f.copy()
+        self.M.apply_dirichlet(b, self.dofs, np.zeros(len(self.dofs)))
+        self.u, self.info = self.M.pcg(b, tol=self.tol, max_iter=self.max_iter, precision=self.precision)
+        c = self.f if isinstance(self.objective, str) else self.objective
+        return float(np.dot(c, self.u))
+
+    def backward(self, dJ=1.0) -> np.ndarray:
+        if self.u is None:
+            raise RuntimeError("forward first")
+        if isinstance(self.objective, str):
+            lam = self.u
+        else:
+            lam, self.adjoint_info = self._solve(np.ascontiguousarray(self.objective, np.float64))
+        return dJ * self.V.adjoint_gradient(self.E0, self.nu, self.theta, self.u, lam)
+
+    def close(self):
+        self.M.close()
+        self.V.close()
+
+
 @dataclass
 class BatchSolution:
     """Per-instance results of a batched solve."""
