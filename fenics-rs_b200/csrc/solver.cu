@@ -573,13 +573,42 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
                                                    const T* __restrict__ p, const T* __restrict__ ap,
                                                    const double* __restrict__ invd, T* __restrict__ z, CgState* st,
                                                    double* partials) {
+  // x, r, D^-1 and p are final before this kernel starts (their writers
+  // completed before the SpMV it depends on began), so the first two
+  // elements of each thread are fetched before the dependency wait; L2-only
+  // loads keep an early start from reading a stale L1 line.
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  const i64 i0 = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  double xa[2], ra[2], da[2];
+  T pa[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const i64 i = i0 + k * stride;
+    if (i < n) {
+      xa[k] = __ldcg(x + i);
+      ra[k] = __ldcg(r + i);
+      da[k] = __ldcg(invd + i);
+      pa[k] = __ldcg(p + i);
+    }
+  }
   grid_dep_sync();
   if (st->done) return;
   const double alpha = st->alpha;
   double rz = 0.0, rr = 0.0;
-  const i64 stride = (i64)gridDim.x * blockDim.x;
-#pragma unroll 2
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += stride) {
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const i64 i = i0 + k * stride;
+    if (i < n) {
+      x[i] = xa[k] + alpha * (double)pa[k];
+      const double ri = ra[k] - alpha * (double)ap[i];
+      r[i] = ri;
+      const double zi = ri * da[k];
+      z[i] = (T)zi;
+      rz += ri * zi;
+      rr += ri * ri;
+    }
+  }
+  for (i64 i = i0 + 2 * stride; i < n; i += stride) {
     x[i] += alpha * (double)p[i];
     const double ri = r[i] - alpha * (double)ap[i];
     r[i] = ri;
@@ -743,7 +772,10 @@ struct Workspace {
   DBuf<CgState> st;
   CgState* host_st = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  int vpr = 0;    // chosen lanes per row (CSR)
+  int vpr = 0;    // lanes per row of the FP64 CSR kernels (tuned with the FP64 SpMV)
+  int vpr32 = 0;  // lanes per row of the FP32 CSR SpMV (tuned with it)
+  int stages[2] = {3, 3};  // ring depth of the tiled block SpMV: FP64, FP32
+  bool tuned[2] = {false, false};
   int grid = 0;   // row kernels
   int vgrid = 0;  // element-wise vector kernels
   int rgrid = 0;  // residual replacement (rarely does work; small grid keeps its no-op cheap)
@@ -811,6 +843,7 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     CUDA_CHECK(cudaMemsetAsync(w->st.p, 0, sizeof(CgState), ctx->stream));
     CUDA_CHECK(cudaMallocHost(&w->host_st, sizeof(CgState)));
     w->vpr = pick_vpr(m);
+    w->vpr32 = w->vpr;
     w->grid = solver_grid(ctx, n);
     w->vgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms * vec_blocks_per_sm()));
     w->rgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms));
@@ -866,7 +899,7 @@ void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* 
   fcu_ctx ctx = m->ctx;
   const int max_row = m->space ? m->space->max_row : 32;
   const int cap = TILE_ROWS * max_row;
-  const int nstage = 3;
+  const int nstage = w->stages[sizeof(T) == 4 ? 1 : 0];
   const size_t smem = nstage * tile_stage_bytes<T>(cap);
   auto kern = k_spmv_tiled<DIFF, T>;
   static int configured_dev[2][2] = {{-1, -1}, {-1, -1}};
@@ -945,7 +978,7 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       if (m->bs == 3 && use_tiled_spmv())
         launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
       else
-        DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, nr, w->pa32.p, w->ap32.p,
+        DISPATCH_ROWS(m->bs, w->vpr32, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, nr, w->pa32.p, w->ap32.p,
                       w->st.p, w->partials.p);
       launch_pdl(ctx, k_update<float>, w->vgrid, n, w->x.p, w->r.p, w->pa32.p, w->ap32.p, w->invd.p, w->z32.p,
                  w->st.p, w->partials.p);
@@ -964,7 +997,7 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
   } else {
     float* pold = parity ? w->pb32.p : w->pa32.p;
     float* pnew = parity ? w->pa32.p : w->pb32.p;
-    DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_DIR32, m->row_ptr, m->col_idx, m->val32.p, nr, w->z32.p, pold, pnew,
+    DISPATCH_ROWS(m->bs, w->vpr32, g, K_SPMV_DIR32, m->row_ptr, m->col_idx, m->val32.p, nr, w->z32.p, pold, pnew,
                   w->ap32.p, w->st.p, w->partials.p);
     launch_pdl(ctx, k_update<float>, g, n, w->x.p, w->r.p, pnew, w->ap32.p, w->invd.p, w->z32.p, w->st.p,
                w->partials.p);
@@ -1037,6 +1070,8 @@ void build_rowsum32(fcu_matrix m) {
   LAUNCH_CHECK(ctx);
 }
 
+void tune_spmv(fcu_matrix m, Workspace* w, bool mixed);
+
 // Core PCG driver on device buffers: b_dev, x0_dev (nullable) -> x_dev.
 // inv_diag_dev (nullable) overrides the matrix diagonal (solve_csr_cg_gpu).
 int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_dev, double tol, i64 max_iter,
@@ -1055,6 +1090,7 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
                                                ctx->stream));
   else ensure_inv_diag(m, w);
   if (mixed) build_rowsum32(m);
+  tune_spmv(m, w, mixed);  // first solve in this precision only
 
   CgState init{};
   init.tol = tol;
@@ -1122,16 +1158,21 @@ void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev) {
   DISPATCH_ROWS(m->bs, vpr, g, K_PLAIN, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, x_dev, y_dev);
 }
 
-// Average time of the PCG SpMV kernel over `reps` launches (diagnostics).
-void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes) {
+// --- SpMV shape tuning --------------------------------------------------------
+// The first solve of a matrix in a precision times the candidate shapes of
+// its SpMV on the matrix itself and keeps the fastest: lanes per row
+// {4, 8, 16, 32} for CSR, ring depth {2, 3, 4} for the tiled 3x3-block
+// kernel. FCU_TUNE=0 keeps the defaults (CSR lanes by mean row length,
+// three stages).
+
+// Solver state and operand for SpMV timing: every launch does the full
+// product (no convergence or breakdown exit).
+void spmv_timing_state(fcu_matrix m, Workspace* w, bool mixed) {
   fcu_ctx ctx = m->ctx;
-  const bool mixed = precision == FCU_MIXED;
-  Workspace* w = ensure_ws(m, mixed);
-  if (mixed) build_rowsum32(m);
   CgState init{};
   init.rz = 1.0;
   init.beta = 0.5;
-  init.gpu_semantics = 1;  // no breakdown exit: every launch does the full product
+  init.gpu_semantics = 1;
   *w->host_st = init;
   CUDA_CHECK(cudaMemcpyAsync(w->st.p, w->host_st, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
   const i64 n = m->n;
@@ -1143,34 +1184,107 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
     CUDA_CHECK(cudaMemsetAsync(w->z64.p, 0x3f, n * sizeof(double), ctx->stream));
     CUDA_CHECK(cudaMemsetAsync(w->pa64.p, 0x3f, n * sizeof(double), ctx->stream));
   }
+}
+
+// One launch of the PCG's SpMV (Ap = A p) with the workspace's shape.
+void enqueue_spmv(fcu_matrix m, Workspace* w, bool mixed) {
+  fcu_ctx ctx = m->ctx;
   const int g = w->grid;
+  if (mixed) {
+    if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+    else
+      DISPATCH_ROWS(m->bs, w->vpr32, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, m->nnodes, w->pa32.p,
+                    w->ap32.p, w->st.p, w->partials.p);
+  } else {
+    if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+    else
+      DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->pa64.p,
+                    w->ap64.p, w->st.p, w->partials.p);
+  }
+}
+
+// Mean device time of `reps` back-to-back SpMV launches (ms).
+double time_spmv_launches(fcu_matrix m, Workspace* w, bool mixed, int reps) {
+  fcu_ctx ctx = m->ctx;
   cudaEvent_t e0, e1;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
   CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
-  for (int r = 0; r < reps; ++r) {
-    if (mixed) {
-      if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
-      else
-        DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, m->nnodes, w->pa32.p,
-                      w->ap32.p, w->st.p, w->partials.p);
-    } else {
-      if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
-      else
-        DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->pa64.p,
-                      w->ap64.p, w->st.p, w->partials.p);
-    }
-  }
+  for (int r = 0; r < reps; ++r) enqueue_spmv(m, w, mixed);
   CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
   CUDA_CHECK(cudaEventSynchronize(e1));
   float t = 0.f;
   CUDA_CHECK(cudaEventElapsedTime(&t, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  *ms = reps > 0 ? (double)t / reps : 0.0;
+  return reps > 0 ? (double)t / reps : 0.0;
+}
+
+bool tuning_enabled() {
+  static int v = [] {
+    const char* e = getenv("FCU_TUNE");
+    return e ? atoi(e) : 1;
+  }();
+  return v != 0;
+}
+
+void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
+  const int k = mixed ? 1 : 0;
+  if (w->tuned[k]) return;
+  w->tuned[k] = true;
+  if (!tuning_enabled()) return;
+  fcu_ctx ctx = m->ctx;
+  spmv_timing_state(m, w, mixed);
+  auto trial = [&]() {
+    enqueue_spmv(m, w, mixed);  // warm
+    return time_spmv_launches(m, w, mixed, 8);
+  };
+  if (m->bs == 3 && use_tiled_spmv()) {
+    int optin = 0;
+    CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const int max_row = m->space ? m->space->max_row : 32;
+    const size_t stage = mixed ? tile_stage_bytes<float>(TILE_ROWS * max_row)
+                               : tile_stage_bytes<double>(TILE_ROWS * max_row);
+    int best = w->stages[k];
+    double best_ms = 1e30;
+    for (int ns = 2; ns <= MAX_STAGES; ++ns) {
+      if (ns * stage + 1024 > (size_t)optin) continue;
+      w->stages[k] = ns;
+      const double ms = trial();
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = ns;
+      }
+    }
+    w->stages[k] = best;
+  } else {
+    int& v = mixed ? w->vpr32 : w->vpr;
+    int best = v;
+    double best_ms = 1e30;
+    for (int c : {4, 8, 16, 32}) {
+      v = c;
+      const double ms = trial();
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+    v = best;
+  }
+}
+
+// Average time of the PCG SpMV kernel over `reps` launches (diagnostics),
+// with the shape the solver uses.
+void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes) {
+  const bool mixed = precision == FCU_MIXED;
+  Workspace* w = ensure_ws(m, mixed);
+  if (mixed) build_rowsum32(m);
+  tune_spmv(m, w, mixed);
+  spmv_timing_state(m, w, mixed);
+  *ms = time_spmv_launches(m, w, mixed, reps);
   const double bs2 = (double)m->bs * m->bs;
   const double wv = mixed ? 4.0 : 8.0;
-  *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)n * wv;
+  *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
 }
 
 // ---------------------------------------------------------------------------
