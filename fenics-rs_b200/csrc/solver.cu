@@ -51,6 +51,7 @@ struct CgState {
   double rz, alpha, beta, bnorm, tol, rr, maxr, delta;
   long long iter, max_iter, updates;
   int done, status, do_update;
+  int pause;  // mixed: a replacement is due; the rest of the graph replay is skipped
   int gpu_semantics;  // solve_csr_cg_gpu: no breakdown test, beta guard, Ok at limit
   int fault;          // a bounded wait in a kernel gave up (reported as FCU_ERR_CUDA)
   // arrival counters of the grid reductions: 32 group counters + 1 top counter
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(VBLOCK) k_spmv_dir(const int* __restrict__ rp,
                                                      const T* __restrict__ pold, T* __restrict__ pnew,
                                                      T* __restrict__ ap, CgState* st, double* partials) {
   grid_dep_sync();
-  if (st->done) return;
+  if (st->done || st->pause) return;
   const XDirection<T> dir{z, pold, (T)st->beta};
   EmitAp<BS, T> em{dir, pnew, ap};
   constexpr bool DIFF = sizeof(T) == 4;
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(VBLOCK) k_spmv_ap(const int* __restrict__ rp, 
                                                     const T* __restrict__ val, i64 nrows, const T* __restrict__ p,
                                                     T* __restrict__ ap, CgState* st, double* partials) {
   grid_dep_sync();
-  if (st->done) return;
+  if (st->done || st->pause) return;
   EmitApPlain<BS, T> em{p, ap};
   constexpr bool DIFF = sizeof(T) == 4;
   spmv_rows<BS, VPR, DIFF, T>(rp, ci, val, nrows, XPlain<T>{p}, em);
@@ -322,7 +323,7 @@ template <class T>
 __global__ void __launch_bounds__(VBLOCK) k_direction(i64 n, T* __restrict__ p, const T* __restrict__ z,
                                                       const CgState* st) {
   grid_dep_sync();
-  if (st->done) return;
+  if (st->done || st->pause) return;
   const T beta = (T)st->beta;
   for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
     p[i] = z[i] + beta * p[i];
@@ -407,14 +408,33 @@ constexpr int SPMV_CONSUMER_WARPS = 16;
 constexpr int SPMV_THREADS = 32 * (SPMV_CONSUMER_WARPS + 1);
 constexpr int MAX_STAGES = 4;
 
+// Output of the tiled kernel: Ap for one scalar row, and p.Ap accumulated
+// from the row's own operand value (already in registers).
+template <class T>
+struct EmitApOwn {
+  T* ap;
+  double dot = 0.0;
+  __device__ __forceinline__ void operator()(i64 node, int a, T s, T own) {
+    ap[node * 3 + a] = s;
+    dot += (double)own * (double)s;
+  }
+};
+
+// The matrix does not depend on the preceding kernel, so the ring's first
+// stages are issued before the programmatic dependency wait and overlap the
+// predecessor's tail; the producer warp's lanes fetch the row-pointer bounds
+// of the CTA's next 32 tiles in one round of loads. Returns false, having
+// computed nothing, when the solver state says the solve is over.
 template <bool DIFF, class T, class GX, class Emit>
-__device__ __forceinline__ void bsr3_tiled_rows(const int* __restrict__ rp, const int* __restrict__ ci,
+__device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, const int* __restrict__ ci,
                                                 const T* __restrict__ val, i64 nrows, int cap_blocks, int nstage,
-                                                const GX& gx, Emit& emit, int* fault) {
+                                                const GX& gx, Emit& emit, CgState* st) {
   extern __shared__ __align__(128) unsigned char tile_smem[];
   __shared__ unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
   const size_t stage_bytes = tile_stage_bytes<T>(cap_blocks);
   const i64 ntiles = (nrows + TILE_ROWS - 1) / TILE_ROWS;
+  const i64 G = gridDim.x;
+  const int mytiles = blockIdx.x < ntiles ? (int)((ntiles - blockIdx.x + G - 1) / G) : 0;
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
@@ -426,59 +446,85 @@ __device__ __forceinline__ void bsr3_tiled_rows(const int* __restrict__ rp, cons
   }
   __syncthreads();
 
-  if (warp == 0) {
-    if (lane == 0) {
-      int k = 0;
-      bool ok = true;
-      for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
-        const int s = k % nstage;
-        const int use = k / nstage;
-        if (use > 0 && !mbar_wait(&empty[s], (unsigned)((use - 1) & 1))) {
-          atomicExch(fault, 1);
-          ok = false;
-          break;
-        }
-        unsigned char* base = tile_smem + s * stage_bytes;
-        TileHeader* h = reinterpret_cast<TileHeader*>(base);
-        unsigned char* rps = base + align128(sizeof(TileHeader));
-        unsigned char* cs = rps + align128((TILE_ROWS + 1) * 4 + 16);
-        unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
-        const i64 r0 = t * TILE_ROWS;
-        const int rows = (int)min((i64)TILE_ROWS, nrows - r0);
-        const int b0 = rp[r0], b1 = rp[r0 + rows];
-        const unsigned rp_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);
-        const uintptr_t c_lo = reinterpret_cast<uintptr_t>(ci + b0) & ~(uintptr_t)15;
-        const uintptr_t c_hi = (reinterpret_cast<uintptr_t>(ci + b1) + 15) & ~(uintptr_t)15;
-        const uintptr_t v_lo = reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) & ~(uintptr_t)15;
-        const uintptr_t v_hi = (reinterpret_cast<uintptr_t>(val + 9 * (i64)b1) + 15) & ~(uintptr_t)15;
-        h->b0 = b0;
-        h->rows = rows;
-        h->col_off = (int)(reinterpret_cast<uintptr_t>(ci + b0) - c_lo);
-        h->val_off = (int)(reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) - v_lo);
-        const unsigned cb = (unsigned)(c_hi - c_lo), vb = (unsigned)(v_hi - v_lo);
-        fence_proxy_async();
-        mbar_arrive_expect_tx(&full[s], rp_bytes + cb + vb);
-        bulk_load(rps, rp + r0, rp_bytes, &full[s]);
-        if (cb) bulk_load(cs, reinterpret_cast<const void*>(c_lo), cb, &full[s]);
-        if (vb) bulk_load(vs, reinterpret_cast<const void*>(v_lo), vb, &full[s]);
-      }
-      if (!ok) {
-        // let copies already issued land before the CTA exits (bounded)
-        for (int s = 0; s < nstage; ++s) mbar_wait(&full[s], 0);
-      }
+  // producer (warp 0): lane j holds the block bounds of tile k0 + j
+  int pb0 = 0, pb1 = 0;
+  auto load_desc = [&](int k0) {
+    const i64 t = blockIdx.x + (i64)(k0 + lane) * G;
+    if (t < ntiles) {
+      const i64 r0 = t * TILE_ROWS;
+      pb0 = rp[r0];
+      pb1 = rp[min(r0 + TILE_ROWS, nrows)];
     }
-    return;
+  };
+  auto issue = [&](int k) {
+    const int b0 = __shfl_sync(FULL, pb0, k & 31), b1 = __shfl_sync(FULL, pb1, k & 31);
+    if (lane == 0) {
+      const int s = k % nstage;
+      unsigned char* base = tile_smem + s * stage_bytes;
+      TileHeader* h = reinterpret_cast<TileHeader*>(base);
+      unsigned char* rps = base + align128(sizeof(TileHeader));
+      unsigned char* cs = rps + align128((TILE_ROWS + 1) * 4 + 16);
+      unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
+      const i64 r0 = (blockIdx.x + (i64)k * G) * TILE_ROWS;
+      const int rows = (int)min((i64)TILE_ROWS, nrows - r0);
+      const unsigned rp_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);
+      const uintptr_t c_lo = reinterpret_cast<uintptr_t>(ci + b0) & ~(uintptr_t)15;
+      const uintptr_t c_hi = (reinterpret_cast<uintptr_t>(ci + b1) + 15) & ~(uintptr_t)15;
+      const uintptr_t v_lo = reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) & ~(uintptr_t)15;
+      const uintptr_t v_hi = (reinterpret_cast<uintptr_t>(val + 9 * (i64)b1) + 15) & ~(uintptr_t)15;
+      h->b0 = b0;
+      h->rows = rows;
+      h->col_off = (int)(reinterpret_cast<uintptr_t>(ci + b0) - c_lo);
+      h->val_off = (int)(reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) - v_lo);
+      const unsigned cb = (unsigned)(c_hi - c_lo), vb = (unsigned)(v_hi - v_lo);
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&full[s], rp_bytes + cb + vb);
+      bulk_load(rps, rp + r0, rp_bytes, &full[s]);
+      if (cb) bulk_load(cs, reinterpret_cast<const void*>(c_lo), cb, &full[s]);
+      if (vb) bulk_load(vs, reinterpret_cast<const void*>(v_lo), vb, &full[s]);
+    }
+  };
+
+  // before the dependency wait: fill the ring (no stage has been used yet)
+  const int prologue = min(nstage, mytiles);
+  if (warp == 0) {
+    load_desc(0);
+    for (int k = 0; k < prologue; ++k) issue(k);
+  }
+  grid_dep_sync();
+  if (st->done || st->pause) {
+    // the copies already issued land before the CTA exits (bounded)
+    if (warp == 0 && lane == 0)
+      for (int s = 0; s < prologue; ++s) mbar_wait(&full[s], 0);
+    return false;
   }
 
-  // consumers
+  if (warp == 0) {
+    bool ok = true;
+    for (int k = prologue; k < mytiles; ++k) {
+      if ((k & 31) == 0) load_desc(k);
+      if (lane == 0) ok = mbar_wait(&empty[k % nstage], (unsigned)(((k / nstage) - 1) & 1));
+      if (!__shfl_sync(FULL, ok ? 1 : 0, 0)) {
+        if (lane == 0) {
+          atomicExch(&st->fault, 1);
+          // copies in flight land before the CTA exits (bounded waits)
+          for (int q = max(0, k - nstage); q < k; ++q) mbar_wait(&full[q % nstage], (unsigned)((q / nstage) & 1));
+        }
+        break;
+      }
+      issue(k);
+    }
+    return true;
+  }
+
+  // consumers: half-warp per block row; lane `sub` handles blocks sub,
+  // sub + 16, ... of it
   const int sub = lane & 15;
   const int row_in_tile = (warp - 1) * 2 + (lane >> 4);
-  int k = 0;
-  for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+  for (int k = 0; k < mytiles; ++k) {
     const int s = k % nstage;
-    const int use = k / nstage;
-    if (!mbar_wait(&full[s], (unsigned)(use & 1))) {
-      if (lane == 0) atomicExch(fault, 1);
+    if (!mbar_wait(&full[s], (unsigned)((k / nstage) & 1))) {
+      if (lane == 0) atomicExch(&st->fault, 1);
       break;
     }
     unsigned char* base = tile_smem + s * stage_bytes;
@@ -489,16 +535,14 @@ __device__ __forceinline__ void bsr3_tiled_rows(const int* __restrict__ rp, cons
     const int* cis = reinterpret_cast<const int*>(cs + h->col_off);
     const T* vls = reinterpret_cast<const T*>(vs + h->val_off);
     const int b0 = h->b0;
-    const i64 row = t * TILE_ROWS + row_in_tile;
+    const i64 row = (blockIdx.x + (i64)k * G) * TILE_ROWS + row_in_tile;
     const bool valid = row_in_tile < h->rows;
     T a0 = T(0), a1 = T(0), a2 = T(0);
+    T x0 = T(0), x1 = T(0), x2 = T(0);
     if (valid) {
-      T x0 = T(0), x1 = T(0), x2 = T(0);
-      if (DIFF) {
-        x0 = gx(3 * row);
-        x1 = gx(3 * row + 1);
-        x2 = gx(3 * row + 2);
-      }
+      x0 = gx(3 * row);
+      x1 = gx(3 * row + 1);
+      x2 = gx(3 * row + 2);
       const int kb1 = rps[row_in_tile + 1] - b0;
       for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += 16) {
         const int c = cis[kb];
@@ -525,19 +569,20 @@ __device__ __forceinline__ void bsr3_tiled_rows(const int* __restrict__ rp, cons
       a1 += __shfl_xor_sync(FULL, a1, o);
       a2 += __shfl_xor_sync(FULL, a2, o);
     }
-    if (valid && sub < 3) emit(row, sub, sub == 0 ? a0 : (sub == 1 ? a1 : a2));
+    if (valid && sub < 3)
+      emit(row, sub, sub == 0 ? a0 : (sub == 1 ? a1 : a2), sub == 0 ? x0 : (sub == 1 ? x1 : x2));
   }
+  return true;
 }
 
 template <int DIFF, class T>
-__global__ void __launch_bounds__(SPMV_THREADS) k_spmv_tiled(const int* __restrict__ rp, const int* __restrict__ ci,
+__global__ void __launch_bounds__(SPMV_THREADS)
+    k_spmv_tiled(const int* __restrict__ rp, const int* __restrict__ ci,
                                                             const T* __restrict__ val, i64 nrows, int cap_blocks,
                                                             int nstage, const T* __restrict__ p, T* __restrict__ ap,
                                                             CgState* st, double* partials) {
-  grid_dep_sync();
-  if (st->done) return;
-  EmitApPlain<3, T> em{p, ap};
-  bsr3_tiled_rows<DIFF != 0, T>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, &st->fault);
+  EmitApOwn<T> em{ap};
+  if (!bsr3_tiled_rows<DIFF != 0, T>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, st)) return;
   double v[1] = {em.dot}, tot[1];
   if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) {
     if (st->fault) {
@@ -592,7 +637,7 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
     }
   }
   grid_dep_sync();
-  if (st->done) return;
+  if (st->done || st->pause) return;
   const double alpha = st->alpha;
   double rz = 0.0, rr = 0.0;
 #pragma unroll
@@ -629,6 +674,7 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
       const double res = sqrt(tot[1]);
       const double rel = st->bnorm > 0.0 ? res / st->bnorm : res;
       st->do_update = (rel < st->tol || res < st->delta * st->maxr) ? 1 : 0;
+      st->pause = st->do_update;  // the host runs the replacement next
       if (!st->do_update) {
         if (st->iter >= st->max_iter) {
           st->done = 1;
@@ -705,6 +751,8 @@ __global__ void __launch_bounds__(VBLOCK) k_mx_replace(const int* __restrict__ r
   double v[2] = {em.rz, em.rr}, tot[2];
   if (grid_reduce<2>(v, partials, st->ticket[2], tot) && threadIdx.x == 0) {
     st->updates += 1;
+    st->do_update = 0;
+    st->pause = 0;
     st->rr = tot[1];
     const double res = sqrt(tot[1]);
     const double rel = st->bnorm > 0.0 ? res / st->bnorm : res;
@@ -778,7 +826,6 @@ struct Workspace {
   bool tuned[2] = {false, false};
   int grid = 0;   // row kernels
   int vgrid = 0;  // element-wise vector kernels
-  int rgrid = 0;  // residual replacement (rarely does work; small grid keeps its no-op cheap)
   ~Workspace() {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
@@ -846,7 +893,6 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     w->vpr32 = w->vpr;
     w->grid = solver_grid(ctx, n);
     w->vgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms * vec_blocks_per_sm()));
-    w->rgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms));
   }
   Workspace* w = m->ws;
   if (!mixed && !w->z64.p) {
@@ -982,8 +1028,6 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
                       w->st.p, w->partials.p);
       launch_pdl(ctx, k_update<float>, w->vgrid, n, w->x.p, w->r.p, w->pa32.p, w->ap32.p, w->invd.p, w->z32.p,
                  w->st.p, w->partials.p);
-      DISPATCH_ROWS(m->bs, w->vpr, w->rgrid, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p,
-                    w->invd.p, w->r.p, w->z32.p, w->st.p, w->partials.p);
     }
     return;
   }
@@ -1001,12 +1045,10 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
                   w->ap32.p, w->st.p, w->partials.p);
     launch_pdl(ctx, k_update<float>, g, n, w->x.p, w->r.p, pnew, w->ap32.p, w->invd.p, w->z32.p, w->st.p,
                w->partials.p);
-    DISPATCH_ROWS(m->bs, w->vpr, g, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
-                  w->r.p, w->z32.p, w->st.p, w->partials.p);
   }
 }
 
-int launches_per_iteration(bool mixed) { return (mixed ? 3 : 2) + (fuse_direction() ? 0 : 1); }
+int launches_per_iteration() { return fuse_direction() ? 2 : 3; }
 
 cudaGraphExec_t get_graph(fcu_matrix m, Workspace* w, bool mixed) {
   fcu_ctx ctx = m->ctx;
@@ -1119,13 +1161,25 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
     w->host_st->status = FCU_OK;
     w->host_st->iter = 0;
   } else if (!w->host_st->done && max_iter > 0) {
+    // Replays of CHUNK iterations. In the mixed solve an iteration that
+    // flags a residual replacement pauses the rest of its replay, and the
+    // replacement runs here before the next replay, right after that
+    // iteration. Every replay completes at least one iteration, and the
+    // iteration limit is enforced on the device, so the loop ends.
     cudaGraphExec_t ge = get_graph(m, w, mixed);
-    for (i64 launched = 0; launched < max_iter + CHUNK; launched += CHUNK) {
+    for (i64 rep = 0; rep <= max_iter + 1; ++rep) {
       CUDA_CHECK(cudaGraphLaunch(ge, ctx->stream));
-      ctx->launches += (i64)CHUNK * launches_per_iteration(mixed);
+      ctx->launches += (i64)CHUNK * launches_per_iteration();
       CUDA_CHECK(cudaMemcpyAsync(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
       if (w->host_st->done) break;
+      if (mixed && w->host_st->do_update) {
+        DISPATCH_ROWS(m->bs, w->vpr, g, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
+                      w->r.p, w->z32.p, w->st.p, w->partials.p);
+        CUDA_CHECK(cudaMemcpyAsync(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+        if (w->host_st->done) break;
+      }
     }
   } else if (!w->host_st->done) {
     w->host_st->status = gpu_semantics ? FCU_OK : FCU_ERR_NO_CONVERGENCE;
