@@ -858,6 +858,61 @@ def solve_poisson_batch(meshes, kappas=None, nodal_sources=None, tol=1e-8, max_i
     return BatchSolution([x[offs[i]:offs[i + 1]] for i in range(len(meshes))], it, rel, st, info, offs)
 
 
+def batch_costs(meshes) -> np.ndarray:
+    """Estimated solve cost of each instance: (cells + vertices) * sqrt(vertices),
+    i.e. work per iteration times the iteration growth of 2D Poisson."""
+    return np.array([(m.nc + m.nv) * np.sqrt(max(m.nv, 1)) for m in meshes], np.float64)
+
+
+def shard_instances(costs, world: int) -> list:
+    """Split instances over `world` ranks, largest first onto the least loaded
+    rank (ties to the lower rank). Deterministic, so every rank computes the
+    same assignment without communicating. Returns one ascending index list
+    per rank."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    costs = np.asarray(costs, np.float64)
+    load = np.zeros(world)
+    shards = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = int(np.argmin(load))
+        shards[r].append(i)
+        load[r] += costs[i]
+    return [sorted(sh) for sh in shards]
+
+
+def solve_poisson_batch_sharded(meshes, kappas=None, nodal_sources=None, tol=1e-8, max_iter=100000, ctx=None,
+                                precision=FCU_MIXED, rank=0, world=1, group=None, solve=None):
+    """The batch split over ranks (one GPU each): rank r solves its shard with
+    the batched solver, then every rank receives every instance's result
+    through one all_gather of Python objects. The solve itself exchanges
+    nothing. `solve` replaces solve_poisson_batch (same arguments), e.g. for
+    host-side tests. Returns (solutions, iterations, rel_residuals, statuses)
+    in instance order."""
+    meshes = list(meshes)
+    mine = shard_instances(batch_costs(meshes), world)[rank]
+    solve = solve or (lambda ms, ks, fs: solve_poisson_batch(ms, ks, fs, tol=tol, max_iter=max_iter, ctx=ctx,
+                                                              precision=precision, raise_on_error=False))
+    local = {}
+    if mine:
+        res = solve([meshes[i] for i in mine], None if kappas is None else [kappas[i] for i in mine],
+                    None if nodal_sources is None else [nodal_sources[i] for i in mine])
+        for j, i in enumerate(mine):
+            local[i] = (np.asarray(res.solutions[j]), int(res.iterations[j]), float(res.rel_residuals[j]),
+                        int(res.statuses[j]))
+    if world > 1:
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, local, group=group)
+        merged = {}
+        for part in parts:
+            merged.update(part)
+        local = merged
+    n = len(meshes)
+    return ([local[i][0] for i in range(n)], np.array([local[i][1] for i in range(n)], np.int64),
+            np.array([local[i][2] for i in range(n)]), np.array([local[i][3] for i in range(n)], np.int32))
+
+
 @dataclass
 class ElasticitySolution:
     """elasticity_solver.rs:13-29 (displacements, iterations, residual)."""
