@@ -98,12 +98,33 @@ __device__ __forceinline__ void p2_metric(const double* __restrict__ X, const in
     S[m] = (g.G[0][D[m]] * g.G[0][E[m]] + g.G[1][D[m]] * g.G[1][E[m]] + g.G[2][D[m]] * g.G[2][E[m]]) * s;
 }
 
+// P2 metric records. A P2 cell feeds ten rows of the row-gather assembly,
+// so its scaled metric (p2_metric) is computed once per assembly call by a
+// cell-parallel pass, and the row kernel reads one 64-byte record per
+// contribution instead of recomputing the geometry from the connectivity and
+// coordinates (three dependent gathers). The record holds exactly the values
+// p2_metric computes: S[0..5], then two pad entries (16-byte aligned, read
+// with 128-bit loads).
+constexpr int P2_GEO = 8;
+
+__global__ void k_p2_metric_records(const int* __restrict__ cn, const double* __restrict__ X,
+                                    const double* __restrict__ coef, i64 nc, double* __restrict__ geo) {
+  for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
+    double S[P2_GEO];
+    p2_metric(X, cn, (int)c, coef ? coef[c] : 1.0, S);
+    S[6] = S[7] = 0.0;
+    double2* o = reinterpret_cast<double2*>(geo + c * P2_GEO);
+#pragma unroll
+    for (int q = 0; q < P2_GEO / 2; ++q) o[q] = make_double2(S[2 * q], S[2 * q + 1]);
+  }
+}
+
 template <int K, int DIM, bool IS_P2>
 __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
     const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
-    const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ coef, i64 nrows,
-    double* __restrict__ v64, float* __restrict__ v32) {
+    const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ coef,
+    const double* __restrict__ p2geo, i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
   constexpr int KS = odd_stride(K);
   __shared__ double stage_all[WARPS][32][KS];
   __shared__ unsigned short ent_all[WARPS][32 * K];
@@ -143,7 +164,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
         if (IS_P2) {
           if (t < nct) {
             int cc = contrib[cs + t];
-            p2_metric(X, cn, cc >> 4, coef ? coef[cc >> 4] : 1.0, metric_all[wib][lane]);
+            const double2* g = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const double2 v = g[q];
+              metric_all[wib][lane][2 * q] = v.x;
+              metric_all[wib][lane][2 * q + 1] = v.y;
+            }
             sa_all[wib][lane] = cc & 15;
           }
           __syncwarp();
@@ -478,17 +505,22 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
   const int nb = assembly_blocks(ctx, s->nnodes);
   if (s->kind == FCU_SPACE_P2) {
     ensure_p2_tables(ctx);
+    DBuf<double> geo;
+    geo.alloc((size_t)me->nc * P2_GEO);
+    k_p2_metric_records<<<grid_for(me->nc, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
+        s->cell_nodes.p, me->coords.p, coef_dev, me->nc, geo.p);
+    LAUNCH_CHECK(ctx);
     k_assemble_scalar<10, 3, true><<<nb, WARPS * 32, 0, ctx->stream>>>(
         s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
-        coef_dev, s->nnodes, m->val64.p, m->val32.p);
+        coef_dev, geo.p, s->nnodes, m->val64.p, m->val32.p);
   } else if (me->dim == 3) {
     k_assemble_scalar<4, 3, false><<<nb, WARPS * 32, 0, ctx->stream>>>(
         s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
-        coef_dev, s->nnodes, m->val64.p, m->val32.p);
+        coef_dev, nullptr, s->nnodes, m->val64.p, m->val32.p);
   } else {
     k_assemble_scalar<3, 2, false><<<nb, WARPS * 32, 0, ctx->stream>>>(
         s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
-        coef_dev, s->nnodes, m->val64.p, m->val32.p);
+        coef_dev, nullptr, s->nnodes, m->val64.p, m->val32.p);
   }
   LAUNCH_CHECK(ctx);
 }

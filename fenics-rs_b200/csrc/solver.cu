@@ -892,7 +892,13 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     w->vpr = pick_vpr(m);
     w->vpr32 = w->vpr;
     w->grid = solver_grid(ctx, n);
-    w->vgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms * vec_blocks_per_sm()));
+    // one wave of the update kernel (its first two elements per thread are
+    // fetched before the dependency wait, which only resident blocks do early)
+    int occ64 = 0, occ32 = 0;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, k_update<double>, VBLOCK, 0));
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_update<float>, VBLOCK, 0));
+    const int vbpsm = std::max(1, std::min(vec_blocks_per_sm(), std::min(occ64, occ32)));
+    w->vgrid = (int)std::max<i64>(1, std::min<i64>((n + VBLOCK - 1) / VBLOCK, (i64)ctx->num_sms * vbpsm));
   }
   Workspace* w = m->ws;
   if (!mixed && !w->z64.p) {
