@@ -423,6 +423,20 @@ def run_workloads(ctx, stream, peak):
                      "iterations": int(info.iterations),
                      "rel_residual": info.rel_residual}
     c2p["speedup_mixed_vs_fp64"] = c2p["fp64"]["ms"] / c2p["mixed"]["ms"]
+    # stress recovery on the solution (compute_element_stresses / compute_vertex_von_mises)
+    cvm = torch.empty(mesh.nc, dtype=torch.float64, device=dev)
+    vvm = torch.empty(mesh.nv, dtype=torch.float64, device=dev)
+    V.element_stresses(210e9, 0.3, x, von_mises=cvm)
+    ms_s, _ = _best_ms(stream, lambda: V.element_stresses(210e9, 0.3, x, von_mises=cvm), k=3)
+    ms_v, _ = _best_ms(stream, lambda: V.vertex_von_mises(cvm, out=vvm), k=3)
+    sbytes = mesh.nc * (16 + 8) + mesh.nv * (24 + 24)
+    vbytes = mesh.nc * (16 + 16 + 8) + mesh.nv * (24 + 8)
+    c2p["stress_recovery"] = {
+        "element_von_mises": {"ms": ms_s, "gbs": sbytes / (ms_s * 1e-3) / 1e9, "bytes": sbytes,
+                              "frac_of_hbm": sbytes / (ms_s * 1e-3) / 1e9 / peak},
+        "vertex_von_mises": {"ms": ms_v, "gbs": vbytes / (ms_v * 1e-3) / 1e9, "bytes": vbytes,
+                             "frac_of_hbm": vbytes / (ms_v * 1e-3) / 1e9 / peak},
+        "max_vertex_von_mises_pa": float(vvm.max())}
     out["c2p"] = c2p
     M.close(); V.close()
 

@@ -32,6 +32,9 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
                    i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
                    fcu_solve_info* info);
 void batch_config(fcu_matrix m, int precision, int* vpr, int* threads, int* cluster);
+void element_stresses_impl(fcu_space s, double lam, double mu, const double* u_dev, double* stress, double* strain,
+                           double* vm, double* trace);
+void vertex_von_mises_impl(fcu_space s, const double* cell_vm_dev, double* out_dev);
 int run_pcg_noalloc(i64 n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
                     const double* inv_diag, const double* b, const double* x0, double rtol, i64 max_iter, double* x,
                     fcu_solve_info* info, void* stream);
@@ -969,6 +972,41 @@ int fcu_adjoint_gradient(fcu_ctx ctx, fcu_space s, double E0, double nu, const d
     if (nc) adjoint_gradient_impl(s, E0, nu, th.p, ud.p, ld.p, g.p);
     g.finish(ctx);
     if (g.on_host() || th.staged.p || ud.staged.p || ld.staged.p) sync(ctx);
+  });
+}
+
+int fcu_element_stresses(fcu_ctx ctx, fcu_space s, double E, double nu, const double* u, double* stress,
+                         double* strain, double* von_mises, double* trace) {
+  return guarded(ctx, [&] {
+    if (!s || (s->kind != FCU_SPACE_P1_VEC3 && !(s->kind == FCU_SPACE_P1 && s->mesh->dim == 3)))
+      fail(FCU_ERR_BAD_ARG, "needs a space on a tetrahedron mesh (P1 or vector P1)");
+    if (!u) fail(FCU_ERR_BAD_ARG, "null displacement");
+    if (!(nu > -1.0 && nu < 0.5)) fail(FCU_ERR_BAD_ARG, "Poisson's ratio must be in (-1.0, 0.5)");
+    // ElasticMaterial::lame_lambda / lame_mu (elasticity.rs:33-47)
+    const double lam = (E * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double mu = E / (2.0 * (1.0 + nu));
+    const i64 nc = s->mesh->nc;
+    DevIn<double> ud(ctx, u, 3 * s->mesh->nv);
+    DevOut<double> so(stress, 9 * nc), eo(strain, 9 * nc), vo(von_mises, nc), to(trace, nc);
+    if (nc) element_stresses_impl(s, lam, mu, ud.p, so.p, eo.p, vo.p, to.p);
+    so.finish(ctx);
+    eo.finish(ctx);
+    vo.finish(ctx);
+    to.finish(ctx);
+    sync(ctx);
+  });
+}
+
+int fcu_vertex_von_mises(fcu_ctx ctx, fcu_space s, const double* cell_von_mises, double* vertex_von_mises) {
+  return guarded(ctx, [&] {
+    if (!s || (s->kind != FCU_SPACE_P1_VEC3 && !(s->kind == FCU_SPACE_P1 && s->mesh->dim == 3)))
+      fail(FCU_ERR_BAD_ARG, "needs a space on a tetrahedron mesh (P1 or vector P1)");
+    if (!cell_von_mises || !vertex_von_mises) fail(FCU_ERR_BAD_ARG, "null argument");
+    DevIn<double> cv(ctx, cell_von_mises, s->mesh->nc);
+    DevOut<double> vo(vertex_von_mises, s->mesh->nv);
+    if (s->mesh->nv) vertex_von_mises_impl(s, cv.p, vo.p);
+    vo.finish(ctx);
+    sync(ctx);
   });
 }
 

@@ -458,3 +458,116 @@ i64 boundary_dofs_impl(fcu_mesh m, fcu_space s_or_null, DBuf<i64>& result) {
   result.alloc(nall);
   return sort_unique(ctx, all.p, nall, result.p);
 }
+
+// ---------------------------------------------------------------------------
+// Stress recovery (elasticity.rs:230-360): per-cell displacement gradient,
+// strain, Cauchy stress and von Mises stress, and the volume-weighted vertex
+// average of the von Mises stress. Compiled without FMA contraction, with the
+// reference's order of summation.
+// ---------------------------------------------------------------------------
+namespace {
+
+// One thread per cell; any output may be null. Degenerate cells give zeros
+// (StressState::default()).
+__global__ void k_element_stresses(const double* __restrict__ X, const int* __restrict__ cells,
+                                   const unsigned char* __restrict__ valid, i64 nc, const double* __restrict__ u,
+                                   double lam, double mu, double* __restrict__ stress, double* __restrict__ strain,
+                                   double* __restrict__ vm, double* __restrict__ trace) {
+  for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
+    double s[3][3] = {{0.0}}, e[3][3] = {{0.0}};
+    double v = 0.0, t = 0.0;
+    if (valid[c]) {
+      int vv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) vv[i] = cells[4 * c + i];
+      const Geo3 g3 = tet_geometry(X, vv);
+      // P1 gradients: g_0 = J^-T (-1,-1,-1), g_k = J^-T e_{k-1}
+      double gr[4][3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        gr[0][r] = -g3.G[r][0] - g3.G[r][1] - g3.G[r][2];
+        gr[1][r] = g3.G[r][0];
+        gr[2][r] = g3.G[r][1];
+        gr[3][r] = g3.G[r][2];
+      }
+      double un[4][3];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) un[k][i] = u[3 * (i64)vv[k] + i];
+      double gu[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          double a = 0.0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) a += un[k][i] * gr[k][j];
+          gu[i][j] = a;
+        }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) e[i][j] = 0.5 * (gu[i][j] + gu[j][i]);
+      const double tr = e[0][0] + e[1][1] + e[2][2];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) s[i][j] = lam * tr * (i == j ? 1.0 : 0.0) + 2.0 * mu * e[i][j];
+      const double d01 = s[0][0] - s[1][1], d12 = s[1][1] - s[2][2], d20 = s[2][2] - s[0][0];
+      const double vm2 =
+          0.5 * (d01 * d01 + d12 * d12 + d20 * d20 + 6.0 * (s[0][1] * s[0][1] + s[1][2] * s[1][2] + s[2][0] * s[2][0]));
+      v = sqrt(fmax(vm2, 0.0));
+      t = s[0][0] + s[1][1] + s[2][2];
+    }
+    if (stress)
+#pragma unroll
+      for (int q = 0; q < 9; ++q) stress[9 * c + q] = s[q / 3][q % 3];
+    if (strain)
+#pragma unroll
+      for (int q = 0; q < 9; ++q) strain[9 * c + q] = e[q / 3][q % 3];
+    if (vm) vm[c] = v;
+    if (trace) trace[c] = t;
+  }
+}
+
+// One thread per vertex: sum over its cells in ascending order (the row's
+// contribution list) of vm * vol and vol, then the quotient (kept as the sum
+// when the volume is ~0, as the reference leaves it).
+__global__ void k_vertex_von_mises(const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+                                   const double* __restrict__ X, const int* __restrict__ cells,
+                                   const double* __restrict__ cell_vm, i64 nv, double* __restrict__ out) {
+  for (i64 v = blockIdx.x * (i64)blockDim.x + threadIdx.x; v < nv; v += (i64)gridDim.x * blockDim.x) {
+    double sv = 0.0, sw = 0.0;
+    for (int q = contrib_ptr[v]; q < contrib_ptr[v + 1]; ++q) {
+      const int c = contrib[q] >> 4;
+      int vv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) vv[i] = cells[4 * (i64)c + i];
+      const Geo3 g3 = tet_geometry(X, vv);
+      const double vol = (1.0 / 6.0) * fabs(g3.det);
+      sv += cell_vm[c] * vol;
+      sw += vol;
+    }
+    out[v] = sw > 1e-15 ? sv / sw : sv;
+  }
+}
+
+}  // namespace
+
+void element_stresses_impl(fcu_space s, double lam, double mu, const double* u_dev, double* stress, double* strain,
+                           double* vm, double* trace) {
+  fcu_mesh m = s->mesh;
+  fcu_ctx ctx = m->ctx;
+  k_element_stresses<<<grid_for(m->nc, 128, ctx->num_sms * 16), 128, 0, ctx->stream>>>(
+      m->coords.p, m->cells.p, m->valid.p, m->nc, u_dev, lam, mu, stress, strain, vm, trace);
+  LAUNCH_CHECK(ctx);
+}
+
+void vertex_von_mises_impl(fcu_space s, const double* cell_vm_dev, double* out_dev) {
+  fcu_mesh m = s->mesh;
+  fcu_ctx ctx = m->ctx;
+  k_vertex_von_mises<<<grid_for(m->nv, 128, ctx->num_sms * 16), 128, 0, ctx->stream>>>(
+      s->contrib_ptr.p, s->contrib.p, m->coords.p, m->cells.p, cell_vm_dev, m->nv, out_dev);
+  LAUNCH_CHECK(ctx);
+}

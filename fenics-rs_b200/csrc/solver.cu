@@ -407,6 +407,7 @@ __host__ __device__ size_t tile_stage_bytes(int cap_blocks) {
 constexpr int SPMV_CONSUMER_WARPS = 16;
 constexpr int SPMV_THREADS = 32 * (SPMV_CONSUMER_WARPS + 1);
 constexpr int MAX_STAGES = 4;
+constexpr int TILED_CTAS_PER_SM = 2;  // resident CTAs of the tiled SpMV per SM
 
 // Output of the tiled kernel: Ap for one scalar row, and p.Ap accumulated
 // from the row's own operand value (already in registers).
@@ -966,8 +967,12 @@ void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* 
   int per_sm = 0;
   CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SPMV_THREADS, smem));
   if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "block rows too long for the tiled SpMV");
+  // The grid sets the order in which p.Ap is reduced, so it does not follow
+  // the ring depth: TILED_CTAS_PER_SM CTAs per SM whenever they fit, which
+  // keeps the iterates identical for every depth the tuner may pick.
   const i64 ntiles = (m->nnodes + TILE_ROWS - 1) / TILE_ROWS;
-  const int grid = (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)per_sm * ctx->num_sms));
+  const int grid =
+      (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)std::min(per_sm, TILED_CTAS_PER_SM) * ctx->num_sms));
   launch_pdl_cfg(ctx, kern, grid, SPMV_THREADS, smem, m->row_ptr, m->col_idx, val, m->nnodes, cap, nstage, p, ap,
                  w->st.p, w->partials.p);
 }
@@ -1307,8 +1312,13 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
                                : tile_stage_bytes<double>(TILE_ROWS * max_row);
     int best = w->stages[k];
     double best_ms = 1e30;
+    int per_sm_max = 0;
+    CUDA_CHECK(cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
     for (int ns = 2; ns <= MAX_STAGES; ++ns) {
-      if (ns * stage + 1024 > (size_t)optin) continue;
+      // every candidate keeps the same grid (TILED_CTAS_PER_SM per SM)
+      if (ns * stage + 1024 > (size_t)optin ||
+          TILED_CTAS_PER_SM * (ns * stage + 2048) > (size_t)per_sm_max)
+        continue;
       w->stages[k] = ns;
       const double ms = trial();
       if (ms < best_ms) {
@@ -1318,13 +1328,19 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
     }
     w->stages[k] = best;
   } else {
+    // Lanes per row change the summation order inside a row, so a shape
+    // replaces the default only when it is clearly (10%) faster: near-ties
+    // then cannot flip the choice, and the iterates, from run to run.
     int& v = mixed ? w->vpr32 : w->vpr;
-    int best = v;
-    double best_ms = 1e30;
+    const int dflt = v;
+    const double dflt_ms = trial();
+    int best = dflt;
+    double best_ms = dflt_ms;
     for (int c : {4, 8, 16, 32}) {
+      if (c == dflt) continue;
       v = c;
       const double ms = trial();
-      if (ms < best_ms) {
+      if (ms < 0.9 * dflt_ms && ms < best_ms) {
         best_ms = ms;
         best = c;
       }

@@ -331,6 +331,23 @@ class FunctionSpace:
         _check(self.ctx, _L().fcu_assemble_surface_traction(self.ctx.h, self.h, nf, pf, pt, pb))
         return out
 
+    def element_stresses(self, E, nu, u, stress=None, strain=None, von_mises=None, trace=None):
+        """Per-cell stress, strain (nc x 9), von Mises stress and trace (nc) into
+        the given outputs (numpy or CUDA tensors; None skips an output)."""
+        pu, ku = _ptr(u, np.float64)
+        ps, ks = _ptr(stress)
+        pe, ke = _ptr(strain)
+        pv, kv = _ptr(von_mises)
+        pt, kt = _ptr(trace)
+        _check(self.ctx, _L().fcu_element_stresses(self.ctx.h, self.h, float(E), float(nu), pu, ps, pe, pv, pt))
+
+    def vertex_von_mises(self, cell_von_mises, out=None):
+        out = np.empty(self.mesh.nv) if out is None else out
+        pc, kc = _ptr(cell_von_mises, np.float64)
+        po, ko = _ptr(out)
+        _check(self.ctx, _L().fcu_vertex_von_mises(self.ctx.h, self.h, pc, po))
+        return out
+
     def adjoint_gradient(self, E0, nu, theta, u, lam, out=None):
         out = np.empty(self.mesh.nc) if out is None else out
         pt, kt = _ptr(theta, np.float64)
@@ -856,6 +873,38 @@ def solve_poisson_batch(meshes, kappas=None, nodal_sources=None, tol=1e-8, max_i
     M.close()
     V.close()
     return BatchSolution([x[offs[i]:offs[i + 1]] for i in range(len(meshes))], it, rel, st, info, offs)
+
+
+@dataclass
+class StressStates:
+    """StressState of every cell (elasticity.rs:230-320), as arrays."""
+    stress: np.ndarray     # [nc, 3, 3]
+    strain: np.ndarray     # [nc, 3, 3]
+    von_mises: np.ndarray  # [nc]
+    trace: np.ndarray      # [nc]
+
+
+def compute_element_stresses(mesh: Mesh, u, material: ElasticMaterial, ctx: Context | None = None) -> StressStates:
+    """compute_element_stresses (elasticity.rs:230-320) on the device."""
+    ctx = ctx or default_context()
+    V = FunctionSpace(ctx, mesh, FCU_SPACE_P1_VEC3)
+    nc = mesh.nc
+    st, ep = np.empty((nc, 3, 3)), np.empty((nc, 3, 3))
+    vm, tr = np.empty(nc), np.empty(nc)
+    V.element_stresses(material.youngs_modulus, material.poissons_ratio, np.ascontiguousarray(u, np.float64),
+                       st, ep, vm, tr)
+    V.close()
+    return StressStates(st, ep, vm, tr)
+
+
+def compute_vertex_von_mises(mesh: Mesh, element_stresses: StressStates, ctx: Context | None = None) -> np.ndarray:
+    """compute_vertex_von_mises (elasticity.rs:323-360): volume-weighted vertex
+    average of the cells' von Mises stress."""
+    ctx = ctx or default_context()
+    V = FunctionSpace(ctx, mesh, FCU_SPACE_P1_VEC3)
+    out = V.vertex_von_mises(np.ascontiguousarray(element_stresses.von_mises, np.float64))
+    V.close()
+    return out
 
 
 def batch_costs(meshes) -> np.ndarray:

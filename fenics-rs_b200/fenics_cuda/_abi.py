@@ -85,6 +85,8 @@ SIGNATURES = {
     "fcu_solve_csr_cg_noalloc": (cint, [i64, vp, vp, vp, vp, vp, vp, dbl, i64, vp, C.POINTER(SolveInfo), vp]),
     "fcu_batch_pcg": (cint, [vp, vp, i64, vp, vp, vp, dbl, i64, cint, vp, vp, vp, C.POINTER(SolveInfo)]),
     "fcu_batch_config": (cint, [vp, cint, C.POINTER(cint), C.POINTER(cint), C.POINTER(cint)]),
+    "fcu_element_stresses": (cint, [vp, vp, dbl, dbl, vp, vp, vp, vp, vp]),
+    "fcu_vertex_von_mises": (cint, [vp, vp, vp, vp]),
     "fcu_spmv": (cint, [vp, vp, vp, vp]),
     "fcu_adjoint_gradient": (cint, [vp, vp, dbl, dbl, vp, vp, vp, vp]),
     "fcu_time_spmv": (cint, [vp, vp, cint, cint, C.POINTER(dbl), C.POINTER(dbl)]),

@@ -233,6 +233,21 @@ int fcu_spmv(fcu_ctx ctx, fcu_matrix m, const double* x, double* y);
 int fcu_adjoint_gradient(fcu_ctx ctx, fcu_space space, double E0, double nu, const double* theta,
                          const double* u, const double* lambda, double* grad);
 
+/* ---- stress recovery --------------------------------------------------------- */
+/* compute_element_stresses (elasticity.rs:230-320) on the space's tetrahedron
+ * mesh (FCU_SPACE_P1_VEC3, or FCU_SPACE_P1 in 3D): per cell the displacement
+ * gradient from u (3*nv, dof = 3*vertex + component), strain = sym(grad u),
+ * Cauchy stress = lambda tr(eps) I + 2 mu eps, von Mises stress and trace.
+ * stress, strain: nc*9 row-major; von_mises, trace: nc; any may be NULL.
+ * Degenerate cells give zeros (StressState::default()). */
+int fcu_element_stresses(fcu_ctx ctx, fcu_space space, double E, double nu, const double* u,
+                         double* stress, double* strain, double* von_mises, double* trace);
+/* compute_vertex_von_mises (elasticity.rs:323-360): volume-weighted average of
+ * the cells' von Mises stress at each vertex (nv), cells summed in ascending
+ * order; vertices with no volume keep the (zero) sum. */
+int fcu_vertex_von_mises(fcu_ctx ctx, fcu_space space, const double* cell_von_mises,
+                         double* vertex_von_mises);
+
 /* ---- diagnostics (no reference counterpart) -------------------------------- */
 /* Average device time of one launch of the SpMV kernel the PCG of `precision`
  * runs on m (Ap = A p with the device p.Ap reduction), over `reps`
