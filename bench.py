@@ -545,6 +545,74 @@ def run_workloads(ctx, stream, peak):
     c5["speedup_mixed_vs_fp64"] = c5["fp64"]["ms"] / c5["mixed"]["ms"]
     out["c5"] = c5
     M.close(); V.close()
+
+    # Mass matrix of the C2 mesh (assemble_elasticity_mass_3d, density 7850)
+    mesh = fcu.box_beam(4.0, 1.0, 1.0, 128, 32, 32)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+    M = fcu.Matrix(ctx, V).assemble_mass(7850.0)
+    ms_m, _ = _best_ms(stream, lambda: M.assemble_mass(7850.0), k=3)
+    stored = V.nnz  # scalar entries of the 3x3 blocks the kernel writes
+    mbytes = mesh.nc * (4 * 4 + 4 * 16) + mesh.nv * 24 + stored * (8 + 4)
+    out["mass_c2"] = {"workload": "vector-P1 mass matrix of the C2 mesh (786,432 tets), density 7850",
+                      "ms": ms_m, "gbs": mbytes / (ms_m * 1e-3) / 1e9, "bytes": mbytes,
+                      "frac_of_hbm": mbytes / (ms_m * 1e-3) / 1e9 / peak}
+    M.close(); V.close()
+
+    # Transient heat: unit square 1024^2, Crank-Nicolson, dt = 1e-4, u = 0 on the boundary
+    mesh = fcu.unit_square(1024, 1024)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
+    Mm = fcu.Matrix(ctx, V).assemble_mass(1.0)
+    K = fcu.Matrix(ctx, V).assemble_stiffness(None)
+    bd = V.boundary_dofs().astype(np.int64)
+    u0 = d64(np.sin(math.pi * mesh.coords[:, 0]) * np.sin(math.pi * mesh.coords[:, 1]))
+    tr = {"workload": "2D transient heat, unit square 1024x1024 x 2 triangles (1,050,625 dofs), diffusivity 1, "
+                      "Crank-Nicolson dt = 1e-4, u0 = sin(pi x) sin(pi y), u = 0 on the boundary, no source, "
+                      "20 steps, each solved by PCG from the previous state to 1e-10",
+          "ndofs": V.ndofs}
+    nsteps = 20
+    for name, prec in (("fp64", fcu.FCU_FP64), ("mixed", fcu.FCU_MIXED)):
+        st = fcu._Stepper(ctx, Mm, K, fcu.FCU_CRANK_NICOLSON, 1e-4)
+        st.set_dirichlet(bd, np.zeros(len(bd)))
+        ua, ub = u0.clone(), torch.empty_like(u0)
+        st.step(ua, None, None, ub, 1e-10, 100000, prec)   # warm-up: tuning and graph capture
+
+        def run():
+            a, b2 = u0.clone(), torch.empty_like(u0)
+            its = []
+            for _ in range(nsteps):
+                its.append(int(st.step(a, None, None, b2, 1e-10, 100000, prec).iterations))
+                a, b2 = b2, a
+            return a, its
+        ms, (uf, its) = _best_ms(stream, run)
+        exact = math.exp(-2 * math.pi ** 2 * nsteps * 1e-4)
+        tr[name] = {"ms": ms, "ms_per_step": ms / nsteps, "iterations_per_step": float(np.mean(its)),
+                    "dof_steps_per_s": V.ndofs * nsteps / (ms * 1e-3),
+                    "center_over_exact": float(uf[512 * 1025 + 512]) / exact}
+        st.close()
+    out["transient_heat"] = tr
+    Mm.close(); K.close(); V.close()
+
+    # Vibration modes: steel cantilever [0,4]x[0,1]x[0,1], 64x16x16 x 6 tets, clamped x = 0
+    mesh = fcu.box_beam(4.0, 1.0, 1.0, 64, 16, 16)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+    K = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+    Mm = fcu.Matrix(ctx, V).assemble_mass(7850.0)
+    cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+    fixed = (3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64)
+    md = {"workload": "lowest 3 vibration modes of a steel cantilever [0,4]x[0,1]x[0,1], 64x16x16 hexes x 6 tets "
+                      "(56,355 dofs), E = 210e9, nu = 0.3, density 7850, clamped x = 0; inverse power iteration, "
+                      "30 iterations at most, tol 1e-6, inner PCG to 1e-9 from the previous iterate",
+          "ndofs": V.ndofs}
+    for name, prec in (("fp64", fcu.FCU_FP64), ("mixed", fcu.FCU_MIXED)):
+        def run():
+            return fcu.solve_vibration_modes(K, Mm, fixed, 3, 30, 1e-6, ctx, precision=prec, inner_tol=1e-9,
+                                             inner_max_iter=50000, return_stats=True)
+        run()
+        ms, (modes, pit, info) = _best_ms(stream, run)
+        md[name] = {"ms": ms, "frequencies_hz": [m.frequency_hz for m in modes],
+                    "power_iterations": [int(p) for p in pit], "inner_iterations": int(info.iterations)}
+    out["modes"] = md
+    K.close(); Mm.close(); V.close()
     return out
 
 

@@ -35,6 +35,27 @@ void batch_config(fcu_matrix m, int precision, int* vpr, int* threads, int* clus
 void element_stresses_impl(fcu_space s, double lam, double mu, const double* u_dev, double* stress, double* strain,
                            double* vm, double* trace);
 void vertex_von_mises_impl(fcu_space s, const double* cell_vm_dev, double* out_dev);
+void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev);
+bool same_pattern(fcu_matrix a, fcu_matrix b);
+void add_scaled_impl(fcu_matrix out, fcu_matrix a, fcu_matrix b, double alpha);
+void scale_values_impl(fcu_matrix m, double s);
+i64 fold_dirichlet_impl(fcu_matrix m, i64 nf, const i64* dofs_dev, bool unit_diag, DBuf<unsigned char>* fixed_out);
+fcu_transient transient_create_impl(fcu_matrix mass, fcu_matrix stiff, int scheme, double dt);
+void transient_destroy_impl(fcu_transient t);
+fcu_ctx transient_ctx(fcu_transient t);
+i64 transient_order(fcu_transient t);
+void transient_set_dirichlet_impl(fcu_transient t, i64 nbc, const i64* dofs_host, const double* vals_host);
+int transient_step_impl(fcu_transient t, const double* un, const double* fn, const double* fnext, double* unext,
+                        double tol, i64 max_iter, int precision, fcu_solve_info* info);
+int vibration_modes_impl(fcu_matrix k, fcu_matrix m, i64 nfixed, const i64* fixed_dev, i64 num_modes,
+                         i64 max_power_iters, double tol, double inner_tol, i64 inner_max_iter, int precision,
+                         fcu_inner_solve inner, void* user, double* eigenvalues, double* modes_dev,
+                         i64* power_iters, fcu_solve_info* info, std::string* err);
+fcu_matrix bsr3_create_impl(fcu_ctx ctx, i64 nn, const uint32_t* rp_dev, const uint32_t* ci_dev, i64 nnzb,
+                            const double* vals_dev, const double* dinv_dev);
+void bsr3_jacobi_smooth_impl(fcu_matrix m, const double* r, double* z, i64 sweeps, double omega, bool zero_init);
+void matrix_block_jacobi_impl(fcu_matrix m, bool enable);
+void matrix_export_bsr3_impl(fcu_matrix m, uint32_t* rp, uint32_t* ci, double* vals, double* dinv);
 int run_pcg_noalloc(i64 n, const uint32_t* row_ptr, const uint32_t* col_idx, const double* vals,
                     const double* inv_diag, const double* b, const double* x0, double rtol, i64 max_iter, double* x,
                     fcu_solve_info* info, void* stream);
@@ -161,17 +182,24 @@ __global__ void k_diag_keys(i64 n, unsigned long long* __restrict__ keys, unsign
 // --- export: space matrices (symmetric node pattern) -------------------------
 // Inclusion rule of the reference pattern: a stored entry (r, c) is exported
 // when its slot is structural (not an inserted diagonal) and neither r nor c
-// is eliminated; an eliminated dof keeps only its diagonal.
+// is eliminated; an eliminated dof keeps only its diagonal. A folded matrix
+// (fold_dirichlet, eigen.rs:55-79: `drop`) also omits every zero value,
+// including a fixed diagonal folded to 0. `val`/`tpos` are read only then.
+// A vector mass matrix (`cdiag`) holds only the same-component entries of
+// each block (mass.rs:118-123).
 template <int BS>
-__global__ void k_export_count(const int* __restrict__ rp, const int* __restrict__ ci,
-                               const unsigned char* __restrict__ dstruct, const unsigned char* __restrict__ dir, i64 nn,
+__global__ void k_export_count(const int* __restrict__ rp, const int* __restrict__ ci, const int* __restrict__ tpos,
+                               const double* __restrict__ val, bool drop, bool cdiag,
+                               const unsigned char* __restrict__ dstruct,
+                               const unsigned char* __restrict__ dir, const double* __restrict__ dcount, i64 nn,
                                i64* __restrict__ cnt) {
   for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nn * BS; c += (i64)gridDim.x * blockDim.x) {
     const i64 w = c / BS;
+    const int be = (int)(c - w * BS);
     const bool dc = dir ? dir[c] != 0 : false;
     i64 k = 0;
     if (dc) {
-      k = 1;
+      k = (drop && dcount[c] == 0.0) ? 0 : 1;
     } else {
       for (int p = rp[w]; p < rp[w + 1]; ++p) {
         const i64 v = ci[p];
@@ -179,6 +207,8 @@ __global__ void k_export_count(const int* __restrict__ rp, const int* __restrict
         for (int a = 0; a < BS; ++a) {
           const i64 r = v * BS + a;
           if (dir && dir[r]) continue;
+          if (cdiag && a != be) continue;
+          if (drop && val[(i64)tpos[p] * BS * BS + a * BS + be] == 0.0) continue;
           ++k;
         }
       }
@@ -189,7 +219,8 @@ __global__ void k_export_count(const int* __restrict__ rp, const int* __restrict
 
 template <int BS>
 __global__ void k_export_fill(const int* __restrict__ rp, const int* __restrict__ ci, const int* __restrict__ tpos,
-                              const unsigned char* __restrict__ dstruct, const unsigned char* __restrict__ dir,
+                              bool drop, bool cdiag, const unsigned char* __restrict__ dstruct,
+                              const unsigned char* __restrict__ dir,
                               const double* __restrict__ dcount, const double* __restrict__ val, i64 nn,
                               const i64* __restrict__ colptr, i64* __restrict__ rowidx, double* __restrict__ vals) {
   for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nn * BS; c += (i64)gridDim.x * blockDim.x) {
@@ -197,6 +228,7 @@ __global__ void k_export_fill(const int* __restrict__ rp, const int* __restrict_
     const int be = (int)(c - w * BS);
     i64 o = colptr[c];
     if (dir && dir[c]) {
+      if (drop && dcount[c] == 0.0) continue;
       if (rowidx) rowidx[o] = c;
       if (vals) vals[o] = dcount[c];
       continue;
@@ -208,6 +240,8 @@ __global__ void k_export_fill(const int* __restrict__ rp, const int* __restrict_
       for (int a = 0; a < BS; ++a) {
         const i64 r = v * BS + a;
         if (dir && dir[r]) continue;
+        if (cdiag && a != be) continue;
+        if (drop && val[q * BS * BS + a * BS + be] == 0.0) continue;
         if (rowidx) rowidx[o] = r;
         if (vals) vals[o] = val[q * BS * BS + a * BS + be];
         ++o;
@@ -217,30 +251,33 @@ __global__ void k_export_fill(const int* __restrict__ rp, const int* __restrict_
 }
 
 // --- export: wrapped CSC matrices (original CSC order) ------------------------
-__global__ void k_wexport_count(const i64* __restrict__ cp, const i64* __restrict__ ri,
-                                const unsigned char* __restrict__ dir, i64 n, i64* __restrict__ cnt) {
+__global__ void k_wexport_count(const i64* __restrict__ cp, const i64* __restrict__ ri, const int* __restrict__ csr_of,
+                                const double* __restrict__ val, bool drop, const unsigned char* __restrict__ dir,
+                                const double* __restrict__ dcount, i64 n, i64* __restrict__ cnt) {
   for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < n; c += (i64)gridDim.x * blockDim.x) {
-    if (dir && dir[c]) { cnt[c] = 1; continue; }
+    if (dir && dir[c]) { cnt[c] = (drop && dcount[c] == 0.0) ? 0 : 1; continue; }
     i64 k = 0;
     for (i64 q = cp[c]; q < cp[c + 1]; ++q)
-      if (!(dir && dir[ri[q]])) ++k;
+      if (!(dir && dir[ri[q]]) && !(drop && val[csr_of[q]] == 0.0)) ++k;
     cnt[c] = k;
   }
 }
 
 __global__ void k_wexport_fill(const i64* __restrict__ cp, const i64* __restrict__ ri, const int* __restrict__ csr_of,
-                               const unsigned char* __restrict__ dir, const double* __restrict__ dcount,
+                               bool drop, const unsigned char* __restrict__ dir, const double* __restrict__ dcount,
                                const double* __restrict__ val, i64 n, const i64* __restrict__ colptr,
                                i64* __restrict__ rowidx, double* __restrict__ vals) {
   for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < n; c += (i64)gridDim.x * blockDim.x) {
     i64 o = colptr[c];
     if (dir && dir[c]) {
+      if (drop && dcount[c] == 0.0) continue;
       if (rowidx) rowidx[o] = c;
       if (vals) vals[o] = dcount[c];
       continue;
     }
     for (i64 q = cp[c]; q < cp[c + 1]; ++q) {
       if (dir && dir[ri[q]]) continue;
+      if (drop && val[csr_of[q]] == 0.0) continue;
       if (rowidx) rowidx[o] = ri[q];
       if (vals) vals[o] = val[csr_of[q]];
       ++o;
@@ -279,6 +316,7 @@ void reset_dirichlet(fcu_matrix m) {
   if (m->bc_applied && m->dirichlet.p)
     CUDA_CHECK(cudaMemsetAsync(m->dirichlet.p, 0, m->n, m->ctx->stream));
   m->bc_applied = false;
+  m->drop_zeros = false;
   m->n_dirichlet = 0;
 }
 
@@ -325,6 +363,59 @@ void matrix_release(fcu_matrix m) {
 }
 
 }  // namespace
+
+// A new matrix on src's pattern holding a copy of its values and Dirichlet
+// state (one reference to it, held by the caller).
+fcu_matrix matrix_clone(fcu_matrix src) {
+  fcu_ctx ctx = src->ctx;
+  std::unique_ptr<fcu_matrix_s> m(new fcu_matrix_s());
+  m->ctx = ctx;
+  m->space = src->space;
+  m->n = src->n;
+  m->nnodes = src->nnodes;
+  m->bs = src->bs;
+  m->nnzb = src->nnzb;
+  m->wrapped_general = src->wrapped_general;
+  auto copy = [&](auto& dst, const auto& from) {
+    if (!from.p) return;
+    dst.alloc(from.n);
+    CUDA_CHECK(cudaMemcpyAsync(dst.p, from.p, from.bytes(), cudaMemcpyDeviceToDevice, ctx->stream));
+  };
+  if (src->space) {
+    m->row_ptr = src->row_ptr;
+    m->col_idx = src->col_idx;
+    m->diag_pos = src->diag_pos;
+  } else {
+    copy(m->own_row_ptr, src->own_row_ptr);
+    copy(m->own_col_idx, src->own_col_idx);
+    copy(m->own_diag_pos, src->own_diag_pos);
+    copy(m->csc_colptr, src->csc_colptr);
+    copy(m->csc_rowidx, src->csc_rowidx);
+    copy(m->csr_of, src->csr_of);
+    m->row_ptr = m->own_row_ptr.p;
+    m->col_idx = m->own_col_idx.p;
+    m->diag_pos = m->own_diag_pos.p;
+  }
+  copy(m->val64, src->val64);
+  copy(m->val32, src->val32);
+  copy(m->dirichlet, src->dirichlet);
+  copy(m->diag_count, src->diag_count);
+  copy(m->diag_struct, src->diag_struct);
+  m->n_dirichlet = src->n_dirichlet;
+  m->bc_applied = src->bc_applied;
+  m->drop_zeros = src->drop_zeros;
+  m->comp_diag = src->comp_diag;
+  copy(m->bdinv, src->bdinv);
+  m->block_jacobi = src->block_jacobi;
+  m->max_row_own = src->max_row_own;
+  m->missing_diag = src->missing_diag;
+  m->has_values = src->has_values;
+  if (m->space) m->space->refs++;
+  ctx->refs++;
+  return m.release();
+}
+
+void matrix_release_ref(fcu_matrix m) { matrix_release(m); }
 
 extern "C" {
 
@@ -648,20 +739,31 @@ void fcu_matrix_destroy(fcu_matrix m) { matrix_release(m); }
 
 static i64 export_counts(fcu_matrix m, DBuf<i64>& colptr) {
   fcu_ctx ctx = m->ctx;
+  if (!m->space && !m->wrapped_general)
+    fail(FCU_ERR_UNSUPPORTED, "a block CSR matrix exports through fcu_matrix_export_bsr3");
   const i64 n = m->n;
   DBuf<i64> cnt;
   cnt.alloc(n + 1);
   CUDA_CHECK(cudaMemsetAsync(cnt.p + n, 0, sizeof(i64), ctx->stream));
   const unsigned char* dir = m->bc_applied ? m->dirichlet.p : nullptr;
+  const bool drop = m->drop_zeros;
   if (m->wrapped_general) {
-    k_wexport_count<<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(m->csc_colptr.p, m->csc_rowidx.p,
-                                                                               dir, n, cnt.p);
-  } else if (m->bs == 3) {
-    k_export_count<3><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(m->row_ptr, m->col_idx,
-                                                                                 m->diag_struct.p, dir, m->nnodes, cnt.p);
+    k_wexport_count<<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
+        m->csc_colptr.p, m->csc_rowidx.p, m->csr_of.p, m->val64.p, drop, dir, m->diag_count.p, n, cnt.p);
   } else {
-    k_export_count<1><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(m->row_ptr, m->col_idx,
-                                                                                 m->diag_struct.p, dir, m->nnodes, cnt.p);
+    const int* tpos = nullptr;
+    if (drop) {
+      build_transpose_positions(m->space);
+      tpos = m->space->tpos.p;
+    }
+    if (m->bs == 3)
+      k_export_count<3><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
+          m->row_ptr, m->col_idx, tpos, m->val64.p, drop, m->comp_diag, m->diag_struct.p, dir, m->diag_count.p,
+          m->nnodes, cnt.p);
+    else
+      k_export_count<1><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
+          m->row_ptr, m->col_idx, tpos, m->val64.p, drop, false, m->diag_struct.p, dir, m->diag_count.p, m->nnodes,
+          cnt.p);
   }
   LAUNCH_CHECK(ctx);
   colptr.alloc(n + 1);
@@ -676,7 +778,8 @@ int fcu_matrix_info(fcu_matrix m, int64_t* n, int64_t* nnz) {
   return guarded(m->ctx, [&] {
     if (n) *n = m->n;
     if (nnz) {
-      if (!m->bc_applied && m->space) *nnz = m->space->nnz_ref;
+      if (!m->space && !m->wrapped_general) *nnz = 9 * m->nnzb;
+      else if (!m->bc_applied && !m->drop_zeros && !m->comp_diag && m->space) *nnz = m->space->nnz_ref;
       else {
         DBuf<i64> cp;
         *nnz = export_counts(m, cp);
@@ -697,17 +800,18 @@ int fcu_matrix_export_csc(fcu_ctx ctx, fcu_matrix m, int64_t* colptr, int64_t* r
     if (rowidx || vals) {
       if (m->wrapped_general) {
         k_wexport_fill<<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
-            m->csc_colptr.p, m->csc_rowidx.p, m->csr_of.p, dir, m->diag_count.p, m->val64.p, n, cp.p, R.p, V.p);
+            m->csc_colptr.p, m->csc_rowidx.p, m->csr_of.p, m->drop_zeros, dir, m->diag_count.p, m->val64.p, n, cp.p,
+            R.p, V.p);
       } else {
         build_transpose_positions(m->space);
         if (m->bs == 3)
           k_export_fill<3><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
-              m->row_ptr, m->col_idx, m->space->tpos.p, m->diag_struct.p, dir, m->diag_count.p, m->val64.p, m->nnodes,
-              cp.p, R.p, V.p);
+              m->row_ptr, m->col_idx, m->space->tpos.p, m->drop_zeros, m->comp_diag, m->diag_struct.p, dir,
+              m->diag_count.p, m->val64.p, m->nnodes, cp.p, R.p, V.p);
         else
           k_export_fill<1><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
-              m->row_ptr, m->col_idx, m->space->tpos.p, m->diag_struct.p, dir, m->diag_count.p, m->val64.p, m->nnodes,
-              cp.p, R.p, V.p);
+              m->row_ptr, m->col_idx, m->space->tpos.p, m->drop_zeros, false, m->diag_struct.p, dir,
+              m->diag_count.p, m->val64.p, m->nnodes, cp.p, R.p, V.p);
       }
       LAUNCH_CHECK(ctx);
     }
@@ -724,6 +828,7 @@ int fcu_assemble_stiffness(fcu_ctx ctx, fcu_matrix m, const double* cell_coef) {
     if (m->space->kind == FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "use fcu_assemble_elasticity for vector spaces");
     DevIn<double> coef(ctx, cell_coef, (size_t)m->space->mesh->nc);
     reset_dirichlet(m);
+    m->comp_diag = false;
     assemble_stiffness_impl(m, coef.p);
     m->has_values = true;
     if (coef.staged.p) sync(ctx);
@@ -736,9 +841,68 @@ int fcu_assemble_elasticity(fcu_ctx ctx, fcu_matrix m, double E, double nu, cons
     if (!(nu > -1.0 && nu < 0.5)) fail(FCU_ERR_BAD_ARG, "Poisson's ratio must be in (-1.0, 0.5) for physical stability");
     DevIn<double> ce(ctx, cell_E, (size_t)m->space->mesh->nc);
     reset_dirichlet(m);
+    m->comp_diag = false;
     assemble_elasticity_impl(m, E, nu, ce.p);
     m->has_values = true;
     if (ce.staged.p) sync(ctx);
+  });
+}
+
+int fcu_assemble_mass(fcu_ctx ctx, fcu_matrix m, double rho, const double* cell_coef) {
+  return guarded(ctx, [&] {
+    if (!m || !m->space) fail(FCU_ERR_BAD_ARG, "matrix has no function space");
+    DevIn<double> coef(ctx, cell_coef, (size_t)m->space->mesh->nc);
+    reset_dirichlet(m);
+    m->comp_diag = m->bs == 3;
+    assemble_mass_impl(m, rho, coef.p);
+    m->has_values = true;
+    if (coef.staged.p) sync(ctx);
+  });
+}
+
+int fcu_matrix_clone(fcu_ctx ctx, fcu_matrix src, fcu_matrix* out) {
+  if (!out) return FCU_ERR_BAD_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    if (!src) fail(FCU_ERR_BAD_ARG, "null matrix");
+    fcu_matrix m = matrix_clone(src);
+    sync(ctx);
+    *out = m;
+  });
+}
+
+int fcu_matrix_add_scaled(fcu_ctx ctx, fcu_matrix out, fcu_matrix a, fcu_matrix b, double alpha) {
+  return guarded(ctx, [&] {
+    if (!out || !a || !b) fail(FCU_ERR_BAD_ARG, "null matrix");
+    if (!a->has_values || !b->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (a->bc_applied || b->bc_applied)
+      fail(FCU_ERR_UNSUPPORTED, "add_scaled_matrices: an operand has eliminated or folded Dirichlet dofs");
+    if (!same_pattern(a, b) || !same_pattern(a, out))
+      fail(FCU_ERR_UNSUPPORTED, "add_scaled_matrices: operands must share one sparsity pattern");
+    reset_dirichlet(out);
+    out->comp_diag = a->comp_diag && b->comp_diag;
+    add_scaled_impl(out, a, b, alpha);
+    out->has_values = true;
+    sync(ctx);
+  });
+}
+
+int fcu_matrix_scale(fcu_ctx ctx, fcu_matrix m, double s) {
+  return guarded(ctx, [&] {
+    if (!m || !m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (m->bc_applied) fail(FCU_ERR_UNSUPPORTED, "scaling a matrix with eliminated Dirichlet dofs");
+    scale_values_impl(m, s);
+    sync(ctx);
+  });
+}
+
+int fcu_matrix_fold_dirichlet(fcu_ctx ctx, fcu_matrix m, int64_t nfixed, const int64_t* fixed, int unit_diag) {
+  return guarded(ctx, [&] {
+    if (!m || !m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (nfixed < 0 || (nfixed > 0 && !fixed)) fail(FCU_ERR_BAD_ARG, "bad fixed dof list");
+    DevIn<i64> d(ctx, fixed, nfixed);
+    fold_dirichlet_impl(m, nfixed, d.p, unit_diag != 0, nullptr);
+    sync(ctx);
   });
 }
 
@@ -1006,6 +1170,199 @@ int fcu_vertex_von_mises(fcu_ctx ctx, fcu_space s, const double* cell_von_mises,
     DevOut<double> vo(vertex_von_mises, s->mesh->nv);
     if (s->mesh->nv) vertex_von_mises_impl(s, cv.p, vo.p);
     vo.finish(ctx);
+    sync(ctx);
+  });
+}
+
+// ---------------------------------------------------------------------------
+// transient stepper and vibration modes
+// ---------------------------------------------------------------------------
+
+int fcu_transient_create(fcu_ctx ctx, fcu_matrix mass, fcu_matrix stiff, int scheme, double dt, fcu_transient* out) {
+  if (!out) return FCU_ERR_BAD_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    if (!mass || !stiff) fail(FCU_ERR_BAD_ARG, "null matrix");
+    if (!mass->has_values || !stiff->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (scheme != FCU_BACKWARD_EULER && scheme != FCU_CRANK_NICOLSON) fail(FCU_ERR_BAD_ARG, "unknown scheme");
+    if (!(dt > 0.0)) fail(FCU_ERR_BAD_ARG, "dt must be positive");
+    if (mass->bc_applied || stiff->bc_applied)
+      fail(FCU_ERR_UNSUPPORTED, "add_scaled_matrices: an operand has eliminated or folded Dirichlet dofs");
+    if (!same_pattern(mass, stiff))
+      fail(FCU_ERR_UNSUPPORTED, "add_scaled_matrices: operands must share one sparsity pattern");
+    fcu_transient t = transient_create_impl(mass, stiff, scheme, dt);
+    sync(ctx);
+    *out = t;
+  });
+}
+
+int fcu_transient_set_dirichlet(fcu_ctx ctx, fcu_transient ts, int64_t nbc, const int64_t* dofs, const double* vals) {
+  return guarded(ctx, [&] {
+    if (!ts || nbc < 0 || (nbc > 0 && (!dofs || !vals))) fail(FCU_ERR_BAD_ARG, "bad Dirichlet arguments");
+    std::vector<i64> d(nbc);
+    std::vector<double> v(nbc);
+    if (nbc) {
+      download(ctx, d.data(), dofs, nbc);
+      download(ctx, v.data(), vals, nbc);
+      sync(ctx);
+    }
+    transient_set_dirichlet_impl(ts, nbc, d.data(), v.data());
+  });
+}
+
+int fcu_transient_step(fcu_ctx ctx, fcu_transient ts, const double* u_n, const double* f_n, const double* f_next,
+                       double* u_next, double tol, int64_t max_iter, int precision, fcu_solve_info* info) {
+  int status = FCU_OK;
+  int rc = guarded(ctx, [&] {
+    if (!ts || !u_n || !u_next) fail(FCU_ERR_BAD_ARG, "null argument");
+    if (transient_ctx(ts) != ctx) fail(FCU_ERR_BAD_ARG, "stepper belongs to another context");
+    if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
+    if (max_iter < 0) fail(FCU_ERR_BAD_ARG, "max_iter must be >= 0");
+    const i64 n = transient_order(ts);
+    DevIn<double> u0(ctx, u_n, n);
+    DevIn<double> f0(ctx, f_n, f_n ? n : 0);
+    DevIn<double> f1(ctx, f_next, f_next ? n : 0);
+    DevOut<double> uo(u_next, n);
+    status = transient_step_impl(ts, u0.p, f0.p, f1.p, uo.p, tol, max_iter, precision, info);
+    uo.finish(ctx);
+    sync(ctx);
+  });
+  if (rc != FCU_OK) return rc;
+  if (status == FCU_ERR_NO_CONVERGENCE)
+    ctx->err = "CG failed to converge within " + std::to_string(max_iter) + " iterations";
+  else if (status == FCU_ERR_BREAKDOWN)
+    ctx->err = "Breakdown in CG: curvature p^T A p is near zero";
+  return status;
+}
+
+void fcu_transient_destroy(fcu_transient ts) { transient_destroy_impl(ts); }
+
+int fcu_vibration_modes(fcu_ctx ctx, fcu_matrix k, fcu_matrix m, int64_t nfixed, const int64_t* fixed,
+                        int64_t num_modes, int64_t max_power_iters, double tol, double inner_tol,
+                        int64_t inner_max_iter, int precision, fcu_inner_solve inner, void* user,
+                        double* eigenvalues, double* mode_shapes, int64_t* power_iterations, fcu_solve_info* info) {
+  int status = FCU_OK;
+  std::string err;
+  int rc = guarded(ctx, [&] {
+    if (!k || !m || !eigenvalues) fail(FCU_ERR_BAD_ARG, "null argument");
+    if (!k->has_values || !m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (k->n != m->n) fail(FCU_ERR_BAD_ARG, "stiffness and mass orders differ");
+    if (num_modes < 0 || max_power_iters < 0 || inner_max_iter < 0 || nfixed < 0 || (nfixed > 0 && !fixed))
+      fail(FCU_ERR_BAD_ARG, "bad arguments");
+    if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
+    const i64 n = k->n;
+    DevIn<i64> fx(ctx, fixed, nfixed);
+    DBuf<double> modes_own;
+    DevOut<double> mo(mode_shapes, mode_shapes ? (size_t)(num_modes * n) : 0);
+    double* modes = mo.p;
+    if (!modes) {
+      modes_own.alloc((size_t)std::max<i64>(num_modes, 1) * n);
+      modes = modes_own.p;
+    }
+    std::vector<double> ev(std::max<i64>(num_modes, 1));
+    std::vector<i64> pit(std::max<i64>(num_modes, 1));
+    status = vibration_modes_impl(k, m, nfixed, fx.p, num_modes, max_power_iters, tol, inner_tol, inner_max_iter,
+                                  precision, inner, user, ev.data(), modes, pit.data(), info, &err);
+    if (status == FCU_OK) {
+      std::copy(ev.begin(), ev.begin() + num_modes, eigenvalues);
+      if (power_iterations) std::copy(pit.begin(), pit.begin() + num_modes, power_iterations);
+      mo.finish(ctx);
+    }
+    sync(ctx);
+  });
+  if (rc != FCU_OK) return rc;
+  if (status != FCU_OK) ctx->err = err;
+  return status;
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 block CSR
+// ---------------------------------------------------------------------------
+
+static fcu_matrix bsr3_from_caller(fcu_ctx ctx, int64_t n_nodes, const uint32_t* row_ptr, const uint32_t* cols,
+                                   const double* vals_flat, const double* dinv_flat) {
+  if (n_nodes <= 0 || !row_ptr) fail(FCU_ERR_BAD_ARG, "bad block CSR arguments");
+  i64 nnzb = 0;
+  {
+    DevIn<uint32_t> rp(ctx, row_ptr + n_nodes, 1);
+    nnzb = read1(ctx, rp.p);
+  }
+  if (nnzb > 0 && (!cols || !vals_flat)) fail(FCU_ERR_BAD_ARG, "bad block CSR arrays");
+  DevIn<uint32_t> rp(ctx, row_ptr, n_nodes + 1);
+  DevIn<uint32_t> ci(ctx, cols, nnzb);
+  DevIn<double> va(ctx, vals_flat, 9 * nnzb);
+  DevIn<double> di(ctx, dinv_flat, dinv_flat ? 9 * n_nodes : 0);
+  return bsr3_create_impl(ctx, n_nodes, rp.p, ci.p, nnzb, va.p, di.p);
+}
+
+int fcu_bsr3_create(fcu_ctx ctx, int64_t n_nodes, const uint32_t* row_ptr, const uint32_t* cols,
+                    const double* vals_flat, const double* dinv_flat, fcu_matrix* out) {
+  if (!out) return FCU_ERR_BAD_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    check_ctx(ctx);
+    *out = bsr3_from_caller(ctx, n_nodes, row_ptr, cols, vals_flat, dinv_flat);
+  });
+}
+
+int fcu_bsr3_jacobi_smooth(fcu_ctx ctx, fcu_matrix m, const double* r, double* z, int64_t sweeps, double omega,
+                           int zero_initial_z) {
+  return guarded(ctx, [&] {
+    if (!m || m->bs != 3 || !r || !z || sweeps < 0) fail(FCU_ERR_BAD_ARG, "bad arguments");
+    if (sweeps == 0) return;
+    DevIn<double> rd(ctx, r, m->n);
+    DevOut<double> zo(z, m->n, zero_initial_z ? nullptr : z, ctx);
+    bsr3_jacobi_smooth_impl(m, rd.p, zo.p, sweeps, omega, zero_initial_z != 0);
+    zo.finish(ctx);
+    sync(ctx);
+  });
+}
+
+int fcu_solve_bsr3_pcg(fcu_ctx ctx, int64_t n_nodes, const uint32_t* row_ptr, const uint32_t* cols,
+                       const double* vals_flat, const double* dinv_flat, const double* b, const double* x0,
+                       double rtol, int64_t max_iter, double* x, fcu_solve_info* info) {
+  int status = FCU_OK;
+  int rc = guarded(ctx, [&] {
+    check_ctx(ctx);
+    if (!b || !x || !dinv_flat) fail(FCU_ERR_BAD_ARG, "null argument");
+    if (max_iter < 0) fail(FCU_ERR_BAD_ARG, "max_iter must be >= 0");
+    struct Own {
+      fcu_matrix p;
+      ~Own() { if (p) matrix_release(p); }
+    } m{bsr3_from_caller(ctx, n_nodes, row_ptr, cols, vals_flat, dinv_flat)};
+    const i64 n = 3 * n_nodes;
+    DevIn<double> bd(ctx, b, n);
+    DevIn<double> xd0(ctx, x0, x0 ? n : 0);
+    DevOut<double> xo(x, n);
+    status = run_pcg(m.p, bd.p, xd0.p, xo.p, rtol, max_iter, FCU_FP64, true, nullptr, info);
+    xo.finish(ctx);
+    sync(ctx);
+  });
+  return rc != FCU_OK ? rc : status;
+}
+
+int fcu_matrix_block_jacobi(fcu_ctx ctx, fcu_matrix m, int enable) {
+  return guarded(ctx, [&] {
+    if (!m || m->bs != 3) fail(FCU_ERR_BAD_ARG, "needs a 3x3 block matrix");
+    if (!m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    matrix_block_jacobi_impl(m, enable != 0);
+    sync(ctx);
+  });
+}
+
+int fcu_matrix_export_bsr3(fcu_ctx ctx, fcu_matrix m, uint32_t* row_ptr, uint32_t* cols, double* vals_flat,
+                           double* dinv_flat) {
+  return guarded(ctx, [&] {
+    if (!m || m->bs != 3) fail(FCU_ERR_BAD_ARG, "needs a 3x3 block matrix");
+    DevOut<uint32_t> rp(row_ptr, row_ptr ? m->nnodes + 1 : 0);
+    DevOut<uint32_t> ci(cols, cols ? m->nnzb : 0);
+    DevOut<double> va(vals_flat, vals_flat ? 9 * m->nnzb : 0);
+    DevOut<double> di(dinv_flat, dinv_flat ? 9 * m->nnodes : 0);
+    matrix_export_bsr3_impl(m, rp.p, ci.p, va.p, di.p);
+    rp.finish(ctx);
+    ci.finish(ctx);
+    va.finish(ctx);
+    di.finish(ctx);
     sync(ctx);
   });
 }

@@ -309,6 +309,128 @@ __global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
 }
 
 // ---------------------------------------------------------------------------
+// Mass matrices (mass.rs:10-250). Entry (a, b) of cell c is s_c F[a][b]:
+// s_c = rho * measure (area |det|/2, volume |det|/6; the P2 products already
+// carry the reference volume, so there the measure is |det|), times the
+// per-cell coefficient when one is given; F = 1/6, 1/12 (triangle), 1/10,
+// 1/20 (tetrahedron) or the exact P2 reference products. Each product is
+// rounded before it is summed, in ascending cell order, as the triplet
+// assembly sums it. The vector space stores s F I_3 per block (the same
+// scalar on each displacement component, mass.rs:118-123).
+// ---------------------------------------------------------------------------
+
+struct MassTable {
+  double F[100];  // F[a * K + b]
+};
+
+template <int K, int DIM, int BS>
+__global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
+    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+    const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
+    const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ coef, double rho,
+    const MassTable tab, i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
+  __shared__ double s_all[WARPS][32];
+  __shared__ int a_all[WARPS][32];
+  __shared__ unsigned short ent_all[WARPS][32 * K];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const i64 nwarps = (i64)gridDim.x * WARPS;
+  for (i64 row = (i64)blockIdx.x * WARPS + wib; row < nrows; row += nwarps) {
+    const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
+    const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
+    const i64 ebase = (i64)K * cs;
+    const bool staged = nct <= 32;
+    if (staged)
+      for (int q = lane; q < K * nct; q += 32) ent_all[wib][q] = slot_ent[ebase + q];
+    __syncwarp();
+    int run = 0;
+    for (int g0 = 0; g0 < L; g0 += 32) {
+      const int s = g0 + lane;
+      const int cnt = (s < L) ? (int)slot_cnt[rs + s] : 0;
+      int tot;
+      const int off = warp_excl_scan(cnt, lane, &tot);
+      i64 e = ebase + run + off;
+      const i64 e1 = e + cnt;
+      run += tot;
+      double acc = 0.0;
+      for (int ch = 0; ch < nct; ch += 32) {
+        const int t = ch + lane;
+        if (t < nct) {
+          const int cc = contrib[cs + t];
+          const int c = cc >> 4;
+          int v[DIM + 1];
+#pragma unroll
+          for (int i = 0; i <= DIM; ++i) v[i] = cn[(i64)c * K + i];
+          const double det = (DIM == 3) ? tet_geometry(X, v).det : tri_geometry(X, v).det;
+          const double meas = (K == 10) ? fabs(det) : (DIM == 3 ? (1.0 / 6.0) * fabs(det) : 0.5 * fabs(det));
+          double sc = __dmul_rn(rho, meas);
+          if (coef) sc = __dmul_rn(sc, coef[c]);
+          s_all[wib][lane] = sc;
+          a_all[wib][lane] = cc & 15;
+        }
+        __syncwarp();
+        while (e < e1) {
+          const unsigned ent = staged ? ent_all[wib][e - ebase] : slot_ent[e];
+          const int tl = (int)(ent >> 4);
+          if (tl >= ch + 32) break;
+          acc = __dadd_rn(acc, __dmul_rn(s_all[wib][tl - ch], tab.F[a_all[wib][tl - ch] * K + (ent & 15)]));
+          ++e;
+        }
+        __syncwarp();
+      }
+      if (s < L) {
+        if (BS == 1) {
+          v64[rs + s] = acc;
+          v32[rs + s] = (float)acc;
+        } else {
+          const i64 o = 9 * ((i64)rs + s);
+#pragma unroll
+          for (int q = 0; q < 9; ++q) {
+            const double v = (q % 4 == 0) ? acc : 0.0;
+            v64[o + q] = v;
+            v32[o + q] = (float)v;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Exact products of the P2 basis on the reference tetrahedron
+// (mass.rs:195-250): every basis function is a sum of barycentric monomials
+// (corner i: 2 l_i^2 - l_i; edge (i, j): 4 l_i l_j), and
+// int l0^m0 l1^m1 l2^m2 l3^m3 = m0! m1! m2! m3! / (m0+m1+m2+m3+3)!.
+// Node order: corners 0-3, then edges 01, 12, 02, 03, 13, 23.
+void p2_mass_products(double out[100]) {
+  const double fact[12] = {1.0, 1.0, 2.0, 6.0, 24.0, 120.0, 720.0, 5040.0, 40320.0, 362880.0, 3628800.0, 39916800.0};
+  struct Term { int m[4]; double c; };
+  std::vector<std::vector<Term>> basis(10);
+  for (int i = 0; i < 4; ++i) {
+    Term sq{{0, 0, 0, 0}, 2.0}, lin{{0, 0, 0, 0}, -1.0};
+    sq.m[i] = 2;
+    lin.m[i] = 1;
+    basis[i] = {sq, lin};
+  }
+  const int edges[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+  for (int e = 0; e < 6; ++e) {
+    Term t{{0, 0, 0, 0}, 4.0};
+    t.m[edges[e][0]] = 1;
+    t.m[edges[e][1]] = 1;
+    basis[4 + e] = {t};
+  }
+  for (int a = 0; a < 10; ++a)
+    for (int b = 0; b < 10; ++b) {
+      double acc = 0.0;
+      for (const Term& ta : basis[a])
+        for (const Term& tb : basis[b]) {
+          int m[4], deg = 0;
+          for (int q = 0; q < 4; ++q) { m[q] = ta.m[q] + tb.m[q]; deg += m[q]; }
+          acc += ta.c * tb.c * fact[m[0]] * fact[m[1]] * fact[m[2]] * fact[m[3]] / fact[deg + 3];
+        }
+      out[a * 10 + b] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Dirichlet elimination (poisson.rs:222-263, elasticity.rs:188-227)
 // ---------------------------------------------------------------------------
 
@@ -537,6 +659,42 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
                                                             s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p,
                                                             s->mesh->coords.p, cellE_dev, lam, mu, s->nnodes,
                                                             m->val64.p, m->val32.p);
+  LAUNCH_CHECK(ctx);
+}
+
+void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev) {
+  fcu_space s = m->space;
+  fcu_ctx ctx = m->ctx;
+  fcu_mesh me = s->mesh;
+  MassTable tab{};
+  if (s->kind == FCU_SPACE_P2) {
+    p2_mass_products(tab.F);
+  } else {
+    const int K = s->k;
+    const double dg = (K == 3) ? 1.0 / 6.0 : 1.0 / 10.0, od = (K == 3) ? 1.0 / 12.0 : 1.0 / 20.0;
+    for (int a = 0; a < K; ++a)
+      for (int b = 0; b < K; ++b) tab.F[a * K + b] = (a == b) ? dg : od;
+  }
+  const int nb = assembly_blocks(ctx, s->nnodes);
+  const int* cn = s->cell_nodes.p;
+  const double* X = me->coords.p;
+  if (s->kind == FCU_SPACE_P2) {
+    k_assemble_mass<10, 3, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                                   s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
+                                                                   tab, s->nnodes, m->val64.p, m->val32.p);
+  } else if (s->kind == FCU_SPACE_P1_VEC3) {
+    k_assemble_mass<4, 3, 3><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                                  s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
+                                                                  tab, s->nnodes, m->val64.p, m->val32.p);
+  } else if (me->dim == 3) {
+    k_assemble_mass<4, 3, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                                  s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
+                                                                  tab, s->nnodes, m->val64.p, m->val32.p);
+  } else {
+    k_assemble_mass<3, 2, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                                  s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
+                                                                  tab, s->nnodes, m->val64.p, m->val32.p);
+  }
   LAUNCH_CHECK(ctx);
 }
 

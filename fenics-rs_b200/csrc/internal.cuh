@@ -164,10 +164,19 @@ struct fcu_matrix_s {
   i64 n_dirichlet = 0;
   DBuf<double> diag_count;        // n: diagonal value for eliminated dofs
   bool bc_applied = false;
+  bool drop_zeros = false;  // folded (eigen.rs:55-79): export omits zero-valued entries
+  bool comp_diag = false;   // vector mass (mass.rs:118-123): only same-component entries are in the pattern
   bool has_values = false;
   DBuf<unsigned char> diag_struct;  // node rows whose diagonal is in the raw pattern
   DBuf<i64> csc_colptr, csc_rowidx; // wrapped CSC: the caller's layout, for export
   DBuf<int> csr_of;                 // wrapped CSC: CSC position -> CSR slot
+  // 3x3 block-Jacobi preconditioner (inverse diagonal blocks, row-major, one
+  // per block row): when present, the FP64 PCG applies it instead of the
+  // point Jacobi diagonal (bsr3_apply_dinv of solve_bsr3_pcg_gpu).
+  DBuf<double> bdinv;
+  bool block_jacobi = false;  // bdinv derived from the values at every solve
+  int max_row_own = 0;  // longest block row of a wrapped block CSR matrix
+  bool missing_diag = false;  // a wrapped block row without a diagonal block
   Workspace* ws = nullptr;
   BatchWorkspace* bws = nullptr;
   ~fcu_matrix_s();

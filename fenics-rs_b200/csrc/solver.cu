@@ -40,6 +40,8 @@
 
 #include "internal.cuh"
 
+void refresh_block_jacobi(fcu_matrix m);  // bsr3.cu
+
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
@@ -249,10 +251,13 @@ __device__ __forceinline__ void spmv_rows(const int* __restrict__ rp, const int*
   }
 }
 
+// cg.rs:102-107: |p.Ap| < 1e-30 is a breakdown (Err). The GPU solvers
+// (gpu.rs:1326-1329, 1034-1037) stop with Ok when p.Ap <= 1e-30; the
+// iteration counts as done.
 __device__ __forceinline__ void set_alpha(CgState* st, double pap) {
-  if (!st->gpu_semantics && fabs(pap) < 1e-30) {
+  if (st->gpu_semantics ? !(pap > 1e-30) : fabs(pap) < 1e-30) {
     st->done = 1;
-    st->status = FCU_ERR_BREAKDOWN;
+    st->status = st->gpu_semantics ? FCU_OK : FCU_ERR_BREAKDOWN;
     st->iter += 1;
   } else {
     st->alpha = st->rz / pap;
@@ -689,6 +694,66 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
   }
 }
 
+// Block-Jacobi variant (FP64): one thread per block row applies the inverse
+// diagonal block to the row's three residual components (bsr3_apply_dinv).
+__global__ void __launch_bounds__(VBLOCK) k_update_block(i64 nn, double* __restrict__ x, double* __restrict__ r,
+                                                         const double* __restrict__ p, const double* __restrict__ ap,
+                                                         const double* __restrict__ bdinv, double* __restrict__ z,
+                                                         CgState* st, double* partials) {
+  grid_dep_sync();
+  if (st->done || st->pause) return;
+  const double alpha = st->alpha;
+  double rz = 0.0, rr = 0.0;
+  for (i64 w = blockIdx.x * (i64)blockDim.x + threadIdx.x; w < nn; w += (i64)gridDim.x * blockDim.x) {
+    double rn[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const i64 i = 3 * w + a;
+      x[i] += alpha * p[i];
+      rn[a] = r[i] - alpha * ap[i];
+      r[i] = rn[a];
+      rr += rn[a] * rn[a];
+    }
+    const double* D = bdinv + 9 * w;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double zi = D[3 * a] * rn[0] + D[3 * a + 1] * rn[1] + D[3 * a + 2] * rn[2];
+      z[3 * w + a] = zi;
+      rz += rn[a] * zi;
+    }
+  }
+  double v[2] = {rz, rr}, tot[2];
+  if (grid_reduce<2>(v, partials, st->ticket[1], tot) && threadIdx.x == 0) decide_after_update(st, tot[0], tot[1]);
+}
+
+// After the initial residual: z = D_b^-1 r and r.z for the block-Jacobi
+// preconditioner (the point-Jacobi z the residual kernel wrote is replaced).
+__global__ void __launch_bounds__(VBLOCK) k_block_init(i64 nn, const double* __restrict__ r,
+                                                       const double* __restrict__ bdinv, double* __restrict__ z,
+                                                       CgState* st, double* partials) {
+  grid_dep_sync();
+  double rz = 0.0;
+  for (i64 w = blockIdx.x * (i64)blockDim.x + threadIdx.x; w < nn; w += (i64)gridDim.x * blockDim.x) {
+    const double* D = bdinv + 9 * w;
+    const double r0 = r[3 * w], r1 = r[3 * w + 1], r2 = r[3 * w + 2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double zi = D[3 * a] * r0 + D[3 * a + 1] * r1 + D[3 * a + 2] * r2;
+      z[3 * w + a] = zi;
+      rz += r[3 * w + a] * zi;
+    }
+  }
+  double v[1] = {rz}, tot[1];
+  if (grid_reduce<1>(v, partials, st->ticket[3], tot) && threadIdx.x == 0) st->rz = tot[0];
+}
+
+// Point diagonal taken from the inverse blocks (read only by the residual
+// kernel, whose z the block-Jacobi pass overwrites).
+__global__ void k_invd_from_blocks(const double* __restrict__ bdinv, i64 n, double* __restrict__ invd) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    invd[i] = bdinv[9 * (i / 3) + 4 * (i % 3)];
+}
+
 // --- residual: r = b - A64 x, z = D^-1 r (init, and the mixed replacement) ----
 template <int BS, class T>
 struct EmitRes {
@@ -950,7 +1015,7 @@ void launch_pdl_cfg(fcu_ctx ctx, void (*kern)(KArgs...), int grid, int block, si
 template <int DIFF, class T>
 void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
   fcu_ctx ctx = m->ctx;
-  const int max_row = m->space ? m->space->max_row : 32;
+  const int max_row = m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32);
   const int cap = TILE_ROWS * max_row;
   const int nstage = w->stages[sizeof(T) == 4 ? 1 : 0];
   const size_t smem = nstage * tile_stage_bytes<T>(cap);
@@ -1028,8 +1093,12 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       else
         DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, nr, w->pa64.p, w->ap64.p,
                       w->st.p, w->partials.p);
-      launch_pdl(ctx, k_update<double>, w->vgrid, n, w->x.p, w->r.p, w->pa64.p, w->ap64.p, w->invd.p, w->z64.p,
-                 w->st.p, w->partials.p);
+      if (m->bdinv.p)
+        launch_pdl(ctx, k_update_block, w->vgrid, m->nnodes, w->x.p, w->r.p, w->pa64.p, w->ap64.p, m->bdinv.p,
+                   w->z64.p, w->st.p, w->partials.p);
+      else
+        launch_pdl(ctx, k_update<double>, w->vgrid, n, w->x.p, w->r.p, w->pa64.p, w->ap64.p, w->invd.p, w->z64.p,
+                   w->st.p, w->partials.p);
     } else {
       launch_pdl(ctx, k_direction<float>, w->vgrid, n, w->pa32.p, w->z32.p, w->st.p);
       if (m->bs == 3 && use_tiled_spmv())
@@ -1097,7 +1166,9 @@ double pcg_bytes_per_iter(fcu_matrix m, bool mixed) {
   const double mat = (double)m->nnzb * (bs2 * w + 4.0) + 4.0 * (double)(m->nnodes + 1);
   const double spmv_vec = 4.0 * n * w;
   const double update = n * (8 + 8 + 8 + 8) + n * (w + w + 8) + n * w;
-  return mat + spmv_vec + update;
+  // block-Jacobi reads 9 inverse-block values per block row instead of 3 diagonal ones
+  const double block = (!mixed && m->bdinv.p) ? 2.0 * n * 8.0 : 0.0;
+  return mat + spmv_vec + update + block;
 }
 
 void ensure_inv_diag(fcu_matrix m, Workspace* w) {
@@ -1132,6 +1203,9 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
   fcu_ctx ctx = m->ctx;
   const bool mixed = precision == FCU_MIXED;
   if (mixed && !m->val32.p) fail(FCU_ERR_BAD_ARG, "matrix has no FP32 copy");
+  if (mixed && m->bdinv.p) fail(FCU_ERR_UNSUPPORTED, "block-Jacobi preconditioning runs in FP64");
+  if (m->block_jacobi && !inv_diag_dev) refresh_block_jacobi(m);
+  if (mixed && m->missing_diag) fail(FCU_ERR_UNSUPPORTED, "the mixed operator needs every diagonal block");
   Workspace* w = ensure_ws(m, mixed);
   const i64 n = m->n, nr = m->nnodes;
   const int g = w->grid;
@@ -1139,9 +1213,14 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
   CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
-  if (inv_diag_dev) CUDA_CHECK(cudaMemcpyAsync(w->invd.p, inv_diag_dev, n * sizeof(double), cudaMemcpyDeviceToDevice,
-                                               ctx->stream));
-  else ensure_inv_diag(m, w);
+  if (inv_diag_dev) {
+    CUDA_CHECK(cudaMemcpyAsync(w->invd.p, inv_diag_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  } else if (m->bdinv.p) {
+    k_invd_from_blocks<<<grid_for(n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(m->bdinv.p, n, w->invd.p);
+    LAUNCH_CHECK(ctx);
+  } else {
+    ensure_inv_diag(m, w);
+  }
   if (mixed) build_rowsum32(m);
   tune_spmv(m, w, mixed);  // first solve in this precision only
 
@@ -1162,6 +1241,8 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
   else
     DISPATCH_ROWS(m->bs, w->vpr, g, K_INIT64, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
                   w->r.p, w->z64.p, w->pa64.p, n, w->st.p, w->partials.p);
+  if (!mixed && m->bdinv.p)
+    launch_pdl(ctx, k_block_init, w->vgrid, m->nnodes, w->r.p, m->bdinv.p, w->z64.p, w->st.p, w->partials.p);
   CUDA_CHECK(cudaMemcpyAsync(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
   bool zero_rhs = gpu_semantics && w->host_st->bnorm == 0.0;
@@ -1214,6 +1295,17 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
   }
   if (!hs.done) return gpu_semantics ? FCU_OK : FCU_ERR_NO_CONVERGENCE;
   return hs.status;
+}
+
+// Drops the captured iteration graphs (their kernels depend on the
+// preconditioner the matrix carries).
+void invalidate_graphs(fcu_matrix m) {
+  if (!m->ws) return;
+  for (auto& g : m->ws->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
 }
 
 void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev) {
@@ -1307,7 +1399,7 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   if (m->bs == 3 && use_tiled_spmv()) {
     int optin = 0;
     CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    const int max_row = m->space ? m->space->max_row : 32;
+    const int max_row = m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32);
     const size_t stage = mixed ? tile_stage_bytes<float>(TILE_ROWS * max_row)
                                : tile_stage_bytes<double>(TILE_ROWS * max_row);
     int best = w->stages[k];

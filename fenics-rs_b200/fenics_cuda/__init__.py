@@ -10,8 +10,12 @@ meaning and error behaviour follow GlassOnTin/fenics-rs:
                            assemble_elasticity_stiffness_3d,
                            assemble_elasticity_body_force_3d,
                            apply_vector_dirichlet_bc, assemble_surface_traction_3d
+  crates/fenics-assembly   assemble_mass_2d/3d, assemble_elasticity_mass_3d (mass.rs)
   crates/fenics-solver     solve_cg, solve_csr_cg_gpu, solve_cg_gpu_or_cpu,
-                           solve_poisson_2d/3d, solve_elasticity_3d
+                           solve_poisson_2d/3d, solve_elasticity_3d,
+                           add_scaled_matrices, TransientHeatSolver,
+                           solve_transient_heat_2d, fold_dirichlet,
+                           solve_vibration_modes(_with_inner)
 
 All compute runs in CUDA kernels on the device; there is no CPU fallback (a
 missing library or device raises). Arrays may be numpy (host) or torch CUDA
@@ -26,8 +30,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (FCU_FP64, FCU_MIXED, FCU_SPACE_P1, FCU_SPACE_P1_VEC3, FCU_SPACE_P2, FCU_SRC_CONSTANT,
-                   FCU_SRC_NODAL, FCU_SRC_SIN_PRODUCT, SolveInfo)
+from ._abi import (FCU_BACKWARD_EULER, FCU_CRANK_NICOLSON, FCU_FP64, FCU_MIXED, FCU_SPACE_P1, FCU_SPACE_P1_VEC3,
+                   FCU_SPACE_P2, FCU_SRC_CONSTANT, FCU_SRC_NODAL, FCU_SRC_SIN_PRODUCT, SolveInfo)
 
 __all__ = [
     "Context", "Mesh", "FunctionSpace", "Matrix", "CscMatrix", "FcuError", "CgError",
@@ -38,6 +42,10 @@ __all__ = [
     "assemble_elasticity_body_force_3d", "apply_vector_dirichlet_bc", "assemble_surface_traction_3d",
     "extract_boundary_facets", "solve_cg", "solve_csr_cg_gpu", "solve_cg_gpu_or_cpu", "GpuSolveResult",
     "solve_poisson_2d", "solve_poisson_3d", "solve_elasticity_3d", "spmv",
+    "assemble_mass_2d", "assemble_mass_3d", "assemble_elasticity_mass_3d", "assemble_mass_p2_3d",
+    "add_scaled_matrices", "TimeSteppingScheme", "TransientHeatSolver", "TransientHeatSolution",
+    "solve_transient_heat_2d", "fold_dirichlet", "VibrationMode", "solve_vibration_modes",
+    "solve_vibration_modes_with_inner", "GpuBsr3Context", "solve_bsr3_pcg_gpu", "spmv_bsr3_multi_gpu",
     "FCU_FP64", "FCU_MIXED",
 ]
 
@@ -429,6 +437,63 @@ class Matrix:
         pc, kc = _ptr(cell_E, np.float64)
         _check(self.ctx, _L().fcu_assemble_elasticity(self.ctx.h, self.h, float(E), float(nu), pc))
         return self
+
+    def assemble_mass(self, rho=1.0, coef=None):
+        """Mass matrix (mass.rs:10-250): rho = density of the vector space,
+        1 for the scalar reference matrices; coef multiplies per cell."""
+        pc, kc = _ptr(coef, np.float64)
+        _check(self.ctx, _L().fcu_assemble_mass(self.ctx.h, self.h, float(rho), pc))
+        return self
+
+    def clone(self) -> "Matrix":
+        h = C.c_void_p()
+        _check(self.ctx, _L().fcu_matrix_clone(self.ctx.h, self.h, C.byref(h)))
+        return Matrix(self.ctx, self.space, h)
+
+    def set_add_scaled(self, a: "Matrix", b: "Matrix", alpha):
+        """self = a + alpha * b on one pattern (add_scaled_matrices, transient.rs:72-97)."""
+        _check(self.ctx, _L().fcu_matrix_add_scaled(self.ctx.h, self.h, a.h, b.h, float(alpha)))
+        return self
+
+    def scale(self, s):
+        _check(self.ctx, _L().fcu_matrix_scale(self.ctx.h, self.h, float(s)))
+        return self
+
+    def fold_dirichlet(self, fixed_dofs, unit_diag: bool):
+        """fold_dirichlet (eigen.rs:55-79), in place."""
+        pd, kd = _ptr(fixed_dofs, np.int64)
+        _check(self.ctx, _L().fcu_matrix_fold_dirichlet(self.ctx.h, self.h, len(fixed_dofs), pd, 1 if unit_diag else 0))
+        return self
+
+    @classmethod
+    def from_bsr3(cls, ctx: Context, n_nodes, row_ptr, cols, vals_flat, dinv_flat=None) -> "Matrix":
+        """A resident 3x3 block CSR matrix (GpuBsr3Context::new, gpu.rs:453-494)."""
+        h = C.c_void_p()
+        pr, kr = _ptr(row_ptr, np.uint32)
+        pc, kc = _ptr(cols, np.uint32)
+        pv, kv = _ptr(vals_flat, np.float64)
+        pd, kd = _ptr(dinv_flat, np.float64)
+        _check(ctx, _L().fcu_bsr3_create(ctx.h, int(n_nodes), pr, pc, pv, pd, C.byref(h)))
+        return cls(ctx, None, h)
+
+    def block_jacobi(self, enable=True):
+        """Block-Jacobi preconditioning from the 3x3 diagonal blocks (FP64 PCG)."""
+        _check(self.ctx, _L().fcu_matrix_block_jacobi(self.ctx.h, self.h, 1 if enable else 0))
+        return self
+
+    def export_bsr3(self, with_dinv=False):
+        """(row_ptr u32, cols u32, vals_flat, dinv_flat or None): the reference's
+        block CSR inputs of solve_bsr3_pcg_gpu."""
+        nn = self.n // 3
+        rp = np.empty(nn + 1, np.uint32)
+        _check(self.ctx, _L().fcu_matrix_export_bsr3(self.ctx.h, self.h, rp.ctypes.data, None, None, None))
+        nb = int(rp[-1])
+        ci = np.empty(nb, np.uint32)
+        va = np.empty(9 * nb)
+        di = np.empty(9 * nn) if with_dinv else None
+        _check(self.ctx, _L().fcu_matrix_export_bsr3(self.ctx.h, self.h, None, ci.ctypes.data, va.ctypes.data,
+                                                     di.ctypes.data if di is not None else None))
+        return rp, ci, va, di
 
     def apply_dirichlet(self, b, dofs, vals):
         """In place on the matrix and b (numpy array or CUDA tensor)."""
@@ -982,3 +1047,418 @@ def solve_elasticity_3d(mesh: Mesh, material: ElasticMaterial, body_force, bc: V
     M.apply_dirichlet(f, d, v)
     x, info = M.pcg(f, tol=tol, max_iter=max_iter, precision=precision)
     return ElasticitySolution(x, mesh.coords + x.reshape(-1, 3), info.iterations, info.residual)
+
+
+# ---------------------------------------------------------------------------
+# mass matrices, transient heat, vibration modes (mass.rs, transient.rs,
+# heat_solver.rs, eigen.rs)
+# ---------------------------------------------------------------------------
+
+def assemble_mass_2d(mesh: Mesh, ctx: Context | None = None) -> CscMatrix:
+    """assemble_mass_2d (mass.rs:10-44)."""
+    if mesh.dim != 2:
+        raise ValueError("triangle mesh expected")
+    return _assembled(FCU_SPACE_P1, mesh, ctx, lambda M: M.assemble_mass(1.0))
+
+
+def assemble_mass_3d(mesh: Mesh, ctx: Context | None = None) -> CscMatrix:
+    """assemble_mass_3d (mass.rs:47-81)."""
+    if mesh.dim != 3:
+        raise ValueError("tetrahedron mesh expected")
+    return _assembled(FCU_SPACE_P1, mesh, ctx, lambda M: M.assemble_mass(1.0))
+
+
+def assemble_elasticity_mass_3d(mesh: Mesh, density, ctx: Context | None = None) -> CscMatrix:
+    """assemble_elasticity_mass_3d (mass.rs:84-127)."""
+    if mesh.dim != 3:
+        raise ValueError("tetrahedron mesh expected")
+    return _assembled(FCU_SPACE_P1_VEC3, mesh, ctx, lambda M: M.assemble_mass(float(density)))
+
+
+def assemble_mass_p2_3d(mesh: Mesh, density=1.0, ctx: Context | None = None) -> CscMatrix:
+    """Scalar P2 mass from the exact reference products of
+    assemble_elasticity_mass_p2_3d (mass.rs:137-250), on this build's P2
+    numbering (vertices, then edges)."""
+    return _assembled(FCU_SPACE_P2, mesh, ctx, lambda M: M.assemble_mass(float(density)))
+
+
+def _as_matrix(ctx, mat):
+    """(Matrix, owned) for a Matrix or a CscMatrix."""
+    if isinstance(mat, Matrix):
+        return mat, False
+    return Matrix.from_csc(ctx, mat), True
+
+
+def add_scaled_matrices(a, b, alpha, ctx: Context | None = None) -> CscMatrix:
+    """add_scaled_matrices (transient.rs:72-97): a + alpha * b. Both operands
+    must have the same pattern (FcuError FCU_ERR_UNSUPPORTED otherwise)."""
+    ctx = ctx or default_context()
+    A, oa = _as_matrix(ctx, a)
+    B, ob = _as_matrix(ctx, b)
+    try:
+        out = A.clone()
+        out.set_add_scaled(A, B, alpha)
+        res = out.export_csc()
+        out.close()
+    finally:
+        if oa:
+            A.close()
+        if ob:
+            B.close()
+    return res
+
+
+def fold_dirichlet(mat, fixed_dofs, unit_diag: bool, ctx: Context | None = None) -> CscMatrix:
+    """fold_dirichlet (eigen.rs:55-79): constrained rows and columns dropped,
+    unit diagonal on them when unit_diag, zero entries dropped."""
+    ctx = ctx or default_context()
+    A, oa = _as_matrix(ctx, mat)
+    try:
+        F = A.clone() if not oa else A
+        F.fold_dirichlet(np.asarray(fixed_dofs, dtype=np.int64), unit_diag)
+        res = F.export_csc()
+        if F is not A:
+            F.close()
+    finally:
+        if oa:
+            A.close()
+    return res
+
+
+class TimeSteppingScheme:
+    """TimeSteppingScheme (transient.rs:11-18)."""
+    BackwardEuler = FCU_BACKWARD_EULER
+    CrankNicolson = FCU_CRANK_NICOLSON
+
+
+class _Stepper:
+    """A device stepper (fcu_transient) for one (mass, stiffness) pair."""
+
+    def __init__(self, ctx: Context, M: Matrix, K: Matrix, scheme: int, dt: float):
+        self.ctx = ctx
+        h = C.c_void_p()
+        _check(ctx, _L().fcu_transient_create(ctx.h, M.h, K.h, int(scheme), float(dt), C.byref(h)))
+        self.h = h
+
+    def set_dirichlet(self, dofs, vals):
+        pd, kd = _ptr(dofs, np.int64)
+        pv, kv = _ptr(vals, np.float64)
+        _check(self.ctx, _L().fcu_transient_set_dirichlet(self.ctx.h, self.h, len(dofs), pd, pv))
+
+    def step(self, u_n, f_n, f_next, u_next, tol, max_iter, precision):
+        pu, ku = _ptr(u_n, np.float64)
+        p0, k0 = _ptr(f_n, np.float64)
+        p1, k1 = _ptr(f_next, np.float64)
+        po, ko = _ptr(u_next)
+        info = SolveInfo()
+        rc = _L().fcu_transient_step(self.ctx.h, self.h, pu, p0, p1, po, float(tol), int(max_iter), precision,
+                                     C.byref(info))
+        _check(self.ctx, rc)
+        return info
+
+    def close(self):
+        if getattr(self, "h", None):
+            _L().fcu_transient_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TransientHeatSolver:
+    """TransientHeatSolver (transient.rs:21-68). step() solves the SPD system
+    (M + theta dt K) u_{n+1} = rhs with Jacobi-PCG to `tol` (relative
+    residual) from u_n, where the reference factorises densely; the device
+    matrices of a (mass, stiffness) pair are formed once and reused."""
+
+    def __init__(self, scheme, dt, ctx: Context | None = None, tol=1e-12, max_iter=100000, precision=FCU_FP64):
+        self.scheme, self.dt = int(scheme), float(dt)
+        self.ctx = ctx or default_context()
+        self.tol, self.max_iter, self.precision = tol, max_iter, precision
+        self._key = None
+        self._stepper = None
+        self._held = []
+        self.last_info = None
+
+    def _prepare(self, mass, stiff):
+        key = (id(mass), id(stiff))
+        if self._key != key:
+            self.close()
+            M, om = _as_matrix(self.ctx, mass)
+            K, ok = _as_matrix(self.ctx, stiff)
+            self._stepper = _Stepper(self.ctx, M, K, self.scheme, self.dt)
+            self._held = [x for x, owned in ((M, om), (K, ok)) if owned]
+            self._key = key
+        return self._stepper
+
+    def step(self, mass_mat, stiff_mat, u_n, f_n, f_next):
+        st = self._prepare(mass_mat, stiff_mat)
+        out = np.empty(len(u_n)) if not _is_torch(u_n) else u_n.new_empty(u_n.shape)
+        self.last_info = st.step(u_n, f_n, f_next, out, self.tol, self.max_iter, self.precision)
+        return out
+
+    def close(self):
+        if self._stepper is not None:
+            self._stepper.close()
+        for m in self._held:
+            m.close()
+        self._stepper, self._held, self._key = None, [], None
+
+
+@dataclass
+class TransientHeatSolution:
+    """heat_solver.rs:13-19"""
+    time_steps: list
+    temperature_history: list
+    final_temperature: np.ndarray
+    iterations: list = field(default_factory=list)
+
+
+def solve_transient_heat_2d(mesh: Mesh, diffusivity, u_initial, bcs, dt, num_steps, scheme, heat_source=None,
+                            ctx: Context | None = None, tol=1e-12, max_iter=100000, precision=FCU_FP64,
+                            keep_history=True, vectorized_source=False) -> TransientHeatSolution:
+    """solve_transient_heat_2d (heat_solver.rs:23-104): P1 mass and
+    diffusivity-scaled stiffness on the device, Dirichlet values written into
+    the state before and after every step. heat_source(t, point) is called
+    per vertex like the reference's closure (or once per time with the
+    (nv, 2) coordinates when vectorized_source); None means no source."""
+    import torch
+    ctx = ctx or default_context()
+    n = mesh.num_vertices()
+    if len(u_initial) != n:
+        raise ValueError(f"Initial temperature size {len(u_initial)} != mesh vertices {n}")
+    V = FunctionSpace(ctx, mesh, FCU_SPACE_P1)
+    M = Matrix(ctx, V).assemble_mass(1.0)
+    K = Matrix(ctx, V).assemble_stiffness(None).scale(diffusivity)
+    st = _Stepper(ctx, M, K, int(scheme), float(dt))
+    dofs, vals = [], []
+    for bc in bcs:
+        dofs.extend(int(d) for d in bc.dofs)
+        vals.extend(float(v) for v in bc.values)
+    if dofs:
+        st.set_dirichlet(np.asarray(dofs, np.int64), np.asarray(vals, np.float64))
+    dev = torch.device("cuda", ctx.device)
+    u = torch.as_tensor(np.asarray(u_initial, dtype=np.float64)).to(dev)
+    un = torch.empty_like(u)
+    coords = mesh.coords
+
+    def source(t):
+        if heat_source is None:
+            return None
+        if vectorized_source:
+            return np.ascontiguousarray(heat_source(t, coords), dtype=np.float64)
+        return np.array([heat_source(t, coords[i]) for i in range(n)], dtype=np.float64)
+
+    times, history, iters = [0.0], [np.asarray(u_initial, dtype=np.float64).copy()] if keep_history else [], []
+    try:
+        for step in range(1, num_steps + 1):
+            t_curr, t_next = (step - 1) * dt, step * dt
+            info = st.step(u, source(t_curr), source(t_next), un, tol, max_iter, precision)
+            iters.append(int(info.iterations))
+            u, un = un, u
+            times.append(t_next)
+            if keep_history:
+                history.append(u.cpu().numpy())
+        final = u.cpu().numpy()
+    finally:
+        st.close()
+        M.close()
+        K.close()
+        V.close()
+    if not keep_history:
+        history = []
+    return TransientHeatSolution(times, history, final, iters)
+
+
+@dataclass
+class VibrationMode:
+    """VibrationMode (eigen.rs:10-19)"""
+    frequency_hz: float
+    omega_rad_s: float
+    eigenvalue: float
+    mode_shape: np.ndarray
+
+
+class _DeviceArray:
+    """A raw device pointer exposed through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, n: int, readonly: bool):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, readonly),
+                                         "version": 3, "strides": None}
+
+
+def _vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, ctx, precision, inner_tol,
+                     inner_max_iter, inner):
+    ctx = ctx or default_context()
+    K, ok = _as_matrix(ctx, k)
+    M, om = _as_matrix(ctx, m)
+    n = K.n
+    fixed = np.ascontiguousarray(fixed_dofs, dtype=np.int64)
+    ev = np.zeros(max(num_modes, 1))
+    shapes = np.zeros((max(num_modes, 1), n))
+    pit = np.zeros(max(num_modes, 1), np.int64)
+    info = SolveInfo()
+    err = []
+    cb = _abi.INNER_SOLVE()
+    if inner is not None:
+        import torch
+        dev = torch.device("cuda", ctx.device)
+
+        def trampoline(user, nn, b, x0, x):
+            try:
+                bh = torch.as_tensor(_DeviceArray(b, nn, False), device=dev).cpu().numpy()
+                x0h = torch.as_tensor(_DeviceArray(x0, nn, False), device=dev).cpu().numpy()
+                res = np.ascontiguousarray(inner(bh, x0h), dtype=np.float64)
+                if res.shape != (nn,):
+                    raise ValueError(f"inner solve returned shape {res.shape}, expected ({nn},)")
+                torch.as_tensor(_DeviceArray(x, nn, False), device=dev).copy_(torch.from_numpy(res))
+                torch.cuda.synchronize(dev)
+                return 0
+            except Exception as e:  # the reference's `?` on the closure's Err
+                err.append(e)
+                return _abi.FCU_ERR_NO_CONVERGENCE
+
+        cb = _abi.INNER_SOLVE(trampoline)
+    try:
+        rc = _L().fcu_vibration_modes(ctx.h, K.h, M.h, len(fixed), fixed.ctypes.data if len(fixed) else None,
+                                      int(num_modes), int(max_power_iters), float(tol), float(inner_tol),
+                                      int(inner_max_iter), precision, cb, None, ev.ctypes.data, shapes.ctypes.data,
+                                      pit.ctypes.data, C.byref(info))
+        if err:
+            raise err[0]
+        _check(ctx, rc)
+    finally:
+        if ok:
+            K.close()
+        if om:
+            M.close()
+    modes = []
+    for i in range(num_modes):
+        lam = float(ev[i])
+        omega = math.sqrt(lam)
+        modes.append(VibrationMode(omega / (2.0 * math.pi), omega, lam, shapes[i].copy()))
+    return modes, pit[:num_modes].copy(), info
+
+
+def solve_vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, ctx: Context | None = None,
+                          precision=FCU_FP64, inner_tol=1e-9, inner_max_iter=1000, return_stats=False):
+    """solve_vibration_modes (eigen.rs:286-300): the lowest modes of
+    K u = omega^2 M u, the inner solve Jacobi-PCG on the device at
+    inner_tol / inner_max_iter (reference: 1e-9, 1000). k, m: CscMatrix or
+    device Matrix on one pattern."""
+    modes, pit, info = _vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, ctx, precision,
+                                        inner_tol, inner_max_iter, None)
+    return (modes, pit, info) if return_stats else modes
+
+
+def solve_vibration_modes_with_inner(k, m, fixed_dofs, num_modes, max_power_iters, tol, inner,
+                                     ctx: Context | None = None):
+    """solve_vibration_modes_with_inner (eigen.rs:94-271): inner(b, x0) -> x
+    solves the folded K x = b on host arrays; an exception from it fails the
+    call like the closure's Err."""
+    modes, _, _ = _vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, ctx, FCU_FP64, 0.0, 0,
+                                   inner)
+    return modes
+
+
+# ---------------------------------------------------------------------------
+# 3x3 block CSR (gpu.rs:434-1141)
+# ---------------------------------------------------------------------------
+
+class GpuBsr3Context:
+    """GpuBsr3Context (gpu.rs:434-658): a resident 3x3 block CSR operator with
+    its inverse diagonal blocks."""
+
+    def __init__(self, n_nodes, row_ptr, cols, vals_flat, dinv_flat, device_index: int | None = None,
+                 ctx: Context | None = None):
+        self.ctx = ctx or (Context(device_index) if device_index not in (None, 0) else default_context())
+        self.n_nodes = int(n_nodes)
+        self._nnzb = int(np.asarray(row_ptr)[-1])
+        self.M = Matrix.from_bsr3(self.ctx, n_nodes, row_ptr, cols, vals_flat, dinv_flat)
+
+    def device_name(self) -> str:
+        import torch
+        return torch.cuda.get_device_name(self.ctx.device)
+
+    def nnz_blocks(self) -> int:
+        return self._nnzb
+
+    def spmv(self, x, y):
+        """y = A x (gpu.rs:505-545); y is filled in place."""
+        self.M.spmv(x, y)
+        return y
+
+    def jacobi_smooth(self, r, z, sweeps, omega, zero_initial_z):
+        """`sweeps` damped block-Jacobi sweeps on z in place (gpu.rs:547-657)."""
+        pr, kr = _ptr(r, np.float64)
+        pz, kz = _ptr(z)
+        if not _is_torch(z) and kz is not z:
+            raise ValueError("z must be a contiguous float64 array (updated in place)")
+        _check(self.ctx, _L().fcu_bsr3_jacobi_smooth(self.ctx.h, self.M.h, pr, pz, int(sweeps), float(omega),
+                                                     1 if zero_initial_z else 0))
+        return z
+
+    def close(self):
+        self.M.close()
+
+
+def solve_bsr3_pcg_gpu(n_nodes, row_ptr, cols, vals_flat, dinv_flat, b, x0=None, rtol=1e-8, max_iter=1000,
+                       device_index: int | None = None, ctx: Context | None = None) -> GpuSolveResult:
+    """solve_bsr3_pcg_gpu (gpu.rs:775-1141): block-Jacobi PCG, Ok at the
+    iteration limit, x = 0 for b = 0."""
+    import time
+    t0 = time.perf_counter()
+    ctx = ctx or (Context(device_index) if device_index not in (None, 0) else default_context())
+    n = 3 * int(n_nodes)
+    x = np.empty(n)
+    pr, kr = _ptr(row_ptr, np.uint32)
+    pc, kc = _ptr(cols, np.uint32)
+    pv, kv = _ptr(vals_flat, np.float64)
+    pd, kd = _ptr(dinv_flat, np.float64)
+    pb, kb = _ptr(b, np.float64)
+    p0, k0 = _ptr(x0, np.float64)
+    info = SolveInfo()
+    _check(ctx, _L().fcu_solve_bsr3_pcg(ctx.h, int(n_nodes), pr, pc, pv, pd, pb, p0, float(rtol), int(max_iter),
+                                        x.ctypes.data, C.byref(info)))
+    wall = (time.perf_counter() - t0) * 1e3
+    nnzb = int(np.asarray(row_ptr)[-1])
+    flops = (nnzb * 18.0 + n * 16.0) * info.iterations
+    import torch
+    return GpuSolveResult(x, int(info.iterations), float(info.rel_residual), wall, float(info.kernel_ms),
+                          flops / max(info.kernel_ms * 1e-3, 1e-12) / 1e9, float(info.effective_bw_gbps),
+                          [torch.cuda.get_device_name(ctx.device)])
+
+
+def spmv_bsr3_multi_gpu(n_nodes, row_ptr, cols, vals_flat, x, max_gpus):
+    """spmv_bsr3_multi_gpu (gpu.rs:662-771): contiguous block-row ranges of
+    ceil(n_nodes / g) rows on g = min(max_gpus, visible devices) devices,
+    each product computed on its device, concatenated on the host. Returns
+    (y, device names)."""
+    import torch
+    nd = max(1, min(int(max_gpus), torch.cuda.device_count()))
+    rp = np.asarray(row_ptr, dtype=np.uint32)
+    n_nodes = int(n_nodes)
+    chunk = (n_nodes + nd - 1) // nd
+    y = np.zeros(3 * n_nodes)
+    names = []
+    for slot in range(nd):
+        r0, r1 = slot * chunk, min((slot + 1) * chunk, n_nodes)
+        if r0 >= r1:
+            continue
+        ctx = default_context() if slot == 0 else Context(slot)
+        # the rows outside [r0, r1) are empty, so the product has zeros there
+        sub = np.concatenate([np.full(r0 + 1, rp[r0]), rp[r0 + 1:r1 + 1], np.full(n_nodes - r1, rp[r1])])
+        sub = (sub - rp[r0]).astype(np.uint32)
+        b0, b1 = int(rp[r0]), int(rp[r1])
+        M = Matrix.from_bsr3(ctx, n_nodes, sub, np.asarray(cols, np.uint32)[b0:b1],
+                             np.asarray(vals_flat, np.float64)[9 * b0:9 * b1])
+        part = M.spmv(x)
+        y[3 * r0:3 * r1] = part[3 * r0:3 * r1]
+        M.close()
+        names.append(torch.cuda.get_device_name(ctx.device))
+        if slot:
+            ctx.close()
+    return y, names

@@ -31,6 +31,9 @@ FCU_SRC_CONSTANT = 0
 FCU_SRC_SIN_PRODUCT = 1
 FCU_SRC_NODAL = 2
 
+FCU_BACKWARD_EULER = 0
+FCU_CRANK_NICOLSON = 1
+
 
 class SolveInfo(C.Structure):
     _fields_ = [
@@ -48,6 +51,9 @@ vp = C.c_void_p
 i64 = C.c_int64
 dbl = C.c_double
 cint = C.c_int
+
+# fcu_inner_solve: int (*)(void* user, int64_t n, const double* b, const double* x0, double* x)
+INNER_SOLVE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p)
 
 # name -> (restype, argtypes); pointer arguments are passed as integers.
 SIGNATURES = {
@@ -74,6 +80,11 @@ SIGNATURES = {
     "fcu_matrix_export_csc": (cint, [vp, vp, vp, vp, vp]),
     "fcu_assemble_stiffness": (cint, [vp, vp, vp]),
     "fcu_assemble_elasticity": (cint, [vp, vp, dbl, dbl, vp]),
+    "fcu_assemble_mass": (cint, [vp, vp, dbl, vp]),
+    "fcu_matrix_clone": (cint, [vp, vp, C.POINTER(vp)]),
+    "fcu_matrix_add_scaled": (cint, [vp, vp, vp, vp, dbl]),
+    "fcu_matrix_scale": (cint, [vp, vp, dbl]),
+    "fcu_matrix_fold_dirichlet": (cint, [vp, vp, i64, vp, cint]),
     "fcu_apply_dirichlet": (cint, [vp, vp, vp, i64, vp, vp]),
     "fcu_quadrature_points": (cint, [vp, vp, vp]),
     "fcu_assemble_rhs_values": (cint, [vp, vp, vp, vp]),
@@ -87,6 +98,17 @@ SIGNATURES = {
     "fcu_batch_config": (cint, [vp, cint, C.POINTER(cint), C.POINTER(cint), C.POINTER(cint)]),
     "fcu_element_stresses": (cint, [vp, vp, dbl, dbl, vp, vp, vp, vp, vp]),
     "fcu_vertex_von_mises": (cint, [vp, vp, vp, vp]),
+    "fcu_transient_create": (cint, [vp, vp, vp, cint, dbl, C.POINTER(vp)]),
+    "fcu_transient_set_dirichlet": (cint, [vp, vp, i64, vp, vp]),
+    "fcu_transient_step": (cint, [vp, vp, vp, vp, vp, vp, dbl, i64, cint, C.POINTER(SolveInfo)]),
+    "fcu_transient_destroy": (None, [vp]),
+    "fcu_vibration_modes": (cint, [vp, vp, vp, i64, vp, i64, i64, dbl, dbl, i64, cint, INNER_SOLVE, vp, vp, vp, vp,
+                                   C.POINTER(SolveInfo)]),
+    "fcu_bsr3_create": (cint, [vp, i64, vp, vp, vp, vp, C.POINTER(vp)]),
+    "fcu_bsr3_jacobi_smooth": (cint, [vp, vp, vp, vp, i64, dbl, cint]),
+    "fcu_solve_bsr3_pcg": (cint, [vp, i64, vp, vp, vp, vp, vp, vp, dbl, i64, vp, C.POINTER(SolveInfo)]),
+    "fcu_matrix_block_jacobi": (cint, [vp, vp, cint]),
+    "fcu_matrix_export_bsr3": (cint, [vp, vp, vp, vp, vp, vp]),
     "fcu_spmv": (cint, [vp, vp, vp, vp]),
     "fcu_adjoint_gradient": (cint, [vp, vp, dbl, dbl, vp, vp, vp, vp]),
     "fcu_time_spmv": (cint, [vp, vp, cint, cint, C.POINTER(dbl), C.POINTER(dbl)]),

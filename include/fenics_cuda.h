@@ -53,10 +53,15 @@ extern "C" {
 #define FCU_SRC_SIN_PRODUCT 1 /* f = p[0] * prod_d sin(p[1] * x_d)              */
 #define FCU_SRC_NODAL 2       /* f = sum_j f_j phi_j, nodal values in `values`  */
 
+/* ---- time-stepping schemes (TimeSteppingScheme, transient.rs:11-18) -------- */
+#define FCU_BACKWARD_EULER 0
+#define FCU_CRANK_NICOLSON 1
+
 typedef struct fcu_ctx_s* fcu_ctx;
 typedef struct fcu_mesh_s* fcu_mesh;
 typedef struct fcu_space_s* fcu_space;
 typedef struct fcu_matrix_s* fcu_matrix;
+typedef struct fcu_transient_s* fcu_transient;
 
 /* Per-solve report; the fields of GpuSolveResult (gpu.rs:24-34) that are
  * numbers, plus status and the absolute residual solve_cg returns. */
@@ -132,6 +137,32 @@ int fcu_assemble_stiffness(fcu_ctx ctx, fcu_matrix m, const double* cell_coef);
  * cell_E (nc, may be NULL) overrides Young's modulus per cell. ElasticMaterial::new
  * rejects nu outside (-1, 0.5) (elasticity.rs:23-26): FCU_ERR_BAD_ARG here. */
 int fcu_assemble_elasticity(fcu_ctx ctx, fcu_matrix m, double E, double nu, const double* cell_E);
+/* Mass matrices (mass.rs:10-250): assemble_mass_2d / assemble_mass_3d on
+ * FCU_SPACE_P1 (rho = 1 gives the reference), assemble_elasticity_mass_3d on
+ * FCU_SPACE_P1_VEC3 (rho = density), and for FCU_SPACE_P2 the scalar mass
+ * from the exact reference-tetrahedron products of
+ * assemble_elasticity_mass_p2_3d (mass.rs:137-250; one component of it).
+ * cell_coef (nc, may be NULL) multiplies each cell's contribution. The
+ * vector mass exports only its same-component entries, as the reference
+ * builds it; it is stored in the space's 3x3 blocks (zeros elsewhere), so it
+ * combines with the stiffness on that space. */
+int fcu_assemble_mass(fcu_ctx ctx, fcu_matrix m, double rho, const double* cell_coef);
+
+/* A new matrix on src's pattern with a copy of its values and Dirichlet state. */
+int fcu_matrix_clone(fcu_ctx ctx, fcu_matrix src, fcu_matrix* out);
+/* add_scaled_matrices (transient.rs:72-97): out = a + alpha * b entry by
+ * entry (each entry a + (alpha * b), as the triplet sum rounds it). a, b and
+ * out share one pattern (one space, or identical wrapped CSC layouts) and
+ * carry no eliminated Dirichlet dofs, else FCU_ERR_UNSUPPORTED; out may be
+ * a or b. */
+int fcu_matrix_add_scaled(fcu_ctx ctx, fcu_matrix out, fcu_matrix a, fcu_matrix b, double alpha);
+/* Every value times s (the diffusivity scaling of heat_solver.rs:48-57). */
+int fcu_matrix_scale(fcu_ctx ctx, fcu_matrix m, double s);
+/* fold_dirichlet (eigen.rs:55-79), in place: entries on a fixed row or column
+ * become zero, a fixed diagonal 1 (unit_diag != 0) or 0; dofs >= n are
+ * ignored. The exported pattern then omits every zero value, as the
+ * reference's rebuilt matrix does. Idempotent. */
+int fcu_matrix_fold_dirichlet(fcu_ctx ctx, fcu_matrix m, int64_t nfixed, const int64_t* fixed, int unit_diag);
 
 /* apply_dirichlet_bc / apply_vector_dirichlet_bc (poisson.rs:222-263,
  * elasticity.rs:188-227), in place on m and b: b_i -= a_ik g_k for free rows,
@@ -225,6 +256,87 @@ int fcu_solve_csr_cg_noalloc(int64_t n, const uint32_t* row_ptr, const uint32_t*
 
 /* y = A x (cg.rs:7-23) with the FP64 values. */
 int fcu_spmv(fcu_ctx ctx, fcu_matrix m, const double* x, double* y);
+
+/* ---- transient heat (transient.rs:21-68, heat_solver.rs:23-104) ------------- */
+/* A stepper for M du/dt + K u = F that keeps its matrices on the device:
+ * lhs = M + dt K (FCU_BACKWARD_EULER) or M + (dt/2) K (FCU_CRANK_NICOLSON),
+ * and the right-hand matrix M or M - (dt/2) K, all formed once by
+ * add_scaled_matrices from the values mass and stiff hold at creation. */
+int fcu_transient_create(fcu_ctx ctx, fcu_matrix mass, fcu_matrix stiff, int scheme, double dt,
+                         fcu_transient* out);
+/* Dirichlet values (heat_solver.rs:82-99) written into the state before each
+ * step and into the new state after it; a repeated dof takes its last value.
+ * nbc = 0 clears them. */
+int fcu_transient_set_dirichlet(fcu_ctx ctx, fcu_transient ts, int64_t nbc, const int64_t* dofs,
+                                const double* vals);
+/* TransientHeatSolver::step (transient.rs:32-68): rhs = M u_n + dt f_next, or
+ * (M - dt/2 K) u_n + (dt/2)(f_n + f_next); then lhs u_next = rhs, solved by
+ * the Jacobi-PCG of fcu_pcg (precision, tol, max_iter) from x0 = u_n where
+ * the reference factorises densely (direct.rs:26-53). f_n / f_next may be
+ * NULL (zero load). u_next may equal u_n. Status as fcu_pcg. */
+int fcu_transient_step(fcu_ctx ctx, fcu_transient ts, const double* u_n, const double* f_n,
+                       const double* f_next, double* u_next, double tol, int64_t max_iter, int precision,
+                       fcu_solve_info* info);
+void fcu_transient_destroy(fcu_transient ts);
+
+/* ---- vibration modes (eigen.rs:94-300) ------------------------------------- */
+/* Inner solve of the inverse iteration (the `inner` closure of
+ * solve_vibration_modes_with_inner, eigen.rs:94-102): solve K x = b in the
+ * folded frame, x0 the previous iterate. b, x0, x are device arrays of n
+ * doubles; the library's stream is idle when it is called, and x must be
+ * complete when it returns. Non-zero return: the solve fails with it. */
+typedef int (*fcu_inner_solve)(void* user, int64_t n, const double* b, const double* x0, double* x);
+/* solve_vibration_modes / solve_vibration_modes_with_inner: the lowest
+ * num_modes modes of K u = lambda M u by inverse power iteration with
+ * mass-orthogonal deflation, on folded copies of k (unit diagonal) and m
+ * (zero), the mass rescaled by mean|diag K| / mean|diag M|, stopping each
+ * mode when the Rayleigh quotient moves less than tol relative to itself or
+ * after max_power_iters. inner == NULL: Jacobi-PCG on the folded stiffness
+ * at inner_tol / inner_max_iter / precision (the reference default is FP64,
+ * 1e-9, 1000). k and m have one order (their patterns may differ). Outputs:
+ * eigenvalues (num_modes),
+ * mode_shapes (num_modes*n, mass-normalised, may be NULL), power_iterations
+ * (num_modes, may be NULL); info: total inner iterations and device time.
+ * A failed inner solve fails the call with its status, as the reference's
+ * `?` does. */
+int fcu_vibration_modes(fcu_ctx ctx, fcu_matrix k, fcu_matrix m, int64_t nfixed, const int64_t* fixed,
+                        int64_t num_modes, int64_t max_power_iters, double tol, double inner_tol,
+                        int64_t inner_max_iter, int precision, fcu_inner_solve inner, void* user,
+                        double* eigenvalues, double* mode_shapes, int64_t* power_iterations,
+                        fcu_solve_info* info);
+
+/* ---- 3x3 block CSR (GpuBsr3Context, solve_bsr3_pcg_gpu; gpu.rs:434-1141) --- */
+/* Block CSR layout of the reference: row_ptr (n_nodes + 1, u32) over block
+ * rows, cols (u32) block columns, vals_flat 9 values per block row-major
+ * (vals_flat[9k + 3a + b] = A(3i + a, 3 cols[k] + b)), dinv_flat the inverse
+ * diagonal block of each block row (9 per row, row-major). */
+/* GpuBsr3Context::new (gpu.rs:453-494): a resident block matrix; dinv_flat may
+ * be NULL. fcu_spmv on it is GpuBsr3Context::spmv (gpu.rs:505-545); fcu_pcg
+ * on it (FCU_FP64) preconditions with the inverse blocks when given. */
+int fcu_bsr3_create(fcu_ctx ctx, int64_t n_nodes, const uint32_t* row_ptr, const uint32_t* cols,
+                    const double* vals_flat, const double* dinv_flat, fcu_matrix* out);
+/* GpuBsr3Context::jacobi_smooth (gpu.rs:547-657): `sweeps` damped block-Jacobi
+ * sweeps z <- z + omega D^-1 (r - A z); with zero_initial_z the first sweep
+ * is z = D^-1 r. sweeps = 0 leaves z untouched. */
+int fcu_bsr3_jacobi_smooth(fcu_ctx ctx, fcu_matrix m, const double* r, double* z, int64_t sweeps, double omega,
+                           int zero_initial_z);
+/* solve_bsr3_pcg_gpu (gpu.rs:775-1141): block-Jacobi PCG in FP64 from x0 (NULL
+ * = 0), stop when ||r||/||b|| < rtol after the x/r update or when
+ * p.Ap <= 1e-30; FCU_OK at the iteration limit (info.rel_residual tells) and
+ * x = 0 when ||b|| = 0, as the reference returns Ok. */
+int fcu_solve_bsr3_pcg(fcu_ctx ctx, int64_t n_nodes, const uint32_t* row_ptr, const uint32_t* cols,
+                       const double* vals_flat, const double* dinv_flat, const double* b, const double* x0,
+                       double rtol, int64_t max_iter, double* x, fcu_solve_info* info);
+/* Block-Jacobi preconditioning of an assembled vector matrix from its own
+ * diagonal blocks (inverted at every FP64 solve), or (enable = 0) back to
+ * point Jacobi. FCU_ERR_BAD_ARG if a diagonal block is singular. */
+int fcu_matrix_block_jacobi(fcu_ctx ctx, fcu_matrix m, int enable);
+/* The block CSR arrays of a 3x3 block matrix (assembled on FCU_SPACE_P1_VEC3
+ * or created by fcu_bsr3_create), the reference's solve_bsr3_pcg_gpu inputs;
+ * any output may be NULL; dinv_flat needs inverse blocks (given at creation
+ * or fcu_matrix_block_jacobi). */
+int fcu_matrix_export_bsr3(fcu_ctx ctx, fcu_matrix m, uint32_t* row_ptr, uint32_t* cols, double* vals_flat,
+                           double* dinv_flat);
 
 /* ---- adjoint sensitivities (no reference counterpart) ----------------------- */
 /* For E_e = E0 * theta_e^3: grad_e = -lambda_e^T (3 theta_e^2 E0 K_e^1) u_e, with

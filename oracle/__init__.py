@@ -12,6 +12,7 @@ the reference file:line for the arithmetic.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from dataclasses import dataclass
@@ -82,6 +83,8 @@ def _load() -> C.CDLL:
         "orc_affine_map_3d": (C.c_int, [f64p, C.POINTER(dbl), f64p]),
         "orc_p2_basis": (None, [f64p, f64p]),
         "orc_p2_grads": (None, [f64p, f64p]),
+        "orc_p2_mass_products": (None, [f64p]),
+        "orc_assemble_mass": (vp, [i64, f64p, i64, i64p, vp, C.c_int, dbl, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -488,3 +491,300 @@ def solve_elasticity_3d(m: Mesh, E, nu, f_body, dofs, tol, max_iter):
     f = body_force_3d(m, f_body)
     Kb, fb = apply_dirichlet_bc(K, f, dofs, np.zeros(len(dofs)))
     return solve_cg(Kb, fb, None, tol, max_iter)
+
+
+# ---------------------------------------------------------------------------
+# Mass matrices, matrix combinations, transient heat, vibration modes
+# (mass.rs, transient.rs, heat_solver.rs, direct.rs, eigen.rs)
+# ---------------------------------------------------------------------------
+
+def p2_mass_products() -> np.ndarray:
+    """build_reference_mass_products_p2 (mass.rs:195-250), 10x10."""
+    out = np.empty(100)
+    lib().orc_p2_mass_products(out)
+    return out.reshape(10, 10)
+
+
+def _mass(m: Mesh, kind: int, density: float, coef=None, cell_dofs=None, ndofs=None) -> Csc:
+    nd = ndofs if ndofs is not None else (3 * m.nv if kind == 2 else m.nv)
+    cd = None if cell_dofs is None else _i64(cell_dofs)
+    cf = None if coef is None else _f64(coef)
+    h = lib().orc_assemble_mass(nd, _f64(m.coords), m.nc, _i64(m.cells), _ptr(cd), kind, float(density), _ptr(cf))
+    return _take_csc(h)
+
+
+def assemble_mass_2d(m: Mesh, coef=None) -> Csc:
+    """assemble_mass_2d (mass.rs:10-44)."""
+    return _mass(m, 0, 1.0, coef)
+
+
+def assemble_mass_3d(m: Mesh, coef=None) -> Csc:
+    """assemble_mass_3d (mass.rs:47-81)."""
+    return _mass(m, 1, 1.0, coef)
+
+
+def assemble_elasticity_mass_3d(m: Mesh, density: float, coef=None) -> Csc:
+    """assemble_elasticity_mass_3d (mass.rs:84-127)."""
+    return _mass(m, 2, density, coef)
+
+
+def assemble_p2_mass_3d(m: Mesh, cell_dofs, ndofs, density: float = 1.0, coef=None) -> Csc:
+    """Scalar P2 mass: density |det J| times the reference products
+    (one component of assemble_elasticity_mass_p2_3d, mass.rs:137-180)."""
+    return _mass(m, 3, density, coef, cell_dofs, ndofs)
+
+
+def _triplets(A: Csc):
+    cols = np.repeat(np.arange(A.n, dtype=np.int64), np.diff(A.colptr))
+    return A.rowidx.astype(np.int64), cols, A.vals
+
+
+def add_scaled_matrices(a: Csc, b: Csc, alpha: float) -> Csc:
+    """add_scaled_matrices (transient.rs:72-97): per column, a's triplets then
+    alpha * b's, summed by the triplet build."""
+    ra, ca, va = _triplets(a)
+    rb, cb, vb = _triplets(b)
+    # interleave per column: all of a's entries of column c, then b's
+    key_a = ca * 2
+    key_b = cb * 2 + 1
+    rows = np.concatenate([ra, rb])
+    cols = np.concatenate([ca, cb])
+    vals = np.concatenate([va, alpha * vb])
+    order = np.argsort(np.concatenate([key_a, key_b]), kind="stable")
+    return csc_from_triplets(a.n, rows[order], cols[order], vals[order])
+
+
+def fold_dirichlet(mat: Csc, fixed_dofs, unit_diag: bool) -> Csc:
+    """fold_dirichlet (eigen.rs:55-79)."""
+    n = mat.n
+    fixed = np.zeros(n, bool)
+    fd = np.asarray(fixed_dofs, dtype=np.int64)
+    fixed[fd[fd < n]] = True
+    rows, cols, vals = _triplets(mat)
+    keep = ~(fixed[rows] | fixed[cols] | (vals == 0.0))
+    rows, cols, vals = rows[keep], cols[keep], vals[keep]
+    if unit_diag:
+        fc = np.nonzero(fixed)[0]
+        # the unit diagonal follows the column's kept entries
+        rows = np.concatenate([rows, fc])
+        cols = np.concatenate([cols, fc])
+        vals = np.concatenate([vals, np.ones(len(fc))])
+        order = np.argsort(cols, kind="stable")
+        rows, cols, vals = rows[order], cols[order], vals[order]
+    return csc_from_triplets(n, rows, cols, vals)
+
+
+def solve_direct(A: Csc, b) -> np.ndarray:
+    """solve_direct (direct.rs:26-53): dense partial-pivoting LU (LAPACK
+    gesv through numpy), for systems of a few thousand dofs at most."""
+    return np.linalg.solve(A.to_scipy().toarray(), np.asarray(b, dtype=np.float64))
+
+
+def transient_step(scheme: int, dt: float, mass: Csc, stiff: Csc, u_n, f_n, f_next) -> np.ndarray:
+    """TransientHeatSolver::step (transient.rs:32-68); scheme 0 = backward
+    Euler, 1 = Crank-Nicolson."""
+    u_n = np.asarray(u_n, dtype=np.float64)
+    if scheme == 0:
+        lhs = add_scaled_matrices(mass, stiff, dt)
+        rhs = spmv(mass, u_n) + dt * np.asarray(f_next, dtype=np.float64)
+    else:
+        half_dt = 0.5 * dt
+        lhs = add_scaled_matrices(mass, stiff, half_dt)
+        rhs_mat = add_scaled_matrices(mass, stiff, -half_dt)
+        rhs = spmv(rhs_mat, u_n) + half_dt * (np.asarray(f_n, dtype=np.float64) + np.asarray(f_next, dtype=np.float64))
+    return solve_direct(lhs, rhs)
+
+
+def solve_transient_heat_2d(m: Mesh, diffusivity, u_initial, bcs, dt, num_steps, scheme, heat_source=None):
+    """solve_transient_heat_2d (heat_solver.rs:23-104); bcs: [(dofs, values)].
+    Returns (times, history, final)."""
+    n = m.nv
+    mass = assemble_mass_2d(m)
+    k = assemble_stiffness_2d(m)
+    stiff = Csc(k.n, k.colptr, k.rowidx, diffusivity * k.vals)
+    u = np.asarray(u_initial, dtype=np.float64).copy()
+    times, hist = [0.0], [u.copy()]
+    for step in range(1, num_steps + 1):
+        t0, t1 = (step - 1) * dt, step * dt
+        f0 = np.zeros(n) if heat_source is None else np.array([heat_source(t0, m.coords[i]) for i in range(n)])
+        f1 = np.zeros(n) if heat_source is None else np.array([heat_source(t1, m.coords[i]) for i in range(n)])
+        for dofs, vals in bcs:
+            for d, v in zip(dofs, vals):
+                u[d] = v
+        un = transient_step(scheme, dt, mass, stiff, u, f0, f1)
+        for dofs, vals in bcs:
+            for d, v in zip(dofs, vals):
+                un[d] = v
+        u = un
+        times.append(t1)
+        hist.append(u.copy())
+    return times, hist, u
+
+
+def _mean_abs_diag(A: Csc) -> float:
+    acc, found = 0.0, 0
+    for c in range(A.n):
+        for p in range(A.colptr[c], A.colptr[c + 1]):
+            if A.rowidx[p] == c:
+                acc += abs(A.vals[p])
+                found += 1
+                break
+    return acc / found if found else 0.0
+
+
+def solve_vibration_modes_with_inner(k: Csc, m: Csc, fixed_dofs, num_modes, max_power_iters, tol, inner):
+    """solve_vibration_modes_with_inner (eigen.rs:94-271). Returns a list of
+    (eigenvalue, mode_shape, power_iterations)."""
+    kd = fold_dirichlet(k, fixed_dofs, True)
+    md = fold_dirichlet(m, fixed_dofs, False)
+    n = kd.n
+    is_fixed = np.zeros(n, bool)
+    fd = np.asarray(fixed_dofs, dtype=np.int64)
+    is_fixed[fd[fd < n]] = True
+    if n - int(is_fixed.sum()) == 0:
+        raise ValueError("No free degrees of freedom in system")
+    kdg, mdg = _mean_abs_diag(kd), _mean_abs_diag(md)
+    s = kdg / mdg if kdg > 0.0 and mdg > 0.0 else 1.0
+    modes, vecs = [], []
+    idx = np.arange(n, dtype=np.int64)
+    for mode in range(num_modes):
+        v = (((idx + 1) * 31 + (mode + 1) * 97) % 1000).astype(np.float64) / 1000.0 - 0.5
+        v[is_fixed] = 0.0
+        m_prev = [spmv(md, p) * s for p in vecs]
+        for mp, prev in zip(m_prev, vecs):
+            v = v - float(np.dot(v, mp)) * prev
+        mv = spmv(md, v) * s
+        norm_m = math.sqrt(float(np.dot(v, mv)))
+        if norm_m > 1e-14:
+            v = v / norm_m
+        prev_r = 0.0
+        its = 0
+        for it in range(max_power_iters):
+            its = it + 1
+            mv = spmv(md, v) * s
+            w = np.array(inner(kd, mv, v), dtype=np.float64)
+            w[is_fixed] = 0.0
+            for mp, prev in zip(m_prev, vecs):
+                w = w - float(np.dot(w, mp)) * prev
+            mw = spmv(md, w)
+            mw_norm = math.sqrt(float(np.dot(w, mw))) * math.sqrt(s)
+            if mw_norm < 1e-15:
+                break
+            w = w / mw_norm
+            r = float(np.dot(w, spmv(kd, w)))
+            v = w
+            denom = max(abs(r), abs(prev_r))
+            if denom == 0.0 or abs(r - prev_r) / denom < tol:
+                break
+            prev_r = r
+        lam = max(float(np.dot(v, spmv(kd, v))) / float(np.dot(v, spmv(md, v))), 0.0)
+        vecs.append(v)
+        modes.append((lam, v, its))
+    return modes
+
+
+def solve_vibration_modes(k: Csc, m: Csc, fixed_dofs, num_modes, max_power_iters, tol,
+                          inner_tol=1e-9, inner_max_iter=1000):
+    """solve_vibration_modes (eigen.rs:286-300): inner solve = solve_cg on
+    the folded stiffness from x0 at 1e-9 / 1000 iterations."""
+    def inner(kd, b, x0):
+        x, _, _ = solve_cg(kd, b, x0, inner_tol, inner_max_iter)
+        return x
+    return solve_vibration_modes_with_inner(k, m, fixed_dofs, num_modes, max_power_iters, tol, inner)
+
+
+# ---------------------------------------------------------------------------
+# 3x3 block CSR (gpu.rs:434-1141): spmv, block-Jacobi sweeps, block-Jacobi PCG
+# ---------------------------------------------------------------------------
+
+def bsr3_spmv(n_nodes, row_ptr, cols, vals_flat, x) -> np.ndarray:
+    """y = A x with row-major 3x3 blocks: y[3i+a] = sum_k sum_b V[k][a][b] x[3 cols[k] + b]."""
+    rp = np.asarray(row_ptr, dtype=np.int64)
+    ci = np.asarray(cols, dtype=np.int64)
+    V = np.asarray(vals_flat, dtype=np.float64).reshape(-1, 3, 3)
+    X = np.asarray(x, dtype=np.float64).reshape(-1, 3)
+    rows = np.repeat(np.arange(n_nodes), np.diff(rp))
+    contrib = np.einsum("kab,kb->ka", V, X[ci])
+    Y = np.zeros((n_nodes, 3))
+    np.add.at(Y, rows, contrib)
+    return Y.ravel()
+
+
+def bsr3_apply_dinv(dinv_flat, r) -> np.ndarray:
+    """bsr3_apply_dinv: z = D^-1 r per block row."""
+    D = np.asarray(dinv_flat, dtype=np.float64).reshape(-1, 3, 3)
+    return np.einsum("kab,kb->ka", D, np.asarray(r, dtype=np.float64).reshape(-1, 3)).ravel()
+
+
+def bsr3_jacobi_smooth(n_nodes, row_ptr, cols, vals_flat, dinv_flat, r, z, sweeps, omega, zero_initial_z):
+    """GpuBsr3Context::jacobi_smooth (gpu.rs:547-657)."""
+    z = np.array(z, dtype=np.float64)
+    if sweeps == 0:
+        return z
+    start = 0
+    if zero_initial_z:
+        z = bsr3_apply_dinv(dinv_flat, r)
+        start = 1
+    for _ in range(start, sweeps):
+        y = bsr3_spmv(n_nodes, row_ptr, cols, vals_flat, z)
+        z = z + omega * bsr3_apply_dinv(dinv_flat, np.asarray(r) - y)
+    return z
+
+
+def bsr3_block_inverse(n_nodes, row_ptr, cols, vals_flat) -> np.ndarray:
+    """Inverse diagonal blocks (numpy LAPACK inverse) of a block CSR matrix."""
+    rp = np.asarray(row_ptr, dtype=np.int64)
+    ci = np.asarray(cols, dtype=np.int64)
+    V = np.asarray(vals_flat, dtype=np.float64).reshape(-1, 3, 3)
+    out = np.empty((n_nodes, 3, 3))
+    for i in range(n_nodes):
+        k = rp[i] + int(np.nonzero(ci[rp[i]:rp[i + 1]] == i)[0][0])
+        out[i] = np.linalg.inv(V[k])
+    return out.ravel()
+
+
+def solve_bsr3_pcg(n_nodes, row_ptr, cols, vals_flat, dinv_flat, b, x0=None, rtol=1e-8, max_iter=1000):
+    """solve_bsr3_pcg_gpu (gpu.rs:775-1141): block-Jacobi PCG; returns
+    (x, iterations, final relative residual). Ok at the limit, x = 0 for
+    b = 0, stop on p.Ap <= 1e-30."""
+    b = np.asarray(b, dtype=np.float64)
+    n = 3 * n_nodes
+    bnorm = math.sqrt(float(np.dot(b, b)))
+    if bnorm == 0.0:
+        return np.zeros(n), 0, 0.0
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    r = b.copy()
+    if x0 is not None:
+        r = r - bsr3_spmv(n_nodes, row_ptr, cols, vals_flat, x)
+    z = bsr3_apply_dinv(dinv_flat, r)
+    p = z.copy()
+    rz = float(np.dot(r, z))
+    final_rel, iters = 1.0, 0
+    for it in range(1, max_iter + 1):
+        iters = it
+        ap = bsr3_spmv(n_nodes, row_ptr, cols, vals_flat, p)
+        pap = float(np.dot(p, ap))
+        if pap <= 1e-30:
+            break
+        alpha = rz / pap
+        x = x + alpha * p
+        r = r - alpha * ap
+        final_rel = math.sqrt(max(float(np.dot(r, r)), 0.0)) / bnorm
+        if final_rel < rtol:
+            break
+        z = bsr3_apply_dinv(dinv_flat, r)
+        rz_new = float(np.dot(r, z))
+        beta = rz_new / max(rz, 1e-30)
+        rz = rz_new
+        p = z + beta * p
+    return x, iters, final_rel
+
+
+def bsr3_from_csc(A: Csc):
+    """The 3x3 block CSR of a vector matrix given as CSC (dof = 3 node + a):
+    block pattern = node pairs with any stored entry."""
+    S = A.to_scipy().tocsr()
+    B = S.tobsr(blocksize=(3, 3))
+    B.sort_indices()
+    return (S.shape[0] // 3, B.indptr.astype(np.uint32), B.indices.astype(np.uint32),
+            np.ascontiguousarray(B.data).ravel())

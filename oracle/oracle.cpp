@@ -807,6 +807,108 @@ void* orc_assemble_p2_stiffness_3d(i64 ndofs, const double* coords, i64 nc, cons
   return build_csc(ndofs, w, R.data(), C.data(), V.data());
 }
 
+// ---------------------------------------------------------------------------
+// Mass matrices (mass.rs:10-250). Entry (i, j) of a cell is measure * factor
+// (assemble_mass_2d: area * {1/6, 1/12}; assemble_mass_3d: vol * {1/10, 1/20};
+// assemble_elasticity_mass_3d: density * vol * factor on each of the three
+// components). Scalar P2 (this build's P2 numbering): density * |det J| *
+// product, the products of build_reference_mass_products_p2. `coef`
+// (nullable) is the per-cell extension: measure * coef_e before the factor.
+// ---------------------------------------------------------------------------
+
+// Barycentric moments over the reference tetrahedron (mass.rs:195-250):
+// corner i is 2 l_i^2 - l_i, edge (i, j) is 4 l_i l_j; the products are
+// summed term by term in that order.
+void orc_p2_mass_products(double* out) {
+  static const double F[12] = {1.0, 1.0, 2.0, 6.0, 24.0, 120.0, 720.0, 5040.0, 40320.0, 362880.0, 3628800.0,
+                               39916800.0};
+  int mono[10][2][4] = {};
+  double cf[10][2] = {};
+  int nterm[10];
+  for (int i = 0; i < 4; ++i) {
+    mono[i][0][i] = 2;
+    cf[i][0] = 2.0;
+    mono[i][1][i] = 1;
+    cf[i][1] = -1.0;
+    nterm[i] = 2;
+  }
+  for (int e = 0; e < 6; ++e) {
+    mono[4 + e][0][P2_EDGE[e][0]] = 1;
+    mono[4 + e][0][P2_EDGE[e][1]] = 1;
+    cf[4 + e][0] = 4.0;
+    nterm[4 + e] = 1;
+  }
+  for (int a = 0; a < 10; ++a)
+    for (int b = 0; b < 10; ++b) {
+      double acc = 0.0;
+      for (int ta = 0; ta < nterm[a]; ++ta)
+        for (int tb = 0; tb < nterm[b]; ++tb) {
+          int m[4], deg = 0;
+          for (int q = 0; q < 4; ++q) {
+            m[q] = mono[a][ta][q] + mono[b][tb][q];
+            deg += m[q];
+          }
+          acc += cf[a][ta] * cf[b][tb] * F[m[0]] * F[m[1]] * F[m[2]] * F[m[3]] / F[deg + 3];
+        }
+      out[10 * a + b] = acc;
+    }
+}
+
+// kind: 0 = P1 triangles, 1 = P1 tetrahedra, 2 = vector P1 tetrahedra,
+// 3 = scalar P2 tetrahedra (cell_dofs gives the ten dofs of each cell).
+void* orc_assemble_mass(i64 ndofs, const double* coords, i64 nc, const i64* cells, const i64* cell_dofs, int kind,
+                        double density, const double* coef) {
+  const int k = kind == 0 ? 3 : (kind == 3 ? 10 : 4);
+  const int bs = kind == 2 ? 3 : 1;
+  const i64 per = (i64)k * k * bs;
+  std::vector<i64> R(per * nc), C(per * nc);
+  std::vector<double> V(per * nc);
+  std::vector<char> ok(nc, 0);
+  double prod[100];
+  orc_p2_mass_products(prod);
+  for (i64 c = 0; c < nc; ++c) {
+    double meas;
+    if (kind == 0) {
+      const i64* t = cells + 3 * c;
+      Map2 m;
+      if (!map_triangle(coords + 2 * t[0], coords + 2 * t[1], coords + 2 * t[2], m)) continue;
+      meas = 0.5 * std::fabs(m.det);
+    } else {
+      const i64* t = cells + 4 * c;
+      Map3 m;
+      if (!map_tet(coords + 3 * t[0], coords + 3 * t[1], coords + 3 * t[2], coords + 3 * t[3], m)) continue;
+      meas = kind == 3 ? std::fabs(m.det) : (1.0 / 6.0) * std::fabs(m.det);
+    }
+    ok[c] = 1;
+    double s = density * meas;
+    if (coef) s = s * coef[c];
+    const i64* d = kind == 3 ? cell_dofs + 10 * c : cells + (i64)k * c;
+    i64 o = per * c;
+    for (int i = 0; i < k; ++i)
+      for (int j = 0; j < k; ++j) {
+        double f = kind == 3 ? prod[10 * i + j] : (i == j ? (k == 3 ? 1.0 / 6.0 : 1.0 / 10.0)
+                                                          : (k == 3 ? 1.0 / 12.0 : 1.0 / 20.0));
+        double v = s * f;
+        for (int a = 0; a < bs; ++a) {
+          R[o] = bs * d[i] + a;
+          C[o] = bs * d[j] + a;
+          V[o] = v;
+          ++o;
+        }
+      }
+  }
+  i64 w = 0;
+  for (i64 c = 0; c < nc; ++c)
+    if (ok[c])
+      for (i64 q = 0; q < per; ++q) {
+        R[w] = R[per * c + q];
+        C[w] = C[per * c + q];
+        V[w] = V[per * c + q];
+        ++w;
+      }
+  return build_csc(ndofs, w, R.data(), C.data(), V.data());
+}
+
 // P2 load b_a = sum_q w_q |det J| f(x_q) phi_a(xi_q) with f given at the
 // Keast points (fq[4c+q]); serial cell-order scatter.
 void orc_assemble_p2_rhs_3d(i64 ndofs, const double* coords, i64 nc, const i64* cells, const i64* cell_dofs,
