@@ -14,9 +14,11 @@ metric is dofs / step time (DOF/s). Inputs are synthetic (generated meshes).
                     [--config c2|c2p] [--no-cpu-baseline] [--no-extra]
 
 After the headline measurement, rank 0 of a 1-GPU run also measures the
-other configurations (2D Poisson 64^2, elasticity at 1.57M dofs, P2 Poisson
-with random coefficient, adjoint sensitivities, the 256-problem batch) and
-reports them under "workloads".
+other configurations (2D Poisson 64^2, elasticity at 1.57M dofs with stress
+recovery, P2 Poisson with random coefficient, adjoint sensitivities, the
+256-problem batch, the C2 mass matrix, block-Jacobi PCG on C2, a 1M-dof
+transient heat run and a cantilever's vibration modes) and reports them
+under "workloads".
 
 --impl reference times the CPU restatement of the reference path (the
 reference itself is Rust and cannot be built here) on the host cores.
@@ -158,12 +160,22 @@ def cpu_reference_run(cfg, iters_full: int | None, sample_iters: int = 150):
         iters_full = 2010  # FP64 Jacobi-PCG iterations to 1e-8 at 128x32x32 (scipy probe of the same iteration)
     t_total = t_setup + t_iter * iters_full
     n = 3 * om.nv
+    # the multi-threaded CSR variant of the same iteration (labelled; cg.rs is sequential)
+    t2 = time.perf_counter()
+    O.cg_fixed_iters_mt(Kb, fb, sample_iters, cores)
+    t_iter_mt = (time.perf_counter() - t2) / sample_iters
+    t_total_mt = t_setup + t_iter_mt * iters_full
     return {
         "value": n / t_total, "unit": "DOF/s", "cores": cores, "kind": "port",
         "sample": f"assembly+body force+Dirichlet in full ({t_setup:.2f} s, {cores} threads for the cell loop), "
                   f"{sample_iters} sequential PCG iterations ({t_iter * 1e3:.1f} ms each) extrapolated to "
                   f"{iters_full} iterations",
         "seconds_sampled": t_setup + t_iter * sample_iters,
+        "multithreaded_csr": {
+            "value": n / t_total_mt, "unit": "DOF/s", "cores": cores, "kind": "port",
+            "sample": f"same setup, {sample_iters} PCG iterations with an OpenMP row-gather SpMV and parallel "
+                      f"vector work on {cores} threads ({t_iter_mt * 1e3:.2f} ms each) extrapolated to "
+                      f"{iters_full} iterations"},
     }
 
 
@@ -556,7 +568,26 @@ def run_workloads(ctx, stream, peak):
     out["mass_c2"] = {"workload": "vector-P1 mass matrix of the C2 mesh (786,432 tets), density 7850",
                       "ms": ms_m, "gbs": mbytes / (ms_m * 1e-3) / 1e9, "bytes": mbytes,
                       "frac_of_hbm": mbytes / (ms_m * 1e-3) / 1e9 / peak}
-    M.close(); V.close()
+    M.close()
+
+    # 3x3 block-Jacobi PCG on the C2 system (solve_bsr3_pcg_gpu's preconditioner) vs point Jacobi, FP64
+    K = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+    cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+    dofs = d64((3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64))
+    b = torch.empty(V.ndofs, dtype=torch.float64, device=dev)
+    V.body_force(np.array([0.0, 0.0, -7.8e4]), out=b)
+    K.apply_dirichlet(b, dofs, torch.zeros(len(dofs), dtype=torch.float64, device=dev))
+    x = torch.empty_like(b)
+    bj = {"workload": "C2 system after Dirichlet elimination, FP64 PCG to 1e-8: 3x3 block-Jacobi (inverse "
+                      "diagonal blocks, recomputed per solve) vs point Jacobi"}
+    for name, on in (("block_jacobi", True), ("point_jacobi", False)):
+        K.block_jacobi(on)
+        K.pcg(b, x=x, tol=1e-8, max_iter=100000)
+        ms, (_, info) = _best_ms(stream, lambda: K.pcg(b, x=x, tol=1e-8, max_iter=100000))
+        bj[name] = {"ms": ms, "iterations": int(info.iterations), "dof_per_s": V.ndofs / (ms * 1e-3),
+                    "effective_gbs": info.effective_bw_gbps}
+    out["bsr3_block_jacobi_c2"] = bj
+    K.close(); V.close()
 
     # Transient heat: unit square 1024^2, Crank-Nicolson, dt = 1e-4, u = 0 on the boundary
     mesh = fcu.unit_square(1024, 1024)

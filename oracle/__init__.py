@@ -84,6 +84,7 @@ def _load() -> C.CDLL:
         "orc_p2_basis": (None, [f64p, f64p]),
         "orc_p2_grads": (None, [f64p, f64p]),
         "orc_p2_mass_products": (None, [f64p]),
+        "orc_cg_fixed_iters_mt": (dbl, [vp, f64p, i64, f64p, C.c_int]),
         "orc_assemble_mass": (vp, [i64, f64p, i64, i64p, vp, C.c_int, dbl, vp]),
     }
     for name, (res, args) in sig.items():
@@ -398,6 +399,15 @@ def solve_cg(A: Csc, b, x0=None, tol=1e-10, max_iter=1000):
     if st == 2:
         raise CgError(f"CG failed to converge within {max_iter} iterations")
     return x, it.value, res.value
+
+
+def cg_fixed_iters_mt(A: Csc, b, iters: int, threads: int = 0):
+    """cg_fixed_iters with an OpenMP row-gather SpMV and parallel vector work
+    (a multi-threaded CSR variant for the CPU baseline; A symmetric)."""
+    x = np.empty(A.n)
+    with _Handle(A) as h:
+        rel = lib().orc_cg_fixed_iters_mt(h, _f64(b), iters, x, threads)
+    return x, rel
 
 
 def cg_fixed_iters(A: Csc, b, iters: int):

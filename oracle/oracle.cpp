@@ -1044,6 +1044,60 @@ int orc_solve_cg(void* h, const double* b, const double* x0, double tol, i64 max
 // Timed-baseline helper: run exactly `iters` PCG iterations (no convergence
 // test) and return the final relative residual. Same arithmetic as
 // orc_solve_cg's loop.
+// Multi-threaded variant for the CPU baseline (labelled as such; the
+// reference's cg.rs is sequential): the same Jacobi-PCG recurrence with a
+// row-gather SpMV (the CSC of a symmetric matrix read as its CSR) and the
+// vector loops and dot products split over `threads` OpenMP threads.
+double orc_cg_fixed_iters_mt(void* h, const double* b, i64 iters, double* x, int threads) {
+  const orc_csc* A = (const orc_csc*)h;
+  const i64 n = A->n;
+  const int nt = nthreads_or_default(threads);
+  std::vector<double> inv(n, 1.0), r(b, b + n), z(n), p(n), ap(n);
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (i64 col = 0; col < n; ++col)
+    for (i64 q = A->colptr[col]; q < A->colptr[col + 1]; ++q)
+      if (A->rowidx[q] == col) {
+        if (std::fabs(A->vals[q]) > 1e-15) inv[col] = 1.0 / A->vals[q];
+        break;
+      }
+  auto dot = [&](const double* u, const double* v) {
+    double s = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : s) num_threads(nt)
+    for (i64 i = 0; i < n; ++i) s += u[i] * v[i];
+    return s;
+  };
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (i64 i = 0; i < n; ++i) {
+    x[i] = 0.0;
+    z[i] = r[i] * inv[i];
+    p[i] = z[i];
+  }
+  const double bn = std::sqrt(dot(b, b));
+  double rz = dot(r.data(), z.data()), rn = bn;
+  for (i64 it = 1; it <= iters; ++it) {
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (i64 row = 0; row < n; ++row) {
+      double s = 0.0;
+      for (i64 q = A->colptr[row]; q < A->colptr[row + 1]; ++q) s += A->vals[q] * p[A->rowidx[q]];
+      ap[row] = s;
+    }
+    const double alpha = rz / dot(p.data(), ap.data());
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (i64 i = 0; i < n; ++i) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * ap[i];
+      z[i] = r[i] * inv[i];
+    }
+    rn = std::sqrt(dot(r.data(), r.data()));
+    const double rzn = dot(r.data(), z.data());
+    const double beta = rzn / rz;
+    rz = rzn;
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (i64 i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+  }
+  return bn > 0.0 ? rn / bn : rn;
+}
+
 double orc_cg_fixed_iters(void* h, const double* b, i64 iters, double* x) {
   const orc_csc* A = (const orc_csc*)h;
   i64 n = A->n;

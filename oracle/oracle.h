@@ -49,6 +49,7 @@ int orc_affine_map_3d(const double* verts, double* det, double* invT);
 void orc_p2_basis(const double* xi, double* phi);
 void orc_p2_grads(const double* xi, double* g);
 void orc_p2_mass_products(double* out);
+double orc_cg_fixed_iters_mt(void* h, const double* b, i64 iters, double* x, int threads);
 void* orc_assemble_mass(i64 ndofs, const double* coords, i64 nc, const i64* cells, const i64* cell_dofs, int kind,
                         double density, const double* coef);
 #ifdef __cplusplus
