@@ -670,6 +670,56 @@ def run_reference(args, cfg):
     }
 
 
+PROFILE_CASES = ("mass_c2", "block_update_c2", "transient_1024")
+
+
+def profile_case(name):
+    """A short run of one kernel on one workload, for profiler captures: no
+    timing, a few launches, a few hundred MB on the device.
+      mass_c2          vector-P1 mass of the C2 mesh, assembled 3 times
+      block_update_c2  12 block-Jacobi FP64 PCG iterations on the C2 system
+      transient_1024   3 Crank-Nicolson steps of the 1024^2 heat problem,
+                       12 PCG iterations each"""
+    import torch
+    import fenics_cuda as fcu
+    ctx = fcu.Context(0)
+    if name in ("mass_c2", "block_update_c2"):
+        mesh = fcu.box_beam(4.0, 1.0, 1.0, 128, 32, 32)
+        V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+        if name == "mass_c2":
+            M = fcu.Matrix(ctx, V)
+            for _ in range(3):
+                M.assemble_mass(7850.0)
+        else:
+            M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+            cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+            dofs = (3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64)
+            b = V.body_force([0.0, 0.0, -7.8e4])
+            M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
+            M.block_jacobi(True)
+            M.pcg(b, tol=1e-30, max_iter=12, raise_on_error=False)
+        ctx.synchronize()
+        M.close(); V.close()
+    elif name == "transient_1024":
+        mesh = fcu.unit_square(1024, 1024)
+        V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
+        Mm = fcu.Matrix(ctx, V).assemble_mass(1.0)
+        K = fcu.Matrix(ctx, V).assemble_stiffness(None)
+        st = fcu._Stepper(ctx, Mm, K, fcu.FCU_CRANK_NICOLSON, 1e-4)
+        dev = torch.device("cuda", 0)
+        u = torch.as_tensor(np.sin(math.pi * mesh.coords[:, 0]) * np.sin(math.pi * mesh.coords[:, 1])).to(dev)
+        un = torch.empty_like(u)
+        for _ in range(3):
+            try:
+                st.step(u, None, None, un, 1e-30, 12, fcu.FCU_FP64)
+            except fcu.CgError:
+                pass   # 12 iterations, no convergence: the point is the kernels
+            u, un = un, u
+        ctx.synchronize()
+        st.close(); Mm.close(); K.close(); V.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -679,7 +729,11 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the C1/C2'/C3/C4/C5 workload measurements")
+    ap.add_argument("--profile", choices=PROFILE_CASES, help="run one kernel's short profiling case and exit")
     args = ap.parse_args()
+    if args.profile:
+        profile_case(args.profile)
+        return
     cfg = CONFIGS[args.config]
     res = run_reference(args, cfg) if args.impl == "reference" else run_cuda(args, cfg)
     if res is not None:

@@ -324,6 +324,23 @@ void check_ctx(fcu_ctx ctx) {
   if (!ctx) fail(FCU_ERR_BAD_ARG, "null context");
 }
 
+// Spaces on the caller's P2 node numbering support mass and stiffness only.
+void reject_node_space(fcu_space s) {
+  if (s && (s->kind == FCU_SPACE_P2_NODES || s->kind == FCU_SPACE_P2_NODES_VEC3))
+    fail(FCU_ERR_UNSUPPORTED, "a P2 space on caller nodes supports mass and stiffness assembly only");
+}
+
+__global__ void k_cells10(const i64* __restrict__ c10, const int* __restrict__ cells4, i64 nc, i64 nv,
+                          int* __restrict__ out, int* __restrict__ bad) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < 10 * nc; t += (i64)gridDim.x * blockDim.x) {
+    const i64 v = c10[t];
+    const i64 c = t / 10;
+    const int a = (int)(t - 10 * c);
+    if (v < 0 || v >= nv || (a < 4 && v != cells4[4 * c + a])) atomicExch(bad, 1);
+    out[t] = (int)v;
+  }
+}
+
 void ctx_release(fcu_ctx c) {
   if (!c || --c->refs > 0) return;
   cudaSetDevice(c->device);
@@ -564,6 +581,35 @@ int fcu_space_create(fcu_ctx ctx, fcu_mesh mesh, int kind, fcu_space* out) {
   });
 }
 
+int fcu_space_create_p2_nodes(fcu_ctx ctx, fcu_mesh mesh, const int64_t* cells10, int vec3, fcu_space* out) {
+  if (!out) return FCU_ERR_BAD_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    if (!mesh || (mesh->nc > 0 && !cells10)) fail(FCU_ERR_BAD_ARG, "null argument");
+    if (mesh->dim != 3) fail(FCU_ERR_BAD_ARG, "P2 spaces need a tetrahedral mesh");
+    if (10 * mesh->nc >= (1ll << 31)) fail(FCU_ERR_UNSUPPORTED, "mesh exceeds 32-bit indexing");
+    std::unique_ptr<fcu_space_s> s(new fcu_space_s());
+    s->ctx = ctx;
+    s->mesh = mesh;
+    s->kind = vec3 ? FCU_SPACE_P2_NODES_VEC3 : FCU_SPACE_P2_NODES;
+    s->cell_nodes.alloc(10 * mesh->nc);
+    if (mesh->nc) {
+      DevIn<i64> c10(ctx, cells10, 10 * mesh->nc);
+      DBuf<int> bad;
+      bad.alloc(1);
+      CUDA_CHECK(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+      k_cells10<<<grid_for(10 * mesh->nc, 256, cap_blocks(ctx)), 256, 0, ctx->stream>>>(
+          c10.p, mesh->cells.p, mesh->nc, mesh->nv, s->cell_nodes.p, bad.p);
+      LAUNCH_CHECK(ctx);
+      if (read1(ctx, bad.p)) fail(FCU_ERR_BAD_ARG, "cell node out of range or corners differ from the mesh cell");
+    }
+    build_space_pattern(s.get());
+    sync(ctx);
+    mesh->refs++;
+    *out = s.release();
+  });
+}
+
 void fcu_space_destroy(fcu_space s) { space_release(s); }
 
 int fcu_space_info(fcu_space s, int64_t* ndofs, int64_t* nnz, int64_t* nedges) {
@@ -602,6 +648,7 @@ int fcu_space_p2_dofmap(fcu_ctx ctx, fcu_space s, int64_t* cell_dofs, int64_t* e
 
 int fcu_space_boundary_dofs(fcu_ctx ctx, fcu_space s, int64_t* out, int64_t* count) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || !count) fail(FCU_ERR_BAD_ARG, "null argument");
     DBuf<i64> res;
     i64 k = boundary_dofs_impl(s->mesh, s, res);
@@ -826,6 +873,7 @@ int fcu_assemble_stiffness(fcu_ctx ctx, fcu_matrix m, const double* cell_coef) {
   return guarded(ctx, [&] {
     if (!m || !m->space) fail(FCU_ERR_BAD_ARG, "matrix has no function space");
     if (m->space->kind == FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "use fcu_assemble_elasticity for vector spaces");
+    if (m->space->kind == FCU_SPACE_P2_NODES_VEC3) fail(FCU_ERR_UNSUPPORTED, "no vector P2 stiffness");
     DevIn<double> coef(ctx, cell_coef, (size_t)m->space->mesh->nc);
     reset_dirichlet(m);
     m->comp_diag = false;
@@ -927,6 +975,7 @@ static i64 num_qpoints(fcu_space s) { return s->mesh->nc * (s->mesh->dim == 2 ? 
 
 int fcu_quadrature_points(fcu_ctx ctx, fcu_space s, double* out) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || !out) fail(FCU_ERR_BAD_ARG, "null argument");
     DevOut<double> o(out, num_qpoints(s) * s->mesh->dim);
     if (s->mesh->nc) quadrature_points_impl(s, o.p);
@@ -937,6 +986,7 @@ int fcu_quadrature_points(fcu_ctx ctx, fcu_space s, double* out) {
 
 int fcu_assemble_rhs_values(fcu_ctx ctx, fcu_space s, const double* fq, double* b) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || !b || (!fq && s->mesh->nc)) fail(FCU_ERR_BAD_ARG, "null argument");
     if (s->kind == FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "scalar spaces only");
     DevIn<double> f(ctx, fq, num_qpoints(s));
@@ -950,6 +1000,7 @@ int fcu_assemble_rhs_values(fcu_ctx ctx, fcu_space s, const double* fq, double* 
 int fcu_assemble_rhs_source(fcu_ctx ctx, fcu_space s, int source, const double* params, const double* values,
                             double* b) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || !b) fail(FCU_ERR_BAD_ARG, "null argument");
     if (s->kind == FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "scalar spaces only");
     double p[2] = {0.0, 0.0};
@@ -970,6 +1021,7 @@ int fcu_assemble_rhs_source(fcu_ctx ctx, fcu_space s, int source, const double* 
 
 int fcu_assemble_body_force(fcu_ctx ctx, fcu_space s, const double* f, double* b) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || !f || !b) fail(FCU_ERR_BAD_ARG, "null argument");
     if (s->kind != FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "vector space only");
     double fh[3];
@@ -984,6 +1036,7 @@ int fcu_assemble_body_force(fcu_ctx ctx, fcu_space s, const double* f, double* b
 int fcu_assemble_surface_traction(fcu_ctx ctx, fcu_space s, int64_t nf, const int64_t* facets, const double* tq,
                                   double* b) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || !b || nf < 0 || (nf > 0 && (!facets || !tq))) fail(FCU_ERR_BAD_ARG, "bad traction arguments");
     if (s->kind != FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "vector space only");
     DevIn<i64> fd(ctx, facets, 3 * nf);
@@ -1127,6 +1180,7 @@ int fcu_spmv(fcu_ctx ctx, fcu_matrix m, const double* x, double* y) {
 int fcu_adjoint_gradient(fcu_ctx ctx, fcu_space s, double E0, double nu, const double* theta, const double* u,
                          const double* lambda, double* grad) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || s->kind != FCU_SPACE_P1_VEC3) fail(FCU_ERR_BAD_ARG, "needs a FCU_SPACE_P1_VEC3 space");
     if (!theta || !u || !lambda || !grad) fail(FCU_ERR_BAD_ARG, "null argument");
     if (!(nu > -1.0 && nu < 0.5)) fail(FCU_ERR_BAD_ARG, "Poisson's ratio must be in (-1.0, 0.5)");
@@ -1142,6 +1196,7 @@ int fcu_adjoint_gradient(fcu_ctx ctx, fcu_space s, double E0, double nu, const d
 int fcu_element_stresses(fcu_ctx ctx, fcu_space s, double E, double nu, const double* u, double* stress,
                          double* strain, double* von_mises, double* trace) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || (s->kind != FCU_SPACE_P1_VEC3 && !(s->kind == FCU_SPACE_P1 && s->mesh->dim == 3)))
       fail(FCU_ERR_BAD_ARG, "needs a space on a tetrahedron mesh (P1 or vector P1)");
     if (!u) fail(FCU_ERR_BAD_ARG, "null displacement");
@@ -1163,6 +1218,7 @@ int fcu_element_stresses(fcu_ctx ctx, fcu_space s, double E, double nu, const do
 
 int fcu_vertex_von_mises(fcu_ctx ctx, fcu_space s, const double* cell_von_mises, double* vertex_von_mises) {
   return guarded(ctx, [&] {
+    reject_node_space(s);
     if (!s || (s->kind != FCU_SPACE_P1_VEC3 && !(s->kind == FCU_SPACE_P1 && s->mesh->dim == 3)))
       fail(FCU_ERR_BAD_ARG, "needs a space on a tetrahedron mesh (P1 or vector P1)");
     if (!cell_von_mises || !vertex_von_mises) fail(FCU_ERR_BAD_ARG, "null argument");

@@ -625,7 +625,7 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
   fcu_ctx ctx = m->ctx;
   fcu_mesh me = s->mesh;
   const int nb = assembly_blocks(ctx, s->nnodes);
-  if (s->kind == FCU_SPACE_P2) {
+  if (s->kind == FCU_SPACE_P2 || s->kind == FCU_SPACE_P2_NODES) {
     ensure_p2_tables(ctx);
     DBuf<double> geo;
     geo.alloc((size_t)me->nc * P2_GEO);
@@ -667,7 +667,8 @@ void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev) {
   fcu_ctx ctx = m->ctx;
   fcu_mesh me = s->mesh;
   MassTable tab{};
-  if (s->kind == FCU_SPACE_P2) {
+  const bool p2 = s->kind == FCU_SPACE_P2 || s->kind == FCU_SPACE_P2_NODES || s->kind == FCU_SPACE_P2_NODES_VEC3;
+  if (p2) {
     p2_mass_products(tab.F);
   } else {
     const int K = s->k;
@@ -678,7 +679,11 @@ void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev) {
   const int nb = assembly_blocks(ctx, s->nnodes);
   const int* cn = s->cell_nodes.p;
   const double* X = me->coords.p;
-  if (s->kind == FCU_SPACE_P2) {
+  if (s->kind == FCU_SPACE_P2_NODES_VEC3) {
+    k_assemble_mass<10, 3, 3><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                                   s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
+                                                                   tab, s->nnodes, m->val64.p, m->val32.p);
+  } else if (p2) {
     k_assemble_mass<10, 3, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                    s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
                                                                    tab, s->nnodes, m->val64.p, m->val32.p);

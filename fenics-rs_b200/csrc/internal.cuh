@@ -177,6 +177,8 @@ struct fcu_matrix_s {
   bool block_jacobi = false;  // bdinv derived from the values at every solve
   int max_row_own = 0;  // longest block row of a wrapped block CSR matrix
   bool missing_diag = false;  // a wrapped block row without a diagonal block
+  DBuf<int> rowblk;     // row blocks of the CSR-stream SpMV (scalar, built on first use)
+  int nrowblk = 0;
   Workspace* ws = nullptr;
   BatchWorkspace* bws = nullptr;
   ~fcu_matrix_s();

@@ -276,7 +276,12 @@ void build_space_pattern(fcu_space s) {
   const i64 nc = m->nc, nv = m->nv;
 
   // --- cell -> node map -----------------------------------------------------
-  if (s->kind == FCU_SPACE_P2) {
+  if (s->kind == FCU_SPACE_P2_NODES || s->kind == FCU_SPACE_P2_NODES_VEC3) {
+    // the caller's ten nodes per cell are already in cell_nodes
+    s->k = 10;
+    s->nnodes = nv;
+    s->bs = s->kind == FCU_SPACE_P2_NODES_VEC3 ? 3 : 1;
+  } else if (s->kind == FCU_SPACE_P2) {
     s->k = 10;
     i64 ne6 = 6 * nc;
     DBuf<unsigned long long> ek, eks;

@@ -56,6 +56,7 @@ struct CgState {
   int pause;  // mixed: a replacement is due; the rest of the graph replay is skipped
   int gpu_semantics;  // solve_csr_cg_gpu: no breakdown test, beta guard, Ok at limit
   int fault;          // a bounded wait in a kernel gave up (reported as FCU_ERR_CUDA)
+  int timing;         // SpMV timing runs: every launch computes alpha, nothing stops
   // arrival counters of the grid reductions: 32 group counters + 1 top counter
   unsigned ticket[4][33];
 };
@@ -255,7 +256,7 @@ __device__ __forceinline__ void spmv_rows(const int* __restrict__ rp, const int*
 // (gpu.rs:1326-1329, 1034-1037) stop with Ok when p.Ap <= 1e-30; the
 // iteration counts as done.
 __device__ __forceinline__ void set_alpha(CgState* st, double pap) {
-  if (st->gpu_semantics ? !(pap > 1e-30) : fabs(pap) < 1e-30) {
+  if (!st->timing && (st->gpu_semantics ? !(pap > 1e-30) : fabs(pap) < 1e-30)) {
     st->done = 1;
     st->status = st->gpu_semantics ? FCU_OK : FCU_ERR_BREAKDOWN;
     st->iter += 1;
@@ -694,33 +695,64 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
   }
 }
 
-// Block-Jacobi variant (FP64): one thread per block row applies the inverse
-// diagonal block to the row's three residual components (bsr3_apply_dinv).
-__global__ void __launch_bounds__(VBLOCK) k_update_block(i64 nn, double* __restrict__ x, double* __restrict__ r,
-                                                         const double* __restrict__ p, const double* __restrict__ ap,
-                                                         const double* __restrict__ bdinv, double* __restrict__ z,
-                                                         CgState* st, double* partials) {
+// Block-Jacobi variant (FP64). Tiles of 96 block rows (288 dofs, one thread
+// per dof): x, r, p, Ap and the thread's row of the inverse block are read
+// with coalesced loads, the new residual goes through shared memory, and
+// each thread forms its z = sum_b Dinv[a][b] r_b (bsr3_apply_dinv). As in
+// k_update, the first tile's x, r, p and inverse blocks are final before the
+// kernel starts and are fetched before the dependency wait.
+constexpr int UB_THREADS = 288;
+
+__global__ void __launch_bounds__(UB_THREADS) k_update_block(i64 nn, double* __restrict__ x, double* __restrict__ r,
+                                                             const double* __restrict__ p,
+                                                             const double* __restrict__ ap,
+                                                             const double* __restrict__ bdinv,
+                                                             double* __restrict__ z, CgState* st, double* partials) {
+  __shared__ double rs[UB_THREADS];
+  const i64 n = 3 * nn;
+  const int t = threadIdx.x;
+  const i64 tstride = (i64)gridDim.x * UB_THREADS;
+  i64 i = blockIdx.x * (i64)UB_THREADS + t;
+  double xa = 0.0, ra = 0.0, pa = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0;
+  if (i < n) {
+    xa = __ldcg(x + i);
+    ra = __ldcg(r + i);
+    pa = __ldcg(p + i);
+    d0 = __ldcg(bdinv + 3 * i);
+    d1 = __ldcg(bdinv + 3 * i + 1);
+    d2 = __ldcg(bdinv + 3 * i + 2);
+  }
   grid_dep_sync();
   if (st->done || st->pause) return;
   const double alpha = st->alpha;
   double rz = 0.0, rr = 0.0;
-  for (i64 w = blockIdx.x * (i64)blockDim.x + threadIdx.x; w < nn; w += (i64)gridDim.x * blockDim.x) {
-    double rn[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const i64 i = 3 * w + a;
-      x[i] += alpha * p[i];
-      rn[a] = r[i] - alpha * ap[i];
-      r[i] = rn[a];
-      rr += rn[a] * rn[a];
+  const i64 first = blockIdx.x * (i64)UB_THREADS;
+  for (i64 tile = first; tile < n; tile += tstride, i += tstride) {
+    const bool ok = i < n;
+    if (ok && tile != first) {
+      xa = x[i];
+      ra = r[i];
+      pa = p[i];
+      d0 = bdinv[3 * i];
+      d1 = bdinv[3 * i + 1];
+      d2 = bdinv[3 * i + 2];
     }
-    const double* D = bdinv + 9 * w;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const double zi = D[3 * a] * rn[0] + D[3 * a + 1] * rn[1] + D[3 * a + 2] * rn[2];
-      z[3 * w + a] = zi;
-      rz += rn[a] * zi;
+    double rn = 0.0;
+    if (ok) {
+      x[i] = xa + alpha * pa;
+      rn = ra - alpha * ap[i];
+      r[i] = rn;
+      rr += rn * rn;
     }
+    rs[t] = rn;
+    __syncthreads();
+    if (ok) {
+      const int b0 = t - t % 3;  // first dof of this block row in the tile
+      const double zi = d0 * rs[b0] + d1 * rs[b0 + 1] + d2 * rs[b0 + 2];
+      z[i] = zi;
+      rz += rn * zi;
+    }
+    __syncthreads();
   }
   double v[2] = {rz, rr}, tot[2];
   if (grid_reduce<2>(v, partials, st->ticket[1], tot) && threadIdx.x == 0) decide_after_update(st, tot[0], tot[1]);
@@ -872,6 +904,129 @@ __global__ void k_spmv_plain(const int* __restrict__ rp, const int* __restrict__
   spmv_rows<BS, VPR, false, double>(rp, ci, val, nrows, XPlain<double>{x}, em);
 }
 
+// ---------------------------------------------------------------------------
+// CSR-stream SpMV for scalar matrices with short rows. CTA-sized row blocks
+// (at most STREAM_ROWS rows and STREAM_NNZ entries, built once per matrix)
+// are taken in turn by each CTA: phase 1 reads the block's entries with
+// coalesced loads (value, and the gathered operand x[col]) into shared
+// memory; phase 2 gives each row to one thread, which sums its entries in
+// column order (the difference form for the mixed operator, the diagonal
+// found through diag_pos). A row longer than STREAM_NNZ is a block of its
+// own, summed in chunks by all threads and reduced in a fixed order.
+// ---------------------------------------------------------------------------
+
+constexpr int STREAM_THREADS = 256;
+constexpr int STREAM_ROWS = 256;
+constexpr int STREAM_NNZ = 2048;
+
+template <bool DIFF, class T, class Emit>
+__device__ __forceinline__ void stream_rows(const int* __restrict__ rp, const int* __restrict__ ci,
+                                            const T* __restrict__ val, const int* __restrict__ dpos,
+                                            const int* __restrict__ rb, int nblk, const T* __restrict__ x, Emit& emit) {
+  __shared__ T sv[STREAM_NNZ];
+  __shared__ T sx[DIFF ? STREAM_NNZ : 1];
+  __shared__ T red[STREAM_THREADS / 32];
+  const int t = threadIdx.x;
+  for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    const int r0 = rb[blk], r1 = rb[blk + 1];
+    const int base = rp[r0], nnz = rp[r1] - base;
+    if (nnz > STREAM_NNZ) {
+      // one long row
+      const T xi = DIFF ? x[r0] : T(0);
+      const int dp = DIFF ? dpos[r0] : -1;
+      T s = T(0);
+      for (int q = base + t; q < base + nnz; q += STREAM_THREADS) {
+        if (DIFF) s += val[q] * (q == dp ? xi : x[ci[q]] - xi);
+        else s += val[q] * x[ci[q]];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+      if ((t & 31) == 0) red[t >> 5] = s;
+      __syncthreads();
+      if (t == 0) {
+        T tot = T(0);
+        for (int w = 0; w < STREAM_THREADS / 32; ++w) tot += red[w];
+        emit((i64)r0, 0, tot);
+      }
+      __syncthreads();
+      continue;
+    }
+#pragma unroll 4
+    for (int q = t; q < nnz; q += STREAM_THREADS) {
+      const int g = base + q;
+      const T v = val[g];
+      const T xj = x[ci[g]];
+      if (DIFF) {
+        sv[q] = v;
+        sx[q] = xj;
+      } else {
+        sv[q] = v * xj;
+      }
+    }
+    __syncthreads();
+    for (int row = r0 + t; row < r1; row += STREAM_THREADS) {
+      const int b = rp[row] - base, e = rp[row + 1] - base;
+      T s = T(0);
+      if (DIFF) {
+        const T xi = x[row];
+        const int dp = dpos[row] - base;
+        for (int q = b; q < e; ++q) s += sv[q] * (q == dp ? xi : sx[q] - xi);
+      } else {
+        for (int q = b; q < e; ++q) s += sv[q];
+      }
+      emit((i64)row, 0, s);
+    }
+    __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(STREAM_THREADS) k_spmv_stream(const int* __restrict__ rp, const int* __restrict__ ci,
+                                                                const T* __restrict__ val,
+                                                                const int* __restrict__ dpos,
+                                                                const int* __restrict__ rb, int nblk,
+                                                                const T* __restrict__ p, T* __restrict__ ap,
+                                                                CgState* st, double* partials) {
+  grid_dep_sync();
+  if (st->done || st->pause) return;
+  EmitApPlain<1, T> em{p, ap};
+  stream_rows<sizeof(T) == 4, T>(rp, ci, val, dpos, rb, nblk, p, em);
+  double v[1] = {em.dot}, tot[1];
+  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) set_alpha(st, tot[0]);
+}
+
+__global__ void __launch_bounds__(STREAM_THREADS) k_spmv_stream_plain(const int* __restrict__ rp,
+                                                                      const int* __restrict__ ci,
+                                                                      const double* __restrict__ val,
+                                                                      const int* __restrict__ rb, int nblk,
+                                                                      const double* __restrict__ x,
+                                                                      double* __restrict__ y) {
+  grid_dep_sync();
+  EmitStore<1> em{y};
+  stream_rows<false, double>(rp, ci, val, nullptr, rb, nblk, x, em);
+}
+
+// Row blocks of the stream kernel: consecutive rows while at most
+// STREAM_ROWS rows and STREAM_NNZ entries fit; a longer row alone.
+void build_row_blocks(fcu_ctx ctx, const int* rp_dev, i64 nrows, DBuf<int>& rb, int* nblk) {
+  std::vector<int> rp(nrows + 1);
+  CUDA_CHECK(cudaMemcpyAsync(rp.data(), rp_dev, (nrows + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  std::vector<int> b;
+  b.push_back(0);
+  i64 r = 0;
+  while (r < nrows) {
+    i64 e = r;
+    while (e < nrows && e - r < STREAM_ROWS && (i64)rp[e + 1] - rp[r] <= STREAM_NNZ) ++e;
+    if (e == r) e = r + 1;  // a row longer than STREAM_NNZ
+    b.push_back((int)e);
+    r = e;
+  }
+  *nblk = (int)b.size() - 1;
+  upload(ctx, rb, b.data(), b.size());
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -886,6 +1041,7 @@ struct Workspace {
   DBuf<CgState> st;
   CgState* host_st = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool stream[2] = {false, false};  // scalar PCG SpMV: CSR-stream kernel (FP64, FP32)
   int vpr = 0;    // lanes per row of the FP64 CSR kernels (tuned with the FP64 SpMV)
   int vpr32 = 0;  // lanes per row of the FP32 CSR SpMV (tuned with it)
   int stages[2] = {3, 3};  // ring depth of the tiled block SpMV: FP64, FP32
@@ -934,6 +1090,35 @@ int vec_blocks_per_sm() {
   return v;
 }
 
+// CSR-stream SpMV for scalar rows of at most 32 entries on average
+// (FCU_STREAM_SPMV=0 disables it).
+bool use_stream_spmv(fcu_matrix m) {
+  static int v = [] {
+    const char* e = getenv("FCU_STREAM_SPMV");
+    return e ? atoi(e) : 1;
+  }();
+  if (!v || m->bs != 1) return false;
+  return m->nnodes > 0 && (double)m->nnzb <= 32.0 * (double)m->nnodes;
+}
+
+// One wave of the block-Jacobi update (its first tile is prefetched before
+// the dependency wait).
+int update_block_grid(fcu_ctx ctx, i64 nn) {
+  static int occ = -1;
+  if (occ < 0) {
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_update_block, UB_THREADS, 0));
+    occ = std::max(1, std::min(occ, 8));
+  }
+  const i64 tiles = (3 * nn + UB_THREADS - 1) / UB_THREADS;
+  return (int)std::max<i64>(1, std::min<i64>(tiles, (i64)ctx->num_sms * occ));
+}
+
+int stream_grid(fcu_ctx ctx, int nblk) { return std::max(1, std::min(nblk, ctx->num_sms * 6)); }
+
+void ensure_row_blocks(fcu_matrix m) {
+  if (!m->nrowblk) build_row_blocks(m->ctx, m->row_ptr, m->nnodes, m->rowblk, &m->nrowblk);
+}
+
 int pick_vpr(fcu_matrix m) {
   if (m->bs == 3) return 16;
   double avg = m->nnodes ? (double)m->nnzb / (double)m->nnodes : 1.0;
@@ -957,6 +1142,10 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     CUDA_CHECK(cudaMallocHost(&w->host_st, sizeof(CgState)));
     w->vpr = pick_vpr(m);
     w->vpr32 = w->vpr;
+    if (m->bs == 1 && use_stream_spmv(m)) {
+      ensure_row_blocks(m);
+      w->stream[0] = w->stream[1] = true;
+    }
     w->grid = solver_grid(ctx, n);
     // one wave of the update kernel (its first two elements per thread are
     // fetched before the dependency wait, which only resident blocks do early)
@@ -1090,12 +1279,16 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       launch_pdl(ctx, k_direction<double>, w->vgrid, n, w->pa64.p, w->z64.p, w->st.p);
       if (m->bs == 3 && use_tiled_spmv())
         launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+      else if (w->stream[0])
+        launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+                       m->col_idx, m->val64.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa64.p, w->ap64.p, w->st.p,
+                       w->partials.p);
       else
         DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, nr, w->pa64.p, w->ap64.p,
                       w->st.p, w->partials.p);
       if (m->bdinv.p)
-        launch_pdl(ctx, k_update_block, w->vgrid, m->nnodes, w->x.p, w->r.p, w->pa64.p, w->ap64.p, m->bdinv.p,
-                   w->z64.p, w->st.p, w->partials.p);
+        launch_pdl_cfg(ctx, k_update_block, update_block_grid(ctx, m->nnodes), UB_THREADS, 0, m->nnodes, w->x.p,
+                       w->r.p, w->pa64.p, w->ap64.p, m->bdinv.p, w->z64.p, w->st.p, w->partials.p);
       else
         launch_pdl(ctx, k_update<double>, w->vgrid, n, w->x.p, w->r.p, w->pa64.p, w->ap64.p, w->invd.p, w->z64.p,
                    w->st.p, w->partials.p);
@@ -1103,6 +1296,10 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       launch_pdl(ctx, k_direction<float>, w->vgrid, n, w->pa32.p, w->z32.p, w->st.p);
       if (m->bs == 3 && use_tiled_spmv())
         launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+      else if (w->stream[1])
+        launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+                       m->col_idx, m->val32.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa32.p, w->ap32.p, w->st.p,
+                       w->partials.p);
       else
         DISPATCH_ROWS(m->bs, w->vpr32, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, nr, w->pa32.p, w->ap32.p,
                       w->st.p, w->partials.p);
@@ -1310,6 +1507,12 @@ void invalidate_graphs(fcu_matrix m) {
 
 void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev) {
   fcu_ctx ctx = m->ctx;
+  if (use_stream_spmv(m)) {
+    ensure_row_blocks(m);
+    launch_pdl_cfg(ctx, k_spmv_stream_plain, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr, m->col_idx,
+                   m->val64.p, m->rowblk.p, m->nrowblk, x_dev, y_dev);
+    return;
+  }
   const int vpr = pick_vpr(m);
   const int g = solver_grid(ctx, m->n);
   DISPATCH_ROWS(m->bs, vpr, g, K_PLAIN, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, x_dev, y_dev);
@@ -1330,6 +1533,7 @@ void spmv_timing_state(fcu_matrix m, Workspace* w, bool mixed) {
   init.rz = 1.0;
   init.beta = 0.5;
   init.gpu_semantics = 1;
+  init.timing = 1;
   *w->host_st = init;
   CUDA_CHECK(cudaMemcpyAsync(w->st.p, w->host_st, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
   const i64 n = m->n;
@@ -1349,11 +1553,19 @@ void enqueue_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   const int g = w->grid;
   if (mixed) {
     if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+    else if (w->stream[1])
+      launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+                     m->col_idx, m->val32.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa32.p, w->ap32.p, w->st.p,
+                     w->partials.p);
     else
       DISPATCH_ROWS(m->bs, w->vpr32, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, m->nnodes, w->pa32.p,
                     w->ap32.p, w->st.p, w->partials.p);
   } else {
     if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+    else if (w->stream[0])
+      launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+                     m->col_idx, m->val64.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa64.p, w->ap64.p, w->st.p,
+                     w->partials.p);
     else
       DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->pa64.p,
                     w->ap64.p, w->st.p, w->partials.p);
@@ -1423,21 +1635,29 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
     // Lanes per row change the summation order inside a row, so a shape
     // replaces the default only when it is clearly (10%) faster: near-ties
     // then cannot flip the choice, and the iterates, from run to run.
+    // Candidates: the CSR-stream kernel (when the rows are short) and CSR
+    // vectors of 4-32 lanes per row.
     int& v = mixed ? w->vpr32 : w->vpr;
+    bool& strm = w->stream[k];
+    const bool dflt_stream = strm;
     const int dflt = v;
     const double dflt_ms = trial();
+    bool best_stream = dflt_stream;
     int best = dflt;
     double best_ms = dflt_ms;
+    strm = false;
     for (int c : {4, 8, 16, 32}) {
-      if (c == dflt) continue;
+      if (c == dflt && !dflt_stream) continue;
       v = c;
       const double ms = trial();
       if (ms < 0.9 * dflt_ms && ms < best_ms) {
         best_ms = ms;
         best = c;
+        best_stream = false;
       }
     }
     v = best;
+    strm = best_stream;
   }
 }
 

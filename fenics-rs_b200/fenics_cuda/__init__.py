@@ -43,6 +43,7 @@ __all__ = [
     "extract_boundary_facets", "solve_cg", "solve_csr_cg_gpu", "solve_cg_gpu_or_cpu", "GpuSolveResult",
     "solve_poisson_2d", "solve_poisson_3d", "solve_elasticity_3d", "spmv",
     "assemble_mass_2d", "assemble_mass_3d", "assemble_elasticity_mass_3d", "assemble_mass_p2_3d",
+    "assemble_elasticity_mass_p2_3d",
     "add_scaled_matrices", "TimeSteppingScheme", "TransientHeatSolver", "TransientHeatSolution",
     "solve_transient_heat_2d", "fold_dirichlet", "VibrationMode", "solve_vibration_modes",
     "solve_vibration_modes_with_inner", "GpuBsr3Context", "solve_bsr3_pcg_gpu", "spmv_bsr3_multi_gpu",
@@ -268,10 +269,16 @@ def extract_boundary_facets(mesh: Mesh, ctx: Context | None = None):
 class FunctionSpace:
     """Dof map + sparsity pattern of P1 / P2 / vector-P1 on a mesh, on the device."""
 
-    def __init__(self, ctx: Context, mesh: Mesh, kind: int):
+    def __init__(self, ctx: Context, mesh: Mesh, kind: int, cells10=None):
         self.ctx, self.mesh, self.kind = ctx, mesh, kind
         h = C.c_void_p()
-        _check(ctx, _L().fcu_space_create(ctx.h, mesh.handle(ctx), kind, C.byref(h)))
+        if kind in (_abi.FCU_SPACE_P2_NODES, _abi.FCU_SPACE_P2_NODES_VEC3):
+            pc, kc = _ptr(cells10, np.int64)
+            _check(ctx, _L().fcu_space_create_p2_nodes(ctx.h, mesh.handle(ctx), pc,
+                                                       1 if kind == _abi.FCU_SPACE_P2_NODES_VEC3 else 0,
+                                                       C.byref(h)))
+        else:
+            _check(ctx, _L().fcu_space_create(ctx.h, mesh.handle(ctx), kind, C.byref(h)))
         self.h = h
         nd, nz, ne = C.c_int64(), C.c_int64(), C.c_int64()
         _L().fcu_space_info(h, C.byref(nd), C.byref(nz), C.byref(ne))
@@ -1080,6 +1087,21 @@ def assemble_mass_p2_3d(mesh: Mesh, density=1.0, ctx: Context | None = None) -> 
     assemble_elasticity_mass_p2_3d (mass.rs:137-250), on this build's P2
     numbering (vertices, then edges)."""
     return _assembled(FCU_SPACE_P2, mesh, ctx, lambda M: M.assemble_mass(float(density)))
+
+
+def assemble_elasticity_mass_p2_3d(vertices, cells, density, ctx: Context | None = None) -> CscMatrix:
+    """assemble_elasticity_mass_p2_3d (mass.rs:137-180): vertices = every P2
+    node, cells = ten nodes per cell (4 corners, then edges 01, 12, 02, 03,
+    13, 23); dof = 3 node + component."""
+    ctx = ctx or default_context()
+    c10 = np.ascontiguousarray(cells, dtype=np.int64).reshape(-1, 10)
+    mesh = Mesh(np.ascontiguousarray(vertices, dtype=np.float64), np.ascontiguousarray(c10[:, :4]))
+    V = FunctionSpace(ctx, mesh, _abi.FCU_SPACE_P2_NODES_VEC3, cells10=c10)
+    M = Matrix(ctx, V).assemble_mass(float(density))
+    A = M.export_csc()
+    M.close()
+    V.close()
+    return A
 
 
 def _as_matrix(ctx, mat):

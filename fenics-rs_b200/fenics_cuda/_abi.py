@@ -23,6 +23,8 @@ FCU_NOALLOC_MAX_N = 131072  # row capacity of fcu_solve_csr_cg_noalloc
 FCU_SPACE_P1 = 1
 FCU_SPACE_P2 = 2
 FCU_SPACE_P1_VEC3 = 3
+FCU_SPACE_P2_NODES = 4
+FCU_SPACE_P2_NODES_VEC3 = 5
 
 FCU_FP64 = 0
 FCU_MIXED = 1
@@ -69,6 +71,7 @@ SIGNATURES = {
     "fcu_boundary_dofs": (cint, [vp, vp, vp, C.POINTER(i64)]),
     "fcu_boundary_facets": (cint, [vp, vp, vp, vp, vp, C.POINTER(i64)]),
     "fcu_space_create": (cint, [vp, vp, cint, C.POINTER(vp)]),
+    "fcu_space_create_p2_nodes": (cint, [vp, vp, vp, cint, C.POINTER(vp)]),
     "fcu_space_destroy": (None, [vp]),
     "fcu_space_info": (cint, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
     "fcu_space_p2_dofmap": (cint, [vp, vp, vp, vp]),

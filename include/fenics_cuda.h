@@ -43,6 +43,10 @@ extern "C" {
 #define FCU_SPACE_P1 1      /* scalar P1 on triangles (dim 2) or tetrahedra (dim 3) */
 #define FCU_SPACE_P2 2      /* scalar P2 on tetrahedra: vertex dofs, then edges     */
 #define FCU_SPACE_P1_VEC3 3 /* vector P1 on tetrahedra, dof = 3*vertex + component  */
+/* P2 on the caller's 10-node tetrahedra (fcu_space_create_p2_nodes): dof =
+ * node (scalar) or 3*node + component (vector); mass and stiffness only. */
+#define FCU_SPACE_P2_NODES 4
+#define FCU_SPACE_P2_NODES_VEC3 5
 
 /* ---- solver precision ----------------------------------------------------- */
 #define FCU_FP64 0  /* FP64 Jacobi-PCG (cg.rs:40-149 arithmetic)                 */
@@ -112,6 +116,13 @@ int fcu_space_info(fcu_space space, int64_t* ndofs, int64_t* nnz, int64_t* nedge
 /* P2: cell dof map (nc*10, P2Tetrahedron local order, lagrange.rs:286-299) and
  * edge vertex pairs (nedges*2); either may be NULL. */
 int fcu_space_p2_dofmap(fcu_ctx ctx, fcu_space space, int64_t* cell_dofs, int64_t* edge_verts);
+/* A P2 space on the caller's numbering (assemble_elasticity_mass_p2_3d,
+ * mass.rs:137-180): `mesh` holds every P2 node as a vertex and each cell's
+ * four corners as its tetrahedron; cells10 (nc*10) gives the ten nodes of
+ * each cell in P2Tetrahedron order (4 corners, then edges 01, 12, 02, 03,
+ * 13, 23), its first four equal to the mesh cell. vec3 != 0 gives
+ * FCU_SPACE_P2_NODES_VEC3. */
+int fcu_space_create_p2_nodes(fcu_ctx ctx, fcu_mesh mesh, const int64_t* cells10, int vec3, fcu_space* out);
 /* Boundary dofs of the space: P1 = boundary_dofs_*; P2 = boundary vertices and
  * boundary edges, sorted. out==NULL queries count. */
 int fcu_space_boundary_dofs(fcu_ctx ctx, fcu_space space, int64_t* out, int64_t* count);

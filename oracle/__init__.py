@@ -544,6 +544,22 @@ def assemble_p2_mass_3d(m: Mesh, cell_dofs, ndofs, density: float = 1.0, coef=No
     return _mass(m, 3, density, coef, cell_dofs, ndofs)
 
 
+def assemble_elasticity_mass_p2_3d(vertices, cells10, density: float) -> Csc:
+    """assemble_elasticity_mass_p2_3d (mass.rs:137-180): vertices = every P2
+    node, cells10 = ten nodes per cell in P2Tetrahedron order."""
+    c10 = _i64(cells10)
+    m = Mesh(np.ascontiguousarray(vertices, dtype=np.float64), np.ascontiguousarray(c10[:, :4]))
+    return _mass(m, 4, density, None, c10, 3 * m.nv)
+
+
+def p2_node_mesh(m: Mesh):
+    """(vertices, cells10) of the P2 node mesh over a tetrahedron mesh: the
+    vertices, then the edge midpoints in this build's edge order."""
+    cd, ev = p2_dofmap(m)
+    mid = 0.5 * (m.coords[ev[:, 0]] + m.coords[ev[:, 1]])
+    return np.concatenate([m.coords, mid]), cd
+
+
 def _triplets(A: Csc):
     cols = np.repeat(np.arange(A.n, dtype=np.int64), np.diff(A.colptr))
     return A.rowidx.astype(np.int64), cols, A.vals

@@ -855,11 +855,13 @@ void orc_p2_mass_products(double* out) {
 }
 
 // kind: 0 = P1 triangles, 1 = P1 tetrahedra, 2 = vector P1 tetrahedra,
-// 3 = scalar P2 tetrahedra (cell_dofs gives the ten dofs of each cell).
+// 3 = scalar P2 tetrahedra (cell_dofs gives the ten dofs of each cell),
+// 4 = vector P2 (assemble_elasticity_mass_p2_3d, mass.rs:137-180: dof
+// 3 node + component, cell_dofs the ten nodes of each cell).
 void* orc_assemble_mass(i64 ndofs, const double* coords, i64 nc, const i64* cells, const i64* cell_dofs, int kind,
                         double density, const double* coef) {
-  const int k = kind == 0 ? 3 : (kind == 3 ? 10 : 4);
-  const int bs = kind == 2 ? 3 : 1;
+  const int k = kind == 0 ? 3 : (kind >= 3 ? 10 : 4);
+  const int bs = (kind == 2 || kind == 4) ? 3 : 1;
   const i64 per = (i64)k * k * bs;
   std::vector<i64> R(per * nc), C(per * nc);
   std::vector<double> V(per * nc);
@@ -877,16 +879,16 @@ void* orc_assemble_mass(i64 ndofs, const double* coords, i64 nc, const i64* cell
       const i64* t = cells + 4 * c;
       Map3 m;
       if (!map_tet(coords + 3 * t[0], coords + 3 * t[1], coords + 3 * t[2], coords + 3 * t[3], m)) continue;
-      meas = kind == 3 ? std::fabs(m.det) : (1.0 / 6.0) * std::fabs(m.det);
+      meas = kind >= 3 ? std::fabs(m.det) : (1.0 / 6.0) * std::fabs(m.det);
     }
     ok[c] = 1;
     double s = density * meas;
     if (coef) s = s * coef[c];
-    const i64* d = kind == 3 ? cell_dofs + 10 * c : cells + (i64)k * c;
+    const i64* d = kind >= 3 ? cell_dofs + 10 * c : cells + (i64)k * c;
     i64 o = per * c;
     for (int i = 0; i < k; ++i)
       for (int j = 0; j < k; ++j) {
-        double f = kind == 3 ? prod[10 * i + j] : (i == j ? (k == 3 ? 1.0 / 6.0 : 1.0 / 10.0)
+        double f = kind >= 3 ? prod[10 * i + j] : (i == j ? (k == 3 ? 1.0 / 6.0 : 1.0 / 10.0)
                                                           : (k == 3 ? 1.0 / 12.0 : 1.0 / 20.0));
         double v = s * f;
         for (int a = 0; a < bs; ++a) {

@@ -67,6 +67,38 @@ def test_p2_one_tet_products(fcu, ctx):
     assert np.max(np.abs(A.toarray()[np.ix_(cd[0], cd[0])] - P)) <= 1e-16
 
 
+def test_vector_p2_mass_on_caller_nodes(fcu, ctx):
+    # assemble_elasticity_mass_p2_3d (mass.rs:137-180): the reference element
+    # (mass.rs:305-323), then a perturbed cube's P2 node mesh, vs the oracle
+    v = np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0.5, 0, 0], [0.5, 0.5, 0], [0, 0.5, 0],
+                  [0, 0, 0.5], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    A = fcu.assemble_elasticity_mass_p2_3d(v, np.arange(10).reshape(1, 10), 1.0, ctx)
+    _same(A, O.assemble_elasticity_mass_p2_3d(v, np.arange(10).reshape(1, 10), 1.0))
+    S = A.to_scipy()
+    assert float(np.ones(30) @ (S @ np.ones(30))) == pytest.approx(0.5, abs=1e-14)
+    m = _perturbed_cube(3, 8)
+    verts, c10 = O.p2_node_mesh(m)
+    # the caller's own numbering: permute the nodes
+    perm = np.random.default_rng(9).permutation(len(verts))
+    inv = np.argsort(perm)
+    verts_p, c10_p = verts[perm], inv[c10]
+    _same(fcu.assemble_elasticity_mass_p2_3d(verts_p, c10_p, 7850.0, ctx),
+          O.assemble_elasticity_mass_p2_3d(verts_p, c10_p, 7850.0))
+    # a space on caller nodes refuses what it does not support
+    fm = fcu.Mesh(verts_p, np.ascontiguousarray(c10_p[:, :4]))
+    V = fcu.FunctionSpace(ctx, fm, fcu._abi.FCU_SPACE_P2_NODES, cells10=c10_p)
+    with pytest.raises(fcu.FcuError):
+        V.body_force([0.0, 0.0, 1.0])
+    Ms = fcu.Matrix(ctx, V).assemble_mass(1.0)
+    assert Ms.export_csc().vals.sum() == pytest.approx(1.0, abs=1e-12)   # the cube's volume
+    Ms.close()
+    V.close()
+    bad = c10_p.copy()
+    bad[0, 0] = bad[0, 1]
+    with pytest.raises(fcu.FcuError):
+        fcu.FunctionSpace(ctx, fm, fcu._abi.FCU_SPACE_P2_NODES_VEC3, cells10=bad)
+
+
 def test_add_scaled_scale_and_fold(fcu, ctx):
     m = _perturbed_cube(3, 5)
     fm = fcu.Mesh(m.coords, m.cells)

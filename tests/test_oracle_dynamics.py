@@ -42,6 +42,17 @@ def test_p2_mass_one_tet_conserves_volume():
     assert A[0, 0] == pytest.approx(1.0 / 420.0, abs=1e-13)
 
 
+def test_vector_p2_mass_one_tet():
+    # mass.rs:305-323: the reference element with its ten nodes, density 1:
+    # 1^T M 1 = 3 / 6 (three components), M(0,0) = 1/420
+    v = np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0.5, 0, 0], [0.5, 0.5, 0], [0, 0.5, 0],
+                  [0, 0, 0.5], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    A = O.assemble_elasticity_mass_p2_3d(v, np.arange(10).reshape(1, 10), 1.0).to_scipy()
+    assert A.shape == (30, 30)
+    assert float(np.ones(30) @ (A @ np.ones(30))) == pytest.approx(3.0 / 6.0, abs=1e-13)
+    assert A[0, 0] == pytest.approx(1.0 / 420.0, abs=1e-13)
+
+
 def test_mass_matrices_measure_and_patterns():
     m2 = O.unit_square(5, 3)
     M = O.assemble_mass_2d(m2)
