@@ -346,8 +346,11 @@ __global__ void __launch_bounds__(VBLOCK) k_direction(i64 n, T* __restrict__ p, 
 // padding past their end), and every mbarrier wait is bounded: on expiry the kernel
 // records a fault in the state record and stops.
 
-constexpr int TILE_ROWS = 32;      // block rows per tile (one half-warp each)
-constexpr int TILE_THREADS = 512;  // 16 warps: all 32 rows of a tile at once
+// Block rows per tile: 32 (a half-warp per row) for FP64 values, 64 (8 lanes
+// per row) for FP32, so that a stage carries about the same bytes in both
+// precisions and the consumers' operand gathers for a tile, one L2 round
+// trip, serve twice the rows in FP32. FCU_TILE64=0 keeps 32 rows for FP32.
+constexpr int TILE_THREADS = 512;  // 16 consumer warps: all rows of a tile at once
 constexpr unsigned WAIT_LIMIT = 1u << 24;
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
@@ -396,9 +399,9 @@ struct TileHeader {
 
 __host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
 
-template <class T>
+template <class T, int TR>
 __host__ __device__ size_t tile_stage_bytes(int cap_blocks) {
-  return align128(sizeof(TileHeader)) + align128((TILE_ROWS + 1) * 4 + 16) + align128((size_t)cap_blocks * 4 + 32) +
+  return align128(sizeof(TileHeader)) + align128((TR + 1) * 4 + 16) + align128((size_t)cap_blocks * 4 + 32) +
          align128((size_t)cap_blocks * 9 * sizeof(T) + 32);
 }
 
@@ -432,14 +435,16 @@ struct EmitApOwn {
 // predecessor's tail; the producer warp's lanes fetch the row-pointer bounds
 // of the CTA's next 32 tiles in one round of loads. Returns false, having
 // computed nothing, when the solver state says the solve is over.
-template <bool DIFF, class T, class GX, class Emit>
+template <bool DIFF, class T, int TR, class GX, class Emit>
 __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, const int* __restrict__ ci,
                                                 const T* __restrict__ val, i64 nrows, int cap_blocks, int nstage,
                                                 const GX& gx, Emit& emit, CgState* st) {
   extern __shared__ __align__(128) unsigned char tile_smem[];
   __shared__ unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
-  const size_t stage_bytes = tile_stage_bytes<T>(cap_blocks);
-  const i64 ntiles = (nrows + TILE_ROWS - 1) / TILE_ROWS;
+  constexpr int LPR = 32 * SPMV_CONSUMER_WARPS / TR;  // consumer lanes per block row
+  static_assert(LPR == 8 || LPR == 16, "tile rows");
+  const size_t stage_bytes = tile_stage_bytes<T, TR>(cap_blocks);
+  const i64 ntiles = (nrows + TR - 1) / TR;
   const i64 G = gridDim.x;
   const int mytiles = blockIdx.x < ntiles ? (int)((ntiles - blockIdx.x + G - 1) / G) : 0;
   const int tid = threadIdx.x;
@@ -458,9 +463,9 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
   auto load_desc = [&](int k0) {
     const i64 t = blockIdx.x + (i64)(k0 + lane) * G;
     if (t < ntiles) {
-      const i64 r0 = t * TILE_ROWS;
+      const i64 r0 = t * TR;
       pb0 = rp[r0];
-      pb1 = rp[min(r0 + TILE_ROWS, nrows)];
+      pb1 = rp[min(r0 + TR, nrows)];
     }
   };
   auto issue = [&](int k) {
@@ -470,10 +475,10 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
       unsigned char* base = tile_smem + s * stage_bytes;
       TileHeader* h = reinterpret_cast<TileHeader*>(base);
       unsigned char* rps = base + align128(sizeof(TileHeader));
-      unsigned char* cs = rps + align128((TILE_ROWS + 1) * 4 + 16);
+      unsigned char* cs = rps + align128((TR + 1) * 4 + 16);
       unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
-      const i64 r0 = (blockIdx.x + (i64)k * G) * TILE_ROWS;
-      const int rows = (int)min((i64)TILE_ROWS, nrows - r0);
+      const i64 r0 = (blockIdx.x + (i64)k * G) * TR;
+      const int rows = (int)min((i64)TR, nrows - r0);
       const unsigned rp_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);
       const uintptr_t c_lo = reinterpret_cast<uintptr_t>(ci + b0) & ~(uintptr_t)15;
       const uintptr_t c_hi = (reinterpret_cast<uintptr_t>(ci + b1) + 15) & ~(uintptr_t)15;
@@ -524,10 +529,10 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
     return true;
   }
 
-  // consumers: half-warp per block row; lane `sub` handles blocks sub,
-  // sub + 16, ... of it
-  const int sub = lane & 15;
-  const int row_in_tile = (warp - 1) * 2 + (lane >> 4);
+  // consumers: LPR lanes per block row; lane `sub` handles blocks sub,
+  // sub + LPR, ... of it
+  const int sub = lane % LPR;
+  const int row_in_tile = (warp - 1) * (32 / LPR) + lane / LPR;
   for (int k = 0; k < mytiles; ++k) {
     const int s = k % nstage;
     if (!mbar_wait(&full[s], (unsigned)((k / nstage) & 1))) {
@@ -537,12 +542,12 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
     unsigned char* base = tile_smem + s * stage_bytes;
     const TileHeader* h = reinterpret_cast<const TileHeader*>(base);
     const int* rps = reinterpret_cast<const int*>(base + align128(sizeof(TileHeader)));
-    const unsigned char* cs = base + align128(sizeof(TileHeader)) + align128((TILE_ROWS + 1) * 4 + 16);
+    const unsigned char* cs = base + align128(sizeof(TileHeader)) + align128((TR + 1) * 4 + 16);
     const unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
     const int* cis = reinterpret_cast<const int*>(cs + h->col_off);
     const T* vls = reinterpret_cast<const T*>(vs + h->val_off);
     const int b0 = h->b0;
-    const i64 row = (blockIdx.x + (i64)k * G) * TILE_ROWS + row_in_tile;
+    const i64 row = (blockIdx.x + (i64)k * G) * TR + row_in_tile;
     const bool valid = row_in_tile < h->rows;
     T a0 = T(0), a1 = T(0), a2 = T(0);
     T x0 = T(0), x1 = T(0), x2 = T(0);
@@ -551,7 +556,7 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
       x1 = gx(3 * row + 1);
       x2 = gx(3 * row + 2);
       const int kb1 = rps[row_in_tile + 1] - b0;
-      for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += 16) {
+      for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += LPR) {
         const int c = cis[kb];
         const T* v = vls + 9 * kb;
         const i64 c3 = 3 * (i64)c;
@@ -571,7 +576,7 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
     __syncwarp();
     if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
 #pragma unroll
-    for (int o = 8; o > 0; o >>= 1) {
+    for (int o = LPR / 2; o > 0; o >>= 1) {
       a0 += __shfl_xor_sync(FULL, a0, o);
       a1 += __shfl_xor_sync(FULL, a1, o);
       a2 += __shfl_xor_sync(FULL, a2, o);
@@ -582,14 +587,13 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
   return true;
 }
 
-template <int DIFF, class T>
+template <int DIFF, class T, int TR>
 __global__ void __launch_bounds__(SPMV_THREADS)
-    k_spmv_tiled(const int* __restrict__ rp, const int* __restrict__ ci,
-                                                            const T* __restrict__ val, i64 nrows, int cap_blocks,
-                                                            int nstage, const T* __restrict__ p, T* __restrict__ ap,
-                                                            CgState* st, double* partials) {
+    k_spmv_tiled(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val, i64 nrows,
+                 int cap_blocks, int nstage, const T* __restrict__ p, T* __restrict__ ap, CgState* st,
+                 double* partials) {
   EmitApOwn<T> em{ap};
-  if (!bsr3_tiled_rows<DIFF != 0, T>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, st)) return;
+  if (!bsr3_tiled_rows<DIFF != 0, T, TR>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, st)) return;
   double v[1] = {em.dot}, tot[1];
   if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) {
     if (st->fault) {
@@ -951,16 +955,34 @@ __device__ __forceinline__ void stream_rows(const int* __restrict__ rp, const in
       __syncthreads();
       continue;
     }
-#pragma unroll 4
-    for (int q = t; q < nnz; q += STREAM_THREADS) {
-      const int g = base + q;
-      const T v = val[g];
-      const T xj = x[ci[g]];
-      if (DIFF) {
-        sv[q] = v;
-        sx[q] = xj;
-      } else {
-        sv[q] = v * xj;
+    // all column and value loads of this thread first, then all gathers:
+    // two dependent latencies per block instead of one per entry
+    constexpr int PER = STREAM_NNZ / STREAM_THREADS;
+    int cols[PER];
+    T vs[PER], xs[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int q = t + k * STREAM_THREADS;
+      if (q < nnz) {
+        cols[k] = ci[base + q];
+        vs[k] = val[base + q];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int q = t + k * STREAM_THREADS;
+      if (q < nnz) xs[k] = x[cols[k]];
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int q = t + k * STREAM_THREADS;
+      if (q < nnz) {
+        if (DIFF) {
+          sv[q] = vs[k];
+          sx[q] = xs[k];
+        } else {
+          sv[q] = vs[k] * xs[k];
+        }
       }
     }
     __syncthreads();
@@ -1113,7 +1135,16 @@ int update_block_grid(fcu_ctx ctx, i64 nn) {
   return (int)std::max<i64>(1, std::min<i64>(tiles, (i64)ctx->num_sms * occ));
 }
 
-int stream_grid(fcu_ctx ctx, int nblk) { return std::max(1, std::min(nblk, ctx->num_sms * 6)); }
+// One resident wave of the stream kernel (its CTAs loop over the row blocks).
+template <class K>
+int stream_grid_for(fcu_ctx ctx, int nblk, K kern) {
+  static int occ = -1;
+  if (occ < 0) {
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, STREAM_THREADS, 0));
+    occ = std::max(1, std::min(occ, 8));
+  }
+  return std::max(1, std::min(nblk, ctx->num_sms * occ));
+}
 
 void ensure_row_blocks(fcu_matrix m) {
   if (!m->nrowblk) build_row_blocks(m->ctx, m->row_ptr, m->nnodes, m->rowblk, &m->nrowblk);
@@ -1199,24 +1230,51 @@ void launch_pdl_cfg(fcu_ctx ctx, void (*kern)(KArgs...), int grid, int block, si
   ctx->launches++;
 }
 
-// Tiled 3x3-block SpMV launch: shared memory for two stages sized by the
+bool tile64_enabled() {
+  static int v = [] {
+    const char* e = getenv("FCU_TILE64");
+    return e ? atoi(e) : 1;
+  }();
+  return v != 0;
+}
+
+// Block rows per tile of the tiled SpMV for FP32 (4) or FP64 (8) values.
+int tile_rows(size_t value_bytes) { return (value_bytes == 4 && tile64_enabled()) ? 64 : 32; }
+
+size_t tile_stage_bytes_rt(size_t value_bytes, int tr, int cap) {
+  if (value_bytes == 4) return tr == 64 ? tile_stage_bytes<float, 64>(cap) : tile_stage_bytes<float, 32>(cap);
+  return tile_stage_bytes<double, 32>(cap);
+}
+
+int max_block_row(fcu_matrix m) { return m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32); }
+
+// Ring depth actually used: the requested depth, lowered until
+// TILED_CTAS_PER_SM CTAs fit on an SM (at least two stages).
+int fitted_stages(fcu_ctx ctx, int requested, size_t stage) {
+  static int per_sm_max = 0;
+  if (!per_sm_max)
+    CUDA_CHECK(cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+  int ns = requested;
+  while (ns > 2 && (size_t)TILED_CTAS_PER_SM * (ns * stage + 2048) > (size_t)per_sm_max) --ns;
+  return ns;
+}
+
+// Tiled 3x3-block SpMV launch: shared memory for the ring sized by the
 // longest block row; grid = resident CTAs (persistent), at most one per tile.
-template <int DIFF, class T>
-void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
+template <int DIFF, class T, int TR>
+void launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
   fcu_ctx ctx = m->ctx;
-  const int max_row = m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32);
-  const int cap = TILE_ROWS * max_row;
-  const int nstage = w->stages[sizeof(T) == 4 ? 1 : 0];
-  const size_t smem = nstage * tile_stage_bytes<T>(cap);
-  auto kern = k_spmv_tiled<DIFF, T>;
-  static int configured_dev[2][2] = {{-1, -1}, {-1, -1}};
-  static size_t configured_smem[2][2] = {{0, 0}, {0, 0}};
-  int& cd = configured_dev[DIFF][sizeof(T) == 8];
-  size_t& cs = configured_smem[DIFF][sizeof(T) == 8];
-  if (cd != ctx->device || cs < smem) {
+  const int cap = TR * max_block_row(m);
+  const size_t stage = tile_stage_bytes<T, TR>(cap);
+  const int nstage = fitted_stages(ctx, w->stages[sizeof(T) == 4 ? 1 : 0], stage);
+  const size_t smem = nstage * stage;
+  auto kern = k_spmv_tiled<DIFF, T, TR>;
+  static int configured_dev = -1;
+  static size_t configured_smem = 0;
+  if (configured_dev != ctx->device || configured_smem < smem) {
     CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    cd = ctx->device;
-    cs = smem;
+    configured_dev = ctx->device;
+    configured_smem = smem;
   }
   int per_sm = 0;
   CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SPMV_THREADS, smem));
@@ -1224,11 +1282,17 @@ void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* 
   // The grid sets the order in which p.Ap is reduced, so it does not follow
   // the ring depth: TILED_CTAS_PER_SM CTAs per SM whenever they fit, which
   // keeps the iterates identical for every depth the tuner may pick.
-  const i64 ntiles = (m->nnodes + TILE_ROWS - 1) / TILE_ROWS;
+  const i64 ntiles = (m->nnodes + TR - 1) / TR;
   const int grid =
       (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)std::min(per_sm, TILED_CTAS_PER_SM) * ctx->num_sms));
   launch_pdl_cfg(ctx, kern, grid, SPMV_THREADS, smem, m->row_ptr, m->col_idx, val, m->nnodes, cap, nstage, p, ap,
                  w->st.p, w->partials.p);
+}
+
+template <int DIFF, class T>
+void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
+  if (tile_rows(sizeof(T)) == 64) launch_spmv_tiled_tr<DIFF, T, 64>(m, w, val, p, ap);
+  else launch_spmv_tiled_tr<DIFF, T, 32>(m, w, val, p, ap);
 }
 
 bool use_tiled_spmv() {
@@ -1280,7 +1344,7 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       if (m->bs == 3 && use_tiled_spmv())
         launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
       else if (w->stream[0])
-        launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+        launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<double>), STREAM_THREADS, 0, m->row_ptr,
                        m->col_idx, m->val64.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa64.p, w->ap64.p, w->st.p,
                        w->partials.p);
       else
@@ -1297,7 +1361,7 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       if (m->bs == 3 && use_tiled_spmv())
         launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
       else if (w->stream[1])
-        launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+        launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<float>), STREAM_THREADS, 0, m->row_ptr,
                        m->col_idx, m->val32.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa32.p, w->ap32.p, w->st.p,
                        w->partials.p);
       else
@@ -1509,7 +1573,7 @@ void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev) {
   fcu_ctx ctx = m->ctx;
   if (use_stream_spmv(m)) {
     ensure_row_blocks(m);
-    launch_pdl_cfg(ctx, k_spmv_stream_plain, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr, m->col_idx,
+    launch_pdl_cfg(ctx, k_spmv_stream_plain, stream_grid_for(ctx, m->nrowblk, k_spmv_stream_plain), STREAM_THREADS, 0, m->row_ptr, m->col_idx,
                    m->val64.p, m->rowblk.p, m->nrowblk, x_dev, y_dev);
     return;
   }
@@ -1554,7 +1618,7 @@ void enqueue_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   if (mixed) {
     if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
     else if (w->stream[1])
-      launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+      launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<float>), STREAM_THREADS, 0, m->row_ptr,
                      m->col_idx, m->val32.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa32.p, w->ap32.p, w->st.p,
                      w->partials.p);
     else
@@ -1563,7 +1627,7 @@ void enqueue_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   } else {
     if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
     else if (w->stream[0])
-      launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid(ctx, m->nrowblk), STREAM_THREADS, 0, m->row_ptr,
+      launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<double>), STREAM_THREADS, 0, m->row_ptr,
                      m->col_idx, m->val64.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa64.p, w->ap64.p, w->st.p,
                      w->partials.p);
     else
@@ -1611,9 +1675,9 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   if (m->bs == 3 && use_tiled_spmv()) {
     int optin = 0;
     CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    const int max_row = m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32);
-    const size_t stage = mixed ? tile_stage_bytes<float>(TILE_ROWS * max_row)
-                               : tile_stage_bytes<double>(TILE_ROWS * max_row);
+    const size_t vb = mixed ? 4 : 8;
+    const int tr = tile_rows(vb);
+    const size_t stage = tile_stage_bytes_rt(vb, tr, tr * max_block_row(m));
     int best = w->stages[k];
     double best_ms = 1e30;
     int per_sm_max = 0;
