@@ -556,6 +556,7 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
       x1 = gx(3 * row + 1);
       x2 = gx(3 * row + 2);
       const int kb1 = rps[row_in_tile + 1] - b0;
+#pragma unroll 2
       for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += LPR) {
         const int c = cis[kb];
         const T* v = vls + 9 * kb;
