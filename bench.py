@@ -657,9 +657,10 @@ def run_reference(args, cfg):
     vals = [r["value"] for r in runs]
     v = statistics.median(vals)
     base = runs[0]
+    ndofs = 3 * (cfg["nx"] + 1) * (cfg["ny"] + 1) * (cfg["nz"] + 1)
     return {
         "metric": METRIC, "value": v, "unit": "DOF/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * ndofs / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated box mesh)",
         "config": {"workload": cfg["workload"]}, "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "DOF/s", "cores": base["cores"], "kind": "port",
