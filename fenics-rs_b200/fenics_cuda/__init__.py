@@ -1454,29 +1454,38 @@ def solve_bsr3_pcg_gpu(n_nodes, row_ptr, cols, vals_flat, dinv_flat, b, x0=None,
                           [torch.cuda.get_device_name(ctx.device)])
 
 
-def spmv_bsr3_multi_gpu(n_nodes, row_ptr, cols, vals_flat, x, max_gpus):
-    """spmv_bsr3_multi_gpu (gpu.rs:662-771): contiguous block-row ranges of
-    ceil(n_nodes / g) rows on g = min(max_gpus, visible devices) devices,
-    each product computed on its device, concatenated on the host. Returns
-    (y, device names)."""
-    import torch
-    nd = max(1, min(int(max_gpus), torch.cuda.device_count()))
-    rp = np.asarray(row_ptr, dtype=np.uint32)
+def bsr3_row_split(n_nodes, row_ptr, parts):
+    """The row split of spmv_bsr3_multi_gpu (gpu.rs:662-771): contiguous
+    block-row ranges of ceil(n_nodes / parts) rows. For each non-empty range
+    returns (r0, r1, sub_row_ptr, b0, b1): a row pointer over all n_nodes rows
+    whose rows outside [r0, r1) are empty, and the range's blocks [b0, b1)."""
+    rp = np.asarray(row_ptr, dtype=np.int64)
     n_nodes = int(n_nodes)
-    chunk = (n_nodes + nd - 1) // nd
-    y = np.zeros(3 * n_nodes)
-    names = []
-    for slot in range(nd):
+    chunk = (n_nodes + parts - 1) // parts
+    out = []
+    for slot in range(parts):
         r0, r1 = slot * chunk, min((slot + 1) * chunk, n_nodes)
         if r0 >= r1:
             continue
+        sub = np.concatenate([np.full(r0 + 1, rp[r0]), rp[r0 + 1:r1 + 1], np.full(n_nodes - r1, rp[r1])]) - rp[r0]
+        out.append((r0, r1, sub.astype(np.uint32), int(rp[r0]), int(rp[r1])))
+    return out
+
+
+def spmv_bsr3_multi_gpu(n_nodes, row_ptr, cols, vals_flat, x, max_gpus):
+    """spmv_bsr3_multi_gpu (gpu.rs:662-771): the block rows split into
+    g = min(max_gpus, visible devices) contiguous ranges (bsr3_row_split), each
+    range's product computed on its device, concatenated on the host. Returns
+    (y, device names)."""
+    import torch
+    nd = max(1, min(int(max_gpus), torch.cuda.device_count()))
+    cols = np.asarray(cols, np.uint32)
+    vals_flat = np.asarray(vals_flat, np.float64)
+    y = np.zeros(3 * int(n_nodes))
+    names = []
+    for slot, (r0, r1, sub, b0, b1) in enumerate(bsr3_row_split(n_nodes, row_ptr, nd)):
         ctx = default_context() if slot == 0 else Context(slot)
-        # the rows outside [r0, r1) are empty, so the product has zeros there
-        sub = np.concatenate([np.full(r0 + 1, rp[r0]), rp[r0 + 1:r1 + 1], np.full(n_nodes - r1, rp[r1])])
-        sub = (sub - rp[r0]).astype(np.uint32)
-        b0, b1 = int(rp[r0]), int(rp[r1])
-        M = Matrix.from_bsr3(ctx, n_nodes, sub, np.asarray(cols, np.uint32)[b0:b1],
-                             np.asarray(vals_flat, np.float64)[9 * b0:9 * b1])
+        M = Matrix.from_bsr3(ctx, n_nodes, sub, cols[b0:b1], vals_flat[9 * b0:9 * b1])
         part = M.spmv(x)
         y[3 * r0:3 * r1] = part[3 * r0:3 * r1]
         M.close()

@@ -43,3 +43,24 @@ def test_bsr3_jacobi_smooth_converges_and_zero_start():
     ex = np.linalg.solve(A, r)
     z40 = O.bsr3_jacobi_smooth(nn, rp, ci, va, dinv, r, np.zeros(3 * nn), 40, 1.0, True)
     assert np.linalg.norm(z40 - ex) < 1e-6 * np.linalg.norm(ex)
+
+
+def test_multi_gpu_row_split_reassembles_the_product():
+    # spmv_bsr3_multi_gpu's split (gpu.rs:662-771): each range's rows, computed
+    # with the range's blocks and a row pointer that empties the other rows,
+    # reassemble the full product for 1-4 parts (host logic; no GPU needed)
+    import fenics_cuda as fcu
+    nn, rp, ci, va, _ = synthetic_bsr3(5)
+    x = np.cos(np.arange(3 * nn))
+    full = O.bsr3_spmv(nn, rp, ci, va, x)
+    for parts in (1, 2, 3, 4):
+        y = np.zeros(3 * nn)
+        split = fcu.bsr3_row_split(nn, rp, parts)
+        assert [(a, b) for a, b, *_ in split] == [(i * -(-nn // parts), min((i + 1) * -(-nn // parts), nn))
+                                                 for i in range(parts) if i * -(-nn // parts) < nn]
+        for r0, r1, sub, b0, b1 in split:
+            assert len(sub) == nn + 1 and sub[0] == 0 and sub[-1] == b1 - b0
+            part = O.bsr3_spmv(nn, sub, ci[b0:b1], va[9 * b0:9 * b1], x)
+            assert not part[:3 * r0].any() and not part[3 * r1:].any()
+            y[3 * r0:3 * r1] = part[3 * r0:3 * r1]
+        assert np.array_equal(y, full)
