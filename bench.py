@@ -434,6 +434,9 @@ def run_workloads(ctx, stream, peak):
         c2p[name] = {"ms": ms, "solve_ms": info.kernel_ms, "dof_per_s": V.ndofs / (ms * 1e-3),
                      "iterations": int(info.iterations),
                      "rel_residual": info.rel_residual}
+        sms, sbytes = M.time_spmv(prec, reps=20)
+        c2p[name]["spmv"] = {"ms": sms, "gbs": sbytes / (sms * 1e-3) / 1e9,
+                             "frac_of_hbm": sbytes / (sms * 1e-3) / 1e9 / peak}
     c2p["speedup_mixed_vs_fp64"] = c2p["fp64"]["ms"] / c2p["mixed"]["ms"]
     # stress recovery on the solution (compute_element_stresses / compute_vertex_von_mises)
     cvm = torch.empty(mesh.nc, dtype=torch.float64, device=dev)
