@@ -26,6 +26,22 @@ constexpr int EWARPS = 6;  // warps per block, elasticity assembly (shared-memor
 __host__ __device__ constexpr int odd_stride(int k) { return (k % 2) ? k : k + 1; }
 constexpr unsigned FULL = 0xffffffffu;
 
+// Sum over the warp by an xor butterfly: every lane ends with the same bits
+// (each step adds the same two operands in every lane of a pair).
+__device__ __forceinline__ double warp_sum_xor(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+// The diagonal slot of a row receives one entry from every cell around the
+// row's node (about 24 on a tetrahedral mesh) while the other slots receive
+// a handful, so a lane summing it alone holds the warp back. The warp sums
+// it instead, chunk by chunk in contribution order, by a fixed butterfly
+// over the contributions staged in the chunk (P1 stiffness, elasticity and
+// mass; P2 stiffness rows are dominated by staging ten-entry rows, and the
+// tree measured no faster there).
+
 __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
   int x = v;
 #pragma unroll
@@ -65,8 +81,13 @@ __device__ __forceinline__ void p1_element_row(const double* __restrict__ X, con
       gr[0][r] = -g.G[r][0] - g.G[r][1] - g.G[r][2];
     }
     double s = (1.0 / 6.0) * fabs(g.det) * coef;
+    // row a selected with compile-time indices (a runtime index would put gr in local memory)
+    double ga[3] = {gr[0][0], gr[0][1], gr[0][2]};
 #pragma unroll
-    for (int b = 0; b < 4; ++b) out[b] = (gr[a][0] * gr[b][0] + gr[a][1] * gr[b][1] + gr[a][2] * gr[b][2]) * s;
+    for (int i = 1; i < 4; ++i)
+      if (a == i) ga[0] = gr[i][0], ga[1] = gr[i][1], ga[2] = gr[i][2];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) out[b] = (ga[0] * gr[b][0] + ga[1] * gr[b][1] + ga[2] * gr[b][2]) * s;
   } else {
     Geo2 g = tri_geometry(X, v);
     double gr[3][2];
@@ -77,8 +98,12 @@ __device__ __forceinline__ void p1_element_row(const double* __restrict__ X, con
       gr[0][r] = -g.G[r][0] - g.G[r][1];
     }
     double s = 0.5 * fabs(g.det) * coef;
+    double ga[2] = {gr[0][0], gr[0][1]};
 #pragma unroll
-    for (int b = 0; b < 3; ++b) out[b] = (gr[a][0] * gr[b][0] + gr[a][1] * gr[b][1]) * s;
+    for (int i = 1; i < 3; ++i)
+      if (a == i) ga[0] = gr[i][0], ga[1] = gr[i][1];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) out[b] = (ga[0] * gr[b][0] + ga[1] * gr[b][1]) * s;
   }
 }
 
@@ -124,7 +149,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
     const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
     const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ coef,
-    const double* __restrict__ p2geo, i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
+    const double* __restrict__ p2geo, const int* __restrict__ diag_pos, i64 nrows,
+    double* __restrict__ v64, float* __restrict__ v32) {
   constexpr int KS = odd_stride(K);
   __shared__ double stage_all[WARPS][32][KS];
   __shared__ unsigned short ent_all[WARPS][32 * K];
@@ -142,6 +168,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
     const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
     const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
     const i64 ebase = (i64)K * cs;
+    const int dl = diag_pos[row] - rs;  // slot of the diagonal
     // The row's (contribution, column) entry list, staged once per row with a
     // coalesced copy when it fits (at most 32 contributions).
     const bool staged = nct <= 32;
@@ -157,10 +184,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
       i64 e = ebase + run + off;
       const i64 e1 = e + cnt;
       run += tot;
+      const bool has_diag = !IS_P2 && dl >= g0 && dl < g0 + 32;  // uniform over the warp
+      if (has_diag && s == dl) e = e1;
       double acc = 0.0;
       for (int ch = 0; ch < nct; ch += 32) {
         // stage element rows of contributions ch .. ch+31
         const int t = ch + lane;
+        int a_own = 0;
         if (IS_P2) {
           if (t < nct) {
             int cc = contrib[cs + t];
@@ -187,10 +217,17 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
         } else {
           if (t < nct) {
             int cc = contrib[cs + t];
+            a_own = cc & 15;
             p1_element_row<K, DIM>(X, cn, cc >> 4, cc & 15, coef ? coef[cc >> 4] : 1.0, stage[lane]);
           }
         }
         __syncwarp();
+        if (has_diag) {
+          double d = 0.0;
+          if (t < nct) d = stage[lane][a_own];
+          d = warp_sum_xor(d);
+          if (s == dl) acc += d;
+        }
         while (e < e1) {
           const unsigned ent = staged ? ent_all[wib][e - ebase] : slot_ent[e];
           const int tl = (int)(ent >> 4);
@@ -216,11 +253,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
 // the block once. Staged per contribution: h = s_e g_i (3) and g_0..g_3 (12).
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
+__global__ void __launch_bounds__(EWARPS * 32, 4) k_assemble_elasticity(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
     const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
     const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ cellE, double lam,
-    double mu, i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
+    double mu, const int* __restrict__ diag_pos, i64 nrows, double* __restrict__ v64,
+    float* __restrict__ v32) {
   __shared__ double st_all[EWARPS][32][17];
   __shared__ double out_all[EWARPS][32 * 9];
   __shared__ unsigned short ent_all[EWARPS][32 * 4];
@@ -232,6 +270,7 @@ __global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
     const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
     const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
     const i64 ebase = 4 * (i64)cs;
+    const int dl = diag_pos[row] - rs;
     const bool staged = nct <= 32;
     if (staged)
       for (int q = lane; q < 4 * nct; q += 32) ent_all[wib][q] = slot_ent[ebase + q];
@@ -245,14 +284,18 @@ __global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
       i64 e = ebase + run + off;
       const i64 e1 = e + cnt;
       run += tot;
+      const bool has_diag = dl >= g0 && dl < g0 + 32;  // uniform over the warp
+      if (has_diag && s == dl) e = e1;
       double M[9];
 #pragma unroll
       for (int q = 0; q < 9; ++q) M[q] = 0.0;
       for (int ch = 0; ch < nct; ch += 32) {
         const int t = ch + lane;
+        int a_own = 0;
         if (t < nct) {
           const int cc = contrib[cs + t];
           const int c = cc >> 4, a = cc & 15;
+          a_own = a;
           int v[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) v[i] = cn[4 * (i64)c + i];
@@ -271,6 +314,25 @@ __global__ void __launch_bounds__(EWARPS * 32) k_assemble_elasticity(
           for (int r = 0; r < 3; ++r) w[r] = sc * w[3 + 3 * a + r];
         }
         __syncwarp();
+        if (has_diag) {
+          // a contribution's diagonal block is (sc g)(g^T) with g the gradient of its own
+          // basis function: symmetric, so six sums cover it
+          const double* w = st[lane];
+          const double* g = w + 3 + 3 * a_own;
+          const bool live = t < nct;
+          const double d00 = warp_sum_xor(live ? w[0] * g[0] : 0.0);
+          const double d11 = warp_sum_xor(live ? w[1] * g[1] : 0.0);
+          const double d22 = warp_sum_xor(live ? w[2] * g[2] : 0.0);
+          const double d01 = warp_sum_xor(live ? w[0] * g[1] : 0.0);
+          const double d02 = warp_sum_xor(live ? w[0] * g[2] : 0.0);
+          const double d12 = warp_sum_xor(live ? w[1] * g[2] : 0.0);
+          if (s == dl) {
+            M[0] += d00; M[4] += d11; M[8] += d22;
+            M[1] += d01; M[3] += d01;
+            M[2] += d02; M[6] += d02;
+            M[5] += d12; M[7] += d12;
+          }
+        }
         while (e < e1) {
           const unsigned ent = staged ? ent_all[wib][e - ebase] : slot_ent[e];
           const int tl = (int)(ent >> 4);
@@ -328,7 +390,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
     const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
     const int* __restrict__ cn, const double* __restrict__ X, const double* __restrict__ coef, double rho,
-    const MassTable tab, i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
+    const MassTable tab, const int* __restrict__ diag_pos, i64 nrows, double* __restrict__ v64,
+    float* __restrict__ v32) {
   __shared__ double s_all[WARPS][32];
   __shared__ int a_all[WARPS][32];
   __shared__ unsigned short ent_all[WARPS][32 * K];
@@ -338,6 +401,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
     const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
     const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
     const i64 ebase = (i64)K * cs;
+    const int dl = diag_pos[row] - rs;
     const bool staged = nct <= 32;
     if (staged)
       for (int q = lane; q < K * nct; q += 32) ent_all[wib][q] = slot_ent[ebase + q];
@@ -351,6 +415,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
       i64 e = ebase + run + off;
       const i64 e1 = e + cnt;
       run += tot;
+      const bool has_diag = dl >= g0 && dl < g0 + 32;  // uniform over the warp
+      if (has_diag && s == dl) e = e1;
       double acc = 0.0;
       for (int ch = 0; ch < nct; ch += 32) {
         const int t = ch + lane;
@@ -368,6 +434,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
           a_all[wib][lane] = cc & 15;
         }
         __syncwarp();
+        if (has_diag) {
+          const int a = a_all[wib][lane];
+          const double d = warp_sum_xor(t < nct ? __dmul_rn(s_all[wib][lane], tab.F[a * K + a]) : 0.0);
+          if (s == dl) acc = __dadd_rn(acc, d);
+        }
         while (e < e1) {
           const unsigned ent = staged ? ent_all[wib][e - ebase] : slot_ent[e];
           const int tl = (int)(ent >> 4);
@@ -634,15 +705,15 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
     LAUNCH_CHECK(ctx);
     k_assemble_scalar<10, 3, true><<<nb, WARPS * 32, 0, ctx->stream>>>(
         s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
-        coef_dev, geo.p, s->nnodes, m->val64.p, m->val32.p);
+        coef_dev, geo.p, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   } else if (me->dim == 3) {
     k_assemble_scalar<4, 3, false><<<nb, WARPS * 32, 0, ctx->stream>>>(
         s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
-        coef_dev, nullptr, s->nnodes, m->val64.p, m->val32.p);
+        coef_dev, nullptr, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   } else {
     k_assemble_scalar<3, 2, false><<<nb, WARPS * 32, 0, ctx->stream>>>(
         s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
-        coef_dev, nullptr, s->nnodes, m->val64.p, m->val32.p);
+        coef_dev, nullptr, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   }
   LAUNCH_CHECK(ctx);
 }
@@ -657,7 +728,7 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
   const int nb = assembly_blocks(ctx, s->nnodes, EWARPS);
   k_assemble_elasticity<<<nb, EWARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                             s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p,
-                                                            s->mesh->coords.p, cellE_dev, lam, mu, s->nnodes,
+                                                            s->mesh->coords.p, cellE_dev, lam, mu, s->diag_pos.p, s->nnodes,
                                                             m->val64.p, m->val32.p);
   LAUNCH_CHECK(ctx);
 }
@@ -682,23 +753,23 @@ void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev) {
   if (s->kind == FCU_SPACE_P2_NODES_VEC3) {
     k_assemble_mass<10, 3, 3><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                    s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
-                                                                   tab, s->nnodes, m->val64.p, m->val32.p);
+                                                                   tab, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   } else if (p2) {
     k_assemble_mass<10, 3, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                    s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
-                                                                   tab, s->nnodes, m->val64.p, m->val32.p);
+                                                                   tab, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   } else if (s->kind == FCU_SPACE_P1_VEC3) {
     k_assemble_mass<4, 3, 3><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                   s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
-                                                                  tab, s->nnodes, m->val64.p, m->val32.p);
+                                                                  tab, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   } else if (me->dim == 3) {
     k_assemble_mass<4, 3, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                   s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
-                                                                  tab, s->nnodes, m->val64.p, m->val32.p);
+                                                                  tab, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   } else {
     k_assemble_mass<3, 2, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                   s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
-                                                                  tab, s->nnodes, m->val64.p, m->val32.p);
+                                                                  tab, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
   }
   LAUNCH_CHECK(ctx);
 }
