@@ -674,12 +674,13 @@ def run_reference(args, cfg):
     }
 
 
-PROFILE_CASES = ("mass_c2", "block_update_c2", "transient_1024")
+PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024")
 
 
 def profile_case(name):
     """A short run of one kernel on one workload, for profiler captures: no
     timing, a few launches, a few hundred MB on the device.
+      elasticity_c2    elasticity stiffness of the C2 mesh, assembled 3 times
       mass_c2          vector-P1 mass of the C2 mesh, assembled 3 times
       block_update_c2  12 block-Jacobi FP64 PCG iterations on the C2 system
       transient_1024   3 Crank-Nicolson steps of the 1024^2 heat problem,
@@ -687,13 +688,16 @@ def profile_case(name):
     import torch
     import fenics_cuda as fcu
     ctx = fcu.Context(0)
-    if name in ("mass_c2", "block_update_c2"):
+    if name in ("elasticity_c2", "mass_c2", "block_update_c2"):
         mesh = fcu.box_beam(4.0, 1.0, 1.0, 128, 32, 32)
         V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
-        if name == "mass_c2":
+        if name in ("elasticity_c2", "mass_c2"):
             M = fcu.Matrix(ctx, V)
             for _ in range(3):
-                M.assemble_mass(7850.0)
+                if name == "mass_c2":
+                    M.assemble_mass(7850.0)
+                else:
+                    M.assemble_elasticity(210e9, 0.3)
         else:
             M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
             cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
