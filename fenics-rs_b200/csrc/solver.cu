@@ -16,20 +16,22 @@
 // errors act on the smooth (bending) modes with a relative size of about
 // eps32 * cond(A).
 //
-// Each iteration is two kernels, one per global reduction of PCG:
-//   spmv     p = z + beta p_old (own rows written, neighbours recomputed on
-//            the fly), Ap = A p, p.Ap reduced on the device -> alpha
-//   update   x += alpha p, r -= alpha Ap, z = D^-1 r written, r.z and r.r ->
-//            beta, convergence / iteration-limit decision
-// plus, in mixed precision, the replacement kernel, which returns at once
-// unless the update kernel asked for it. p is double-buffered across
-// iterations. Every reduction ends in the block that finishes last, which sums
+// Each iteration is three kernels, two of them ending in a global reduction:
+//   direction  p = z + beta p
+//   spmv       Ap = A p, p.Ap reduced on the device -> alpha
+//   update     x += alpha p, r -= alpha Ap, z = D^-1 r written, r.z and r.r ->
+//              beta, convergence / iteration-limit decision
+// (FCU_FUSE_DIRECTION=1 selects a two-kernel form in which the SpMV forms
+// p = z + beta p_old on the fly, p double-buffered; it measured slower.) In
+// mixed precision each replay of the graph starts with the replacement
+// kernel, which returns at once unless an iteration of the previous replay
+// asked for it. Every reduction ends in the block that finishes last, which sums
 // the per-block partials in a fixed order (deterministic) and writes
 // alpha / beta / flags to a small device state record. The loop is captured
 // once per matrix as a CUDA graph of CHUNK iterations, launched with
 // programmatic dependent launch so each kernel is scheduled while its
-// predecessor drains; kernels of a finished solve return at once, and the host
-// polls the state once per chunk.
+// predecessor drains; kernels of a finished solve return at once. The host
+// reads the state once per replay while the next replay is already queued.
 
 #include <algorithm>
 #include <atomic>
@@ -1062,7 +1064,8 @@ struct Workspace {
   DBuf<double> z64, pa64, pb64, ap64;  // FP64 path: z, p (two buffers), Ap
   DBuf<float> z32, pa32, pb32, ap32;   // mixed path
   DBuf<CgState> st;
-  CgState* host_st = nullptr;
+  CgState* host_st = nullptr;  // two pinned records: [0] set-up and final state, [0]/[1] alternate between replays
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // a replay's state record has arrived on the host
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool stream[2] = {false, false};  // scalar PCG SpMV: CSR-stream kernel (FP64, FP32)
   int vpr = 0;    // lanes per row of the FP64 CSR kernels (tuned with the FP64 SpMV)
@@ -1074,6 +1077,8 @@ struct Workspace {
   ~Workspace() {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
     if (host_st) cudaFreeHost(host_st);
   }
 };
@@ -1171,7 +1176,8 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     w->partials.alloc(3 * MAXG);
     w->st.alloc(1);
     CUDA_CHECK(cudaMemsetAsync(w->st.p, 0, sizeof(CgState), ctx->stream));
-    CUDA_CHECK(cudaMallocHost(&w->host_st, sizeof(CgState)));
+    CUDA_CHECK(cudaMallocHost(&w->host_st, 2 * sizeof(CgState)));
+    for (auto& e : w->ev) CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     w->vpr = pick_vpr(m);
     w->vpr32 = w->vpr;
     if (m->bs == 1 && use_stream_spmv(m)) {
@@ -1392,6 +1398,9 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
 
 int launches_per_iteration() { return fuse_direction() ? 2 : 3; }
 
+// Kernels in one replay of the iteration graph.
+int launches_per_replay(bool mixed) { return CHUNK * launches_per_iteration() + (mixed ? 1 : 0); }
+
 cudaGraphExec_t get_graph(fcu_matrix m, Workspace* w, bool mixed) {
   fcu_ctx ctx = m->ctx;
   cudaGraphExec_t& ge = w->graph[mixed ? 1 : 0];
@@ -1400,6 +1409,11 @@ cudaGraphExec_t get_graph(fcu_matrix m, Workspace* w, bool mixed) {
   const i64 launches0 = ctx->launches;
   CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   try {
+    // mixed: the residual replacement that an iteration of the previous
+    // replay asked for (r = b - A64 x); it returns at once otherwise
+    if (mixed)
+      DISPATCH_ROWS(m->bs, w->vpr, w->grid, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->x.p, w->b.p,
+                    w->invd.p, w->r.p, w->z32.p, w->st.p, w->partials.p);
     for (int it = 0; it < CHUNK; ++it) enqueue_iteration(m, w, mixed, it & 1);
   } catch (...) {
     cudaStreamEndCapture(ctx->stream, &g);
@@ -1515,26 +1529,41 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
     w->host_st->status = FCU_OK;
     w->host_st->iter = 0;
   } else if (!w->host_st->done && max_iter > 0) {
-    // Replays of CHUNK iterations. In the mixed solve an iteration that
-    // flags a residual replacement pauses the rest of its replay, and the
-    // replacement runs here before the next replay, right after that
-    // iteration. Every replay completes at least one iteration, and the
-    // iteration limit is enforced on the device, so the loop ends.
+    // Replays of CHUNK iterations, each followed by a copy of the state
+    // record to the host. The host keeps one replay queued beyond the one
+    // whose state it is reading, so the GPU does not wait for the host
+    // between replays. In the mixed solve an iteration that flags a residual
+    // replacement pauses the rest of its replay, and the next replay's first
+    // kernel performs the replacement, right after that iteration. Kernels of
+    // a replay queued after the solve ended return at once and change
+    // nothing. Every replay but the first completes at least one iteration
+    // and the iteration limit is enforced on the device, so max_iter + 2
+    // replays always suffice.
     cudaGraphExec_t ge = get_graph(m, w, mixed);
-    for (i64 rep = 0; rep <= max_iter + 1; ++rep) {
+    CgState* hs = w->host_st;
+    auto issue = [&](int slot) {
       CUDA_CHECK(cudaGraphLaunch(ge, ctx->stream));
-      ctx->launches += (i64)CHUNK * launches_per_iteration();
-      CUDA_CHECK(cudaMemcpyAsync(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
-      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-      if (w->host_st->done) break;
-      if (mixed && w->host_st->do_update) {
-        DISPATCH_ROWS(m->bs, w->vpr, g, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, nr, w->x.p, w->b.p, w->invd.p,
-                      w->r.p, w->z32.p, w->st.p, w->partials.p);
-        CUDA_CHECK(cudaMemcpyAsync(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
-        CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-        if (w->host_st->done) break;
+      ctx->launches += launches_per_replay(mixed);
+      CUDA_CHECK(cudaMemcpyAsync(&hs[slot], w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaEventRecord(w->ev[slot], ctx->stream));
+    };
+    const i64 max_replays = max_iter + 2;
+    int slot = 0;
+    issue(0);
+    i64 issued = 1;
+    for (;;) {
+      const bool more = issued < max_replays;
+      if (more) {
+        issue(slot ^ 1);
+        ++issued;
       }
+      CUDA_CHECK(cudaEventSynchronize(w->ev[slot]));
+      if (hs[slot].done || !more) break;
+      slot ^= 1;
     }
+    // the final state, after any replay still queued
+    CUDA_CHECK(cudaMemcpyAsync(&hs[0], w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
   } else if (!w->host_st->done) {
     w->host_st->status = gpu_semantics ? FCU_OK : FCU_ERR_NO_CONVERGENCE;
   }
