@@ -25,9 +25,12 @@
 // p = z + beta p_old on the fly, p double-buffered; it measured slower.) In
 // mixed precision each replay of the graph starts with the replacement
 // kernel, which returns at once unless an iteration of the previous replay
-// asked for it. Every reduction ends in the block that finishes last, which sums
-// the per-block partials in a fixed order (deterministic) and writes
-// alpha / beta / flags to a small device state record. The loop is captured
+// asked for it. The SpMV only stores per-block p.Ap partials; every block
+// of the update kernel adds them in the same fixed order and forms alpha
+// itself. The update's own reduction (r.z, r.r) ends in the block that
+// finishes last, which sums the per-block partials in a fixed order and
+// writes beta and the flags to a small device state record. Both orders are
+// fixed, so a solve repeats bit for bit. The loop is captured
 // once per matrix as a CUDA graph of CHUNK iterations, launched with
 // programmatic dependent launch so each kernel is scheduled while its
 // predecessor drains; kernels of a finished solve return at once. The host
@@ -49,6 +52,11 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int VBLOCK = 256;  // threads per block in solver kernels
 constexpr int MAXG = 4096;   // max blocks of a reducing kernel (partials capacity)
+// Regions of the partials buffer (MAXG doubles each): 0-2 for grid_reduce,
+// 3 for the SpMV's per-block p.Ap, which the update kernel reads while it
+// writes its own partials into regions 0-1.
+constexpr int PAP_REGION = 3;
+constexpr int PARTIAL_REGIONS = 4;
 constexpr int CHUNK = 16;    // iterations per graph launch (even: p double buffer)
 
 struct CgState {
@@ -254,17 +262,73 @@ __device__ __forceinline__ void spmv_rows(const int* __restrict__ rp, const int*
   }
 }
 
-// cg.rs:102-107: |p.Ap| < 1e-30 is a breakdown (Err). The GPU solvers
-// (gpu.rs:1326-1329, 1034-1037) stop with Ok when p.Ap <= 1e-30; the
-// iteration counts as done.
-__device__ __forceinline__ void set_alpha(CgState* st, double pap) {
-  if (!st->timing && (st->gpu_semantics ? !(pap > 1e-30) : fabs(pap) < 1e-30)) {
-    st->done = 1;
-    st->status = st->gpu_semantics ? FCU_OK : FCU_ERR_BREAKDOWN;
-    st->iter += 1;
-  } else {
-    st->alpha = st->rz / pap;
+// The SpMV's p.Ap: each block stores its sum (fixed order) in the PAP_REGION
+// of the partials; no grid-wide step follows in the SpMV itself.
+__device__ __forceinline__ void store_pap_partial(double dot, double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = (int)(blockDim.x >> 5);
+  const double x = warp_sum(dot);
+  if (lane == 0) sh[w] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < nw; ++q) t += sh[q];
+    partials[PAP_REGION * MAXG + blockIdx.x] = t;
   }
+}
+
+// The update kernel's alpha = r.z / p.Ap. Every block adds the SpMV's np
+// per-block partials in the same fixed order (so all blocks hold the same
+// alpha, and it is the same in every run), which takes the SpMV's grid-wide
+// reduction off the critical path. cg.rs:102-107: |p.Ap| < 1e-30 is a
+// breakdown (Err); the GPU solvers (gpu.rs:1326-1329, 1034-1037) stop with Ok
+// when p.Ap <= 1e-30, the iteration counting as done. A bulk-copy fault of the
+// tiled SpMV ends the solve with FCU_ERR_CUDA. Returns false when the solve
+// ends here; block 0 records it. Called by all threads of the block.
+__device__ __forceinline__ bool take_alpha(CgState* st, const double* __restrict__ partials, int np,
+                                           double* alpha) {
+  __shared__ double sh[32];
+  __shared__ double pap_s;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = (int)(blockDim.x >> 5);
+  double s = 0.0;
+  for (int b = threadIdx.x; b < np; b += blockDim.x) s += __ldcg(&partials[PAP_REGION * MAXG + b]);
+  s = warp_sum(s);
+  if (lane == 0) sh[w] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < nw; ++q) t += sh[q];
+    pap_s = t;
+  }
+  __syncthreads();
+  const double pap = pap_s;
+  const bool fault = st->fault != 0;
+  const bool brk = !st->timing && (st->gpu_semantics ? !(pap > 1e-30) : fabs(pap) < 1e-30);
+  if (fault || brk) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->done = 1;
+      if (fault) {
+        st->status = FCU_ERR_CUDA;
+      } else {
+        st->status = st->gpu_semantics ? FCU_OK : FCU_ERR_BREAKDOWN;
+        st->iter += 1;
+      }
+    }
+    return false;
+  }
+  *alpha = st->rz / pap;
+  return true;
+}
+
+// Reads the stop flags once per block (block 0 of the update kernel may set
+// `done` while other blocks start), so that the block's threads agree.
+__device__ __forceinline__ bool block_stopped(const CgState* st) {
+  __shared__ int stop;
+  if (threadIdx.x == 0) stop = (st->done || st->pause) ? 1 : 0;
+  __syncthreads();
+  return stop != 0;
 }
 
 // --- spmv: p = z + beta p_old ; Ap = A p ; p.Ap -> alpha -----------------------
@@ -296,8 +360,7 @@ __global__ void __launch_bounds__(VBLOCK) k_spmv_dir(const int* __restrict__ rp,
   EmitAp<BS, T> em{dir, pnew, ap};
   constexpr bool DIFF = sizeof(T) == 4;
   spmv_rows<BS, VPR, DIFF, T>(rp, ci, val, nrows, dir, em);
-  double v[1] = {em.dot}, tot[1];
-  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) set_alpha(st, tot[0]);
+  store_pap_partial(em.dot, partials);
 }
 
 // Unfused variant: p already updated by k_direction; Ap = A p.
@@ -322,8 +385,7 @@ __global__ void __launch_bounds__(VBLOCK) k_spmv_ap(const int* __restrict__ rp, 
   EmitApPlain<BS, T> em{p, ap};
   constexpr bool DIFF = sizeof(T) == 4;
   spmv_rows<BS, VPR, DIFF, T>(rp, ci, val, nrows, XPlain<T>{p}, em);
-  double v[1] = {em.dot}, tot[1];
-  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) set_alpha(st, tot[0]);
+  store_pap_partial(em.dot, partials);
 }
 
 // p = z + beta p (in place), for the unfused iteration.
@@ -597,15 +659,7 @@ __global__ void __launch_bounds__(SPMV_THREADS)
                  double* partials) {
   EmitApOwn<T> em{ap};
   if (!bsr3_tiled_rows<DIFF != 0, T, TR>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, st)) return;
-  double v[1] = {em.dot}, tot[1];
-  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) {
-    if (st->fault) {
-      st->done = 1;
-      st->status = FCU_ERR_CUDA;
-    } else {
-      set_alpha(st, tot[0]);
-    }
-  }
+  store_pap_partial(em.dot, partials);
 }
 
 // --- update -----------------------------------------------------------------
@@ -631,7 +685,7 @@ template <class T>
 __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x, double* __restrict__ r,
                                                    const T* __restrict__ p, const T* __restrict__ ap,
                                                    const double* __restrict__ invd, T* __restrict__ z, CgState* st,
-                                                   double* partials) {
+                                                   double* partials, int npap) {
   // x, r, D^-1 and p are final before this kernel starts (their writers
   // completed before the SpMV it depends on began), so the first two
   // elements of each thread are fetched before the dependency wait; L2-only
@@ -651,8 +705,9 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
     }
   }
   grid_dep_sync();
-  if (st->done || st->pause) return;
-  const double alpha = st->alpha;
+  if (block_stopped(st)) return;
+  double alpha;
+  if (!take_alpha(st, partials, npap, &alpha)) return;
   double rz = 0.0, rr = 0.0;
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
@@ -714,7 +769,8 @@ __global__ void __launch_bounds__(UB_THREADS) k_update_block(i64 nn, double* __r
                                                              const double* __restrict__ p,
                                                              const double* __restrict__ ap,
                                                              const double* __restrict__ bdinv,
-                                                             double* __restrict__ z, CgState* st, double* partials) {
+                                                             double* __restrict__ z, CgState* st, double* partials,
+                                                             int npap) {
   __shared__ double rs[UB_THREADS];
   const i64 n = 3 * nn;
   const int t = threadIdx.x;
@@ -730,8 +786,9 @@ __global__ void __launch_bounds__(UB_THREADS) k_update_block(i64 nn, double* __r
     d2 = __ldcg(bdinv + 3 * i + 2);
   }
   grid_dep_sync();
-  if (st->done || st->pause) return;
-  const double alpha = st->alpha;
+  if (block_stopped(st)) return;
+  double alpha;
+  if (!take_alpha(st, partials, npap, &alpha)) return;
   double rz = 0.0, rr = 0.0;
   const i64 first = blockIdx.x * (i64)UB_THREADS;
   for (i64 tile = first; tile < n; tile += tstride, i += tstride) {
@@ -1016,8 +1073,7 @@ __global__ void __launch_bounds__(STREAM_THREADS) k_spmv_stream(const int* __res
   if (st->done || st->pause) return;
   EmitApPlain<1, T> em{p, ap};
   stream_rows<sizeof(T) == 4, T>(rp, ci, val, dpos, rb, nblk, p, em);
-  double v[1] = {em.dot}, tot[1];
-  if (grid_reduce<1>(v, partials, st->ticket[0], tot) && threadIdx.x == 0) set_alpha(st, tot[0]);
+  store_pap_partial(em.dot, partials);
 }
 
 __global__ void __launch_bounds__(STREAM_THREADS) k_spmv_stream_plain(const int* __restrict__ rp,
@@ -1173,7 +1229,7 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     w->n = m->n;
     const i64 n = m->n;
     w->x.alloc(n); w->r.alloc(n); w->b.alloc(n); w->invd.alloc(n);
-    w->partials.alloc(3 * MAXG);
+    w->partials.alloc(PARTIAL_REGIONS * MAXG);
     w->st.alloc(1);
     CUDA_CHECK(cudaMemsetAsync(w->st.p, 0, sizeof(CgState), ctx->stream));
     CUDA_CHECK(cudaMallocHost(&w->host_st, 2 * sizeof(CgState)));
@@ -1269,7 +1325,7 @@ int fitted_stages(fcu_ctx ctx, int requested, size_t stage) {
 // Tiled 3x3-block SpMV launch: shared memory for the ring sized by the
 // longest block row; grid = resident CTAs (persistent), at most one per tile.
 template <int DIFF, class T, int TR>
-void launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
+int launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
   fcu_ctx ctx = m->ctx;
   const int cap = TR * max_block_row(m);
   const size_t stage = tile_stage_bytes<T, TR>(cap);
@@ -1294,12 +1350,14 @@ void launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, 
       (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)std::min(per_sm, TILED_CTAS_PER_SM) * ctx->num_sms));
   launch_pdl_cfg(ctx, kern, grid, SPMV_THREADS, smem, m->row_ptr, m->col_idx, val, m->nnodes, cap, nstage, p, ap,
                  w->st.p, w->partials.p);
+  return grid;
 }
 
+// Returns the grid (the number of p.Ap partials the update kernel adds).
 template <int DIFF, class T>
-void launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
-  if (tile_rows(sizeof(T)) == 64) launch_spmv_tiled_tr<DIFF, T, 64>(m, w, val, p, ap);
-  else launch_spmv_tiled_tr<DIFF, T, 32>(m, w, val, p, ap);
+int launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
+  if (tile_rows(sizeof(T)) == 64) return launch_spmv_tiled_tr<DIFF, T, 64>(m, w, val, p, ap);
+  return launch_spmv_tiled_tr<DIFF, T, 32>(m, w, val, p, ap);
 }
 
 bool use_tiled_spmv() {
@@ -1348,34 +1406,38 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
     // direction (p = z + beta p, in place on buffer a) then SpMV
     if (!mixed) {
       launch_pdl(ctx, k_direction<double>, w->vgrid, n, w->pa64.p, w->z64.p, w->st.p);
-      if (m->bs == 3 && use_tiled_spmv())
-        launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
-      else if (w->stream[0])
-        launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<double>), STREAM_THREADS, 0, m->row_ptr,
-                       m->col_idx, m->val64.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa64.p, w->ap64.p, w->st.p,
-                       w->partials.p);
-      else
+      int npap = g;
+      if (m->bs == 3 && use_tiled_spmv()) {
+        npap = launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+      } else if (w->stream[0]) {
+        npap = stream_grid_for(ctx, m->nrowblk, k_spmv_stream<double>);
+        launch_pdl_cfg(ctx, k_spmv_stream<double>, npap, STREAM_THREADS, 0, m->row_ptr, m->col_idx, m->val64.p,
+                       m->diag_pos, m->rowblk.p, m->nrowblk, w->pa64.p, w->ap64.p, w->st.p, w->partials.p);
+      } else {
         DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_AP64, m->row_ptr, m->col_idx, m->val64.p, nr, w->pa64.p, w->ap64.p,
                       w->st.p, w->partials.p);
+      }
       if (m->bdinv.p)
         launch_pdl_cfg(ctx, k_update_block, update_block_grid(ctx, m->nnodes), UB_THREADS, 0, m->nnodes, w->x.p,
-                       w->r.p, w->pa64.p, w->ap64.p, m->bdinv.p, w->z64.p, w->st.p, w->partials.p);
+                       w->r.p, w->pa64.p, w->ap64.p, m->bdinv.p, w->z64.p, w->st.p, w->partials.p, npap);
       else
         launch_pdl(ctx, k_update<double>, w->vgrid, n, w->x.p, w->r.p, w->pa64.p, w->ap64.p, w->invd.p, w->z64.p,
-                   w->st.p, w->partials.p);
+                   w->st.p, w->partials.p, npap);
     } else {
       launch_pdl(ctx, k_direction<float>, w->vgrid, n, w->pa32.p, w->z32.p, w->st.p);
-      if (m->bs == 3 && use_tiled_spmv())
-        launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
-      else if (w->stream[1])
-        launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<float>), STREAM_THREADS, 0, m->row_ptr,
-                       m->col_idx, m->val32.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa32.p, w->ap32.p, w->st.p,
-                       w->partials.p);
-      else
+      int npap = g;
+      if (m->bs == 3 && use_tiled_spmv()) {
+        npap = launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+      } else if (w->stream[1]) {
+        npap = stream_grid_for(ctx, m->nrowblk, k_spmv_stream<float>);
+        launch_pdl_cfg(ctx, k_spmv_stream<float>, npap, STREAM_THREADS, 0, m->row_ptr, m->col_idx, m->val32.p,
+                       m->diag_pos, m->rowblk.p, m->nrowblk, w->pa32.p, w->ap32.p, w->st.p, w->partials.p);
+      } else {
         DISPATCH_ROWS(m->bs, w->vpr32, g, K_SPMV_AP32, m->row_ptr, m->col_idx, m->val32.p, nr, w->pa32.p, w->ap32.p,
                       w->st.p, w->partials.p);
+      }
       launch_pdl(ctx, k_update<float>, w->vgrid, n, w->x.p, w->r.p, w->pa32.p, w->ap32.p, w->invd.p, w->z32.p,
-                 w->st.p, w->partials.p);
+                 w->st.p, w->partials.p, npap);
     }
     return;
   }
@@ -1385,14 +1447,14 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
     DISPATCH_ROWS(m->bs, w->vpr, g, K_SPMV_DIR64, m->row_ptr, m->col_idx, m->val64.p, nr, w->z64.p, pold, pnew,
                   w->ap64.p, w->st.p, w->partials.p);
     launch_pdl(ctx, k_update<double>, g, n, w->x.p, w->r.p, pnew, w->ap64.p, w->invd.p, w->z64.p, w->st.p,
-               w->partials.p);
+               w->partials.p, g);
   } else {
     float* pold = parity ? w->pb32.p : w->pa32.p;
     float* pnew = parity ? w->pa32.p : w->pb32.p;
     DISPATCH_ROWS(m->bs, w->vpr32, g, K_SPMV_DIR32, m->row_ptr, m->col_idx, m->val32.p, nr, w->z32.p, pold, pnew,
                   w->ap32.p, w->st.p, w->partials.p);
     launch_pdl(ctx, k_update<float>, g, n, w->x.p, w->r.p, pnew, w->ap32.p, w->invd.p, w->z32.p, w->st.p,
-               w->partials.p);
+               w->partials.p, g);
   }
 }
 
@@ -1811,7 +1873,7 @@ struct NoAllocHeader {
 static_assert(sizeof(NoAllocHeader) <= 1024, "header region");
 
 constexpr size_t NA_HEADER_WORDS = 1024 / sizeof(double);
-constexpr size_t NA_PARTIAL_WORDS = 3 * MAXG;
+constexpr size_t NA_PARTIAL_WORDS = PARTIAL_REGIONS * MAXG;
 constexpr size_t NA_VEC_WORDS = (size_t)NOALLOC_MAX_N;
 constexpr size_t NA_WORDS = NA_HEADER_WORDS + NA_PARTIAL_WORDS + 4 * NA_VEC_WORDS;
 
@@ -1871,7 +1933,7 @@ void noalloc_chunk(cudaStream_t s, int g, int vg, const int* rp, const int* ci, 
   for (int it = 0; it < CHUNK; ++it) {
     k_direction<double><<<vg, VBLOCK, 0, s>>>(n, p, z, st);
     k_spmv_ap<1, VPR, double><<<g, VBLOCK, 0, s>>>(rp, ci, val, n, p, ap, st, partials);
-    k_update<double><<<vg, VBLOCK, 0, s>>>(n, x, r, p, ap, invd, z, st, partials);
+    k_update<double><<<vg, VBLOCK, 0, s>>>(n, x, r, p, ap, invd, z, st, partials, g);
   }
   CUDA_CHECK(cudaGetLastError());
 }
