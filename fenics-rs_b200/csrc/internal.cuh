@@ -4,8 +4,10 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -98,6 +100,10 @@ struct fcu_ctx_s {
   i64 launches = 0;          // kernels launched by this library on this context
   DBuf<unsigned char> temp;  // reusable scratch (CUB temporary storage)
   int num_sms = 148;
+  // SpMV shapes the PCG tuner picked, by matrix shape (block size, rows,
+  // stored blocks, longest row, precision): a later matrix of the same shape
+  // (a new solve on the same mesh) takes them without timing candidates.
+  std::map<std::array<i64, 5>, std::array<int, 2>> spmv_tune;
   unsigned char* temp_bytes(size_t b) {
     if (temp.n < b) temp.alloc(b);
     return temp.p;

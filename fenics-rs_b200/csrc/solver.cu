@@ -1678,8 +1678,9 @@ void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev) {
 // The first solve of a matrix in a precision times the candidate shapes of
 // its SpMV on the matrix itself and keeps the fastest: lanes per row
 // {4, 8, 16, 32} for CSR, ring depth {2, 3, 4} for the tiled 3x3-block
-// kernel. FCU_TUNE=0 keeps the defaults (CSR lanes by mean row length,
-// three stages).
+// kernel. The choice is kept in the context by matrix shape, so a later
+// matrix of the same shape takes it without timing. FCU_TUNE=0 keeps the
+// defaults (CSR lanes by mean row length, three stages).
 
 // Solver state and operand for SpMV timing: every launch does the full
 // product (no convergence or breakdown exit).
@@ -1759,12 +1760,24 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   w->tuned[k] = true;
   if (!tuning_enabled()) return;
   fcu_ctx ctx = m->ctx;
+  const std::array<i64, 5> key = {m->bs, m->n, m->nnzb, max_block_row(m), k};
+  const bool tiled = m->bs == 3 && use_tiled_spmv();
+  auto known = ctx->spmv_tune.find(key);
+  if (known != ctx->spmv_tune.end()) {
+    if (tiled) {
+      w->stages[k] = known->second[0];
+    } else {
+      (mixed ? w->vpr32 : w->vpr) = known->second[0];
+      w->stream[k] = known->second[1] != 0;
+    }
+    return;
+  }
   spmv_timing_state(m, w, mixed);
   auto trial = [&]() {
     enqueue_spmv(m, w, mixed);  // warm
     return time_spmv_launches(m, w, mixed, 8);
   };
-  if (m->bs == 3 && use_tiled_spmv()) {
+  if (tiled) {
     int optin = 0;
     CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     const size_t vb = mixed ? 4 : 8;
@@ -1787,6 +1800,7 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
       }
     }
     w->stages[k] = best;
+    ctx->spmv_tune[key] = {best, 0};
   } else {
     // Lanes per row change the summation order inside a row, so a shape
     // replaces the default only when it is clearly (10%) faster: near-ties
@@ -1814,6 +1828,7 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
     }
     v = best;
     strm = best_stream;
+    ctx->spmv_tune[key] = {best, best_stream ? 1 : 0};
   }
 }
 

@@ -811,19 +811,29 @@ class PoissonSolution:
     residual: float
 
 
+def _device_vector(ctx: Context, n: int):
+    """A device vector for the drivers: the load vector and the solution stay
+    on the device from assembly to the end of the solve. It is allocated on
+    the context's stream, the stream the library's kernels use it on."""
+    import torch
+    dev = torch.device("cuda", ctx.device)
+    with torch.cuda.stream(torch.cuda.ExternalStream(ctx.stream, device=dev)):
+        return torch.empty(n, dtype=torch.float64, device=dev)
+
+
 def _solve_poisson(mesh: Mesh, source, boundary_value, tol, max_iter, ctx, precision):
     ctx = ctx or default_context()
     V = FunctionSpace(ctx, mesh, FCU_SPACE_P1)
     M = Matrix(ctx, V).assemble_stiffness()
     q = V.quadrature_points()
     fq = np.broadcast_to(np.asarray(source(*[q[:, d] for d in range(mesh.dim)]), np.float64), (len(q),)).copy()
-    b = V.rhs_values(fq)
+    b = V.rhs_values(fq, out=_device_vector(ctx, V.ndofs))
     bd = V.boundary_dofs()
     bv = np.broadcast_to(np.asarray(boundary_value(*[mesh.coords[bd, d] for d in range(mesh.dim)]),
                                     np.float64), (len(bd),)).copy()
     M.apply_dirichlet(b, bd, bv)
-    x, info = M.pcg(b, tol=tol, max_iter=max_iter, precision=precision)
-    return PoissonSolution(x, info.iterations, info.residual)
+    x, info = M.pcg(b, x=_device_vector(ctx, V.ndofs), tol=tol, max_iter=max_iter, precision=precision)
+    return PoissonSolution(x.cpu().numpy(), info.iterations, info.residual)
 
 
 def solve_poisson_2d(mesh: Mesh, source, boundary_value, tol, max_iter, ctx=None, precision=FCU_FP64):
@@ -1049,10 +1059,11 @@ def solve_elasticity_3d(mesh: Mesh, material: ElasticMaterial, body_force, bc: V
     ctx = ctx or default_context()
     V = FunctionSpace(ctx, mesh, FCU_SPACE_P1_VEC3)
     M = Matrix(ctx, V).assemble_elasticity(material.youngs_modulus, material.poissons_ratio)
-    f = V.body_force(body_force)
+    f = V.body_force(body_force, out=_device_vector(ctx, V.ndofs))
     d, v = bc.arrays()
     M.apply_dirichlet(f, d, v)
-    x, info = M.pcg(f, tol=tol, max_iter=max_iter, precision=precision)
+    xd, info = M.pcg(f, x=_device_vector(ctx, V.ndofs), tol=tol, max_iter=max_iter, precision=precision)
+    x = xd.cpu().numpy()
     return ElasticitySolution(x, mesh.coords + x.reshape(-1, 3), info.iterations, info.residual)
 
 
