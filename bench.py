@@ -674,7 +674,7 @@ def run_reference(args, cfg):
     }
 
 
-PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024")
+PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5")
 
 
 def profile_case(name):
@@ -684,7 +684,11 @@ def profile_case(name):
       mass_c2          vector-P1 mass of the C2 mesh, assembled 3 times
       block_update_c2  12 block-Jacobi FP64 PCG iterations on the C2 system
       transient_1024   3 Crank-Nicolson steps of the 1024^2 heat problem,
-                       12 PCG iterations each"""
+                       12 PCG iterations each
+      batch_c5         the C5 batch of 256 Poisson problems, mixed PCG capped
+                       at 60 iterations per instance, 3 launches of the
+                       persistent batch kernel (shape fixed by FCU_BATCH_* if
+                       set, else tuned first)"""
     import torch
     import fenics_cuda as fcu
     ctx = fcu.Context(0)
@@ -706,6 +710,22 @@ def profile_case(name):
             M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
             M.block_jacobi(True)
             M.pcg(b, tol=1e-30, max_iter=12, raise_on_error=False)
+        ctx.synchronize()
+        M.close(); V.close()
+    elif name == "batch_c5":
+        rng = np.random.default_rng(2024)
+        ns = rng.integers(32, 257, size=256)
+        meshes = [fcu.unit_square(int(n), int(n)) for n in ns]
+        kap = np.concatenate([np.exp(rng.standard_normal(m.nc)) for m in meshes])
+        fs = np.concatenate([rng.uniform(-1.0, 1.0, m.nv) for m in meshes])
+        mesh, offs = fcu.concat_meshes(meshes)
+        V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
+        M = fcu.Matrix(ctx, V).assemble_stiffness(kap)
+        b = V.rhs_source(fcu.FCU_SRC_NODAL, nodal=fs)
+        bd = V.boundary_dofs()
+        M.apply_dirichlet(b, bd, np.zeros(len(bd)))
+        for _ in range(3):
+            M.batch_pcg(offs, b, tol=1e-8, max_iter=60, precision=fcu.FCU_MIXED, raise_on_error=False)
         ctx.synchronize()
         M.close(); V.close()
     elif name == "transient_1024":
