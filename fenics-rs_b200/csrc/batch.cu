@@ -107,10 +107,9 @@ __device__ __forceinline__ T batch_row(const int* __restrict__ rp, const int* __
 // columns, then all its operand entries, before the arithmetic. Entries are
 // summed in CSR order; unused slots read row 0's operand with weight 0.
 template <bool DIFF, class T>
-__device__ __forceinline__ T batch_row1(const int* __restrict__ rp, const int* __restrict__ ci,
-                                        const T* __restrict__ val, i64 row, const T* __restrict__ xv) {
+__device__ __forceinline__ T batch_row1(int a0, int a1, const int* __restrict__ ci, const T* __restrict__ val, i64 row,
+                                        const T* __restrict__ xv) {
   constexpr int E = sizeof(T) == 4 ? 8 : 4;
-  const int a0 = rp[row], a1 = rp[row + 1];
   const T xa = DIFF ? xv[row] : T(0);
   T s = T(0);
   for (int k0 = a0; k0 < a1; k0 += E) {
@@ -166,7 +165,24 @@ __device__ __forceinline__ void batch_spmv(const int* __restrict__ rp, const int
                                            Emit emit) {
   const int tid = threadIdx.x;
   if (VPR == 1) {
-    for (i64 row = c0 + tid; row < c1; row += BT) emit(row, batch_row1<DIFF, T>(rp, ci, val, row, v));
+    // the next row's bounds are fetched while this row is summed
+    i64 row = c0 + tid;
+    int a0 = 0, a1 = 0;
+    if (row < c1) {
+      a0 = rp[row];
+      a1 = rp[row + 1];
+    }
+    for (; row < c1; row += BT) {
+      const i64 nxt = row + BT;
+      int n0 = 0, n1 = 0;
+      if (nxt < c1) {
+        n0 = rp[nxt];
+        n1 = rp[nxt + 1];
+      }
+      emit(row, batch_row1<DIFF, T>(a0, a1, ci, val, row, v));
+      a0 = n0;
+      a1 = n1;
+    }
   } else {
     constexpr int G = BT / VPR;
     const int g = tid / VPR, sub = tid % VPR;
