@@ -185,6 +185,7 @@ struct fcu_matrix_s {
   bool missing_diag = false;  // a wrapped block row without a diagonal block
   DBuf<int> rowblk;     // row blocks of the CSR-stream SpMV (scalar, built on first use)
   int nrowblk = 0;
+  int tile_cap1[4] = {0, 0, 0, 0};  // scalar tiled SpMV: most entries in a tile of 32, 64, 128, 256 rows
   Workspace* ws = nullptr;
   BatchWorkspace* bws = nullptr;
   ~fcu_matrix_s();

@@ -399,7 +399,9 @@ __global__ void __launch_bounds__(VBLOCK) k_direction(i64 n, T* __restrict__ p, 
     p[i] = z[i] + beta * p[i];
 }
 
-// --- 3x3-block SpMV with TMA-staged tiles --------------------------------------
+// --- block and scalar SpMV with TMA-staged tiles --------------------------------
+// (3x3-block CSR, and scalar CSR in FP64, where each stored "block" is one
+// entry and 2-16 lanes share a row.)
 // A persistent CTA walks tiles of TR consecutive block rows. One thread streams
 // each tile's row pointers, column indices and block values into shared memory
 // with bulk asynchronous copies (cp.async.bulk, completion counted on an
@@ -463,10 +465,12 @@ struct TileHeader {
 
 __host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
 
-template <class T, int TR>
+// BS x BS values per stored block: BS = 3 (3x3-block CSR) or 1 (scalar CSR,
+// where a "block" is one entry).
+template <class T, int TR, int BS = 3>
 __host__ __device__ size_t tile_stage_bytes(int cap_blocks) {
   return align128(sizeof(TileHeader)) + align128((TR + 1) * 4 + 16) + align128((size_t)cap_blocks * 4 + 32) +
-         align128((size_t)cap_blocks * 9 * sizeof(T) + 32);
+         align128((size_t)cap_blocks * BS * BS * sizeof(T) + 32);
 }
 
 // Warp-specialised pipeline: warp 0 is the producer (one elected lane issues
@@ -484,12 +488,12 @@ constexpr int TILED_CTAS_PER_SM = 2;  // resident CTAs of the tiled SpMV per SM
 
 // Output of the tiled kernel: Ap for one scalar row, and p.Ap accumulated
 // from the row's own operand value (already in registers).
-template <class T>
+template <class T, int BS = 3>
 struct EmitApOwn {
   T* ap;
   double dot = 0.0;
   __device__ __forceinline__ void operator()(i64 node, int a, T s, T own) {
-    ap[node * 3 + a] = s;
+    ap[node * BS + a] = s;
     dot += (double)own * (double)s;
   }
 };
@@ -499,15 +503,17 @@ struct EmitApOwn {
 // predecessor's tail; the producer warp's lanes fetch the row-pointer bounds
 // of the CTA's next 32 tiles in one round of loads. Returns false, having
 // computed nothing, when the solver state says the solve is over.
-template <bool DIFF, class T, int TR, class GX, class Emit>
-__device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, const int* __restrict__ ci,
-                                                const T* __restrict__ val, i64 nrows, int cap_blocks, int nstage,
-                                                const GX& gx, Emit& emit, CgState* st) {
+template <bool DIFF, class T, int TR, int BS, class GX, class Emit>
+__device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int* __restrict__ ci,
+                                           const T* __restrict__ val, i64 nrows, int cap_blocks, int nstage,
+                                           const GX& gx, Emit& emit, CgState* st) {
   extern __shared__ __align__(128) unsigned char tile_smem[];
   __shared__ unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
   constexpr int LPR = 32 * SPMV_CONSUMER_WARPS / TR;  // consumer lanes per block row
-  static_assert(LPR == 8 || LPR == 16, "tile rows");
-  const size_t stage_bytes = tile_stage_bytes<T, TR>(cap_blocks);
+  constexpr int VPB = BS * BS;                         // values per stored block
+  static_assert(BS == 1 || BS == 3, "block size");
+  static_assert(BS == 1 ? (LPR >= 2 && LPR <= 16) : (LPR == 8 || LPR == 16), "tile rows");
+  const size_t stage_bytes = tile_stage_bytes<T, TR, BS>(cap_blocks);
   const i64 ntiles = (nrows + TR - 1) / TR;
   const i64 G = gridDim.x;
   const int mytiles = blockIdx.x < ntiles ? (int)((ntiles - blockIdx.x + G - 1) / G) : 0;
@@ -546,12 +552,12 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
       const unsigned rp_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);
       const uintptr_t c_lo = reinterpret_cast<uintptr_t>(ci + b0) & ~(uintptr_t)15;
       const uintptr_t c_hi = (reinterpret_cast<uintptr_t>(ci + b1) + 15) & ~(uintptr_t)15;
-      const uintptr_t v_lo = reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) & ~(uintptr_t)15;
-      const uintptr_t v_hi = (reinterpret_cast<uintptr_t>(val + 9 * (i64)b1) + 15) & ~(uintptr_t)15;
+      const uintptr_t v_lo = reinterpret_cast<uintptr_t>(val + VPB * (i64)b0) & ~(uintptr_t)15;
+      const uintptr_t v_hi = (reinterpret_cast<uintptr_t>(val + VPB * (i64)b1) + 15) & ~(uintptr_t)15;
       h->b0 = b0;
       h->rows = rows;
       h->col_off = (int)(reinterpret_cast<uintptr_t>(ci + b0) - c_lo);
-      h->val_off = (int)(reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) - v_lo);
+      h->val_off = (int)(reinterpret_cast<uintptr_t>(val + VPB * (i64)b0) - v_lo);
       const unsigned cb = (unsigned)(c_hi - c_lo), vb = (unsigned)(v_hi - v_lo);
       fence_proxy_async();
       mbar_arrive_expect_tx(&full[s], rp_bytes + cb + vb);
@@ -613,6 +619,28 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
     const int b0 = h->b0;
     const i64 row = (blockIdx.x + (i64)k * G) * TR + row_in_tile;
     const bool valid = row_in_tile < h->rows;
+    if constexpr (BS == 1) {
+      // scalar row: lane `sub` sums entries sub, sub + LPR, ... (difference
+      // form for the mixed operator: the diagonal slot holds the row sum)
+      T a = T(0), xo = T(0);
+      if (valid) {
+        xo = gx(row);
+        const int kb1 = rps[row_in_tile + 1] - b0;
+#pragma unroll 2
+        for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += LPR) {
+          const int c = cis[kb];
+          const T v = vls[kb];
+          const T y = DIFF ? (c == (int)row ? xo : gx(c) - xo) : gx(c);
+          a += v * y;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) a += __shfl_xor_sync(FULL, a, o);
+      if (valid && sub == 0) emit(row, 0, a, xo);
+      continue;
+    }
     T a0 = T(0), a1 = T(0), a2 = T(0);
     T x0 = T(0), x1 = T(0), x2 = T(0);
     if (valid) {
@@ -652,13 +680,13 @@ __device__ __forceinline__ bool bsr3_tiled_rows(const int* __restrict__ rp, cons
   return true;
 }
 
-template <int DIFF, class T, int TR>
+template <int DIFF, class T, int TR, int BS = 3>
 __global__ void __launch_bounds__(SPMV_THREADS)
     k_spmv_tiled(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val, i64 nrows,
                  int cap_blocks, int nstage, const T* __restrict__ p, T* __restrict__ ap, CgState* st,
                  double* partials) {
-  EmitApOwn<T> em{ap};
-  if (!bsr3_tiled_rows<DIFF != 0, T, TR>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, st)) return;
+  EmitApOwn<T, BS> em{ap};
+  if (!tiled_rows<DIFF != 0, T, TR, BS>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, st)) return;
   store_pap_partial(em.dot, partials);
 }
 
@@ -1124,6 +1152,7 @@ struct Workspace {
   cudaEvent_t ev[2] = {nullptr, nullptr};  // a replay's state record has arrived on the host
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool stream[2] = {false, false};  // scalar PCG SpMV: CSR-stream kernel (FP64, FP32)
+  bool tiled1[2] = {false, false};  // scalar PCG SpMV: tiled kernel (FP64, FP32), ring depth in stages[]
   int vpr = 0;    // lanes per row of the FP64 CSR kernels (tuned with the FP64 SpMV)
   int vpr32 = 0;  // lanes per row of the FP32 CSR SpMV (tuned with it)
   int stages[2] = {3, 3};  // ring depth of the tiled block SpMV: FP64, FP32
@@ -1309,7 +1338,66 @@ size_t tile_stage_bytes_rt(size_t value_bytes, int tr, int cap) {
   return tile_stage_bytes<double, 32>(cap);
 }
 
+size_t scalar_stage_bytes(size_t value_bytes, int tr, int cap) {
+  const bool f = value_bytes == 4;
+  switch (tr) {
+    case 256: return f ? tile_stage_bytes<float, 256, 1>(cap) : tile_stage_bytes<double, 256, 1>(cap);
+    case 128: return f ? tile_stage_bytes<float, 128, 1>(cap) : tile_stage_bytes<double, 128, 1>(cap);
+    case 64: return f ? tile_stage_bytes<float, 64, 1>(cap) : tile_stage_bytes<double, 64, 1>(cap);
+    default: return f ? tile_stage_bytes<float, 32, 1>(cap) : tile_stage_bytes<double, 32, 1>(cap);
+  }
+}
+
 int max_block_row(fcu_matrix m) { return m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32); }
+
+// Rows per tile of the scalar tiled SpMV: 512 consumer lanes, 2-16 per row,
+// about four entries per lane at the mean row length.
+int scalar_tile_rows(fcu_matrix m) {
+  const double mean = m->nnodes > 0 ? (double)m->nnzb / (double)m->nnodes : 1.0;
+  return mean <= 8.0 ? 256 : mean <= 16.0 ? 128 : mean <= 48.0 ? 64 : 32;
+}
+
+__global__ void k_tile_cap(const int* __restrict__ rp, i64 nrows, int tr, int* __restrict__ cap) {
+  const i64 ntiles = (nrows + tr - 1) / tr;
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < ntiles; t += (i64)gridDim.x * blockDim.x) {
+    const i64 r0 = t * tr, r1 = std::min<i64>(r0 + tr, nrows);
+    atomicMax(cap, rp[r1] - rp[r0]);
+  }
+}
+
+// Most entries in one tile of `tr` rows (scalar CSR), computed once per matrix.
+int scalar_tile_cap(fcu_matrix m, int tr) {
+  const int slot = tr == 32 ? 0 : tr == 64 ? 1 : tr == 128 ? 2 : 3;
+  if (m->tile_cap1[slot] > 0) return m->tile_cap1[slot];
+  fcu_ctx ctx = m->ctx;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CUDA_CHECK(cudaStreamIsCapturing(ctx->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) fail(FCU_ERR_CUDA, "tile sizes of the scalar tiled SpMV requested during capture");
+  DBuf<int> cap;
+  cap.alloc(1);
+  CUDA_CHECK(cudaMemsetAsync(cap.p, 0, sizeof(int), ctx->stream));
+  const i64 ntiles = (m->nnodes + tr - 1) / tr;
+  k_tile_cap<<<grid_for(std::max<i64>(ntiles, 1), 256, ctx->num_sms * 4), 256, 0, ctx->stream>>>(m->row_ptr, m->nnodes,
+                                                                                                 tr, cap.p);
+  LAUNCH_CHECK(ctx);
+  int h = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&h, cap.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  m->tile_cap1[slot] = std::max(h, 1);
+  return m->tile_cap1[slot];
+}
+
+// Whether the scalar tiled SpMV fits: two ring stages of the longest tile,
+// TILED_CTAS_PER_SM CTAs per SM.
+bool scalar_tiled_fits(fcu_matrix m, bool mixed) {
+  fcu_ctx ctx = m->ctx;
+  int optin = 0, per_sm_max = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  CUDA_CHECK(cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+  const int tr = scalar_tile_rows(m);
+  const size_t stage = scalar_stage_bytes(mixed ? 4 : 8, tr, scalar_tile_cap(m, tr));
+  return 2 * stage + 1024 <= (size_t)optin && TILED_CTAS_PER_SM * (2 * stage + 2048) <= (size_t)per_sm_max;
+}
 
 // Ring depth actually used: the requested depth, lowered until
 // TILED_CTAS_PER_SM CTAs fit on an SM (at least two stages).
@@ -1324,14 +1412,14 @@ int fitted_stages(fcu_ctx ctx, int requested, size_t stage) {
 
 // Tiled 3x3-block SpMV launch: shared memory for the ring sized by the
 // longest block row; grid = resident CTAs (persistent), at most one per tile.
-template <int DIFF, class T, int TR>
+template <int DIFF, class T, int TR, int BS = 3>
 int launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
   fcu_ctx ctx = m->ctx;
-  const int cap = TR * max_block_row(m);
-  const size_t stage = tile_stage_bytes<T, TR>(cap);
+  const int cap = BS == 3 ? TR * max_block_row(m) : scalar_tile_cap(m, TR);
+  const size_t stage = tile_stage_bytes<T, TR, BS>(cap);
   const int nstage = fitted_stages(ctx, w->stages[sizeof(T) == 4 ? 1 : 0], stage);
   const size_t smem = nstage * stage;
-  auto kern = k_spmv_tiled<DIFF, T, TR>;
+  auto kern = k_spmv_tiled<DIFF, T, TR, BS>;
   static int configured_dev = -1;
   static size_t configured_smem = 0;
   if (configured_dev != ctx->device || configured_smem < smem) {
@@ -1341,7 +1429,7 @@ int launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T
   }
   int per_sm = 0;
   CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SPMV_THREADS, smem));
-  if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "block rows too long for the tiled SpMV");
+  if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "rows too long for the tiled SpMV");
   // The grid sets the order in which p.Ap is reduced, so it does not follow
   // the ring depth: TILED_CTAS_PER_SM CTAs per SM whenever they fit, which
   // keeps the iterates identical for every depth the tuner may pick.
@@ -1358,6 +1446,18 @@ template <int DIFF, class T>
 int launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
   if (tile_rows(sizeof(T)) == 64) return launch_spmv_tiled_tr<DIFF, T, 64>(m, w, val, p, ap);
   return launch_spmv_tiled_tr<DIFF, T, 32>(m, w, val, p, ap);
+}
+
+// Scalar CSR through the tiled kernel: tile rows by mean row length, so that
+// each of the 2-16 lanes of a row sums a few entries.
+template <int DIFF, class T>
+int launch_spmv_tiled_scalar(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
+  switch (scalar_tile_rows(m)) {
+    case 256: return launch_spmv_tiled_tr<DIFF, T, 256, 1>(m, w, val, p, ap);
+    case 128: return launch_spmv_tiled_tr<DIFF, T, 128, 1>(m, w, val, p, ap);
+    case 64: return launch_spmv_tiled_tr<DIFF, T, 64, 1>(m, w, val, p, ap);
+    default: return launch_spmv_tiled_tr<DIFF, T, 32, 1>(m, w, val, p, ap);
+  }
 }
 
 bool use_tiled_spmv() {
@@ -1409,6 +1509,8 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       int npap = g;
       if (m->bs == 3 && use_tiled_spmv()) {
         npap = launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+      } else if (w->tiled1[0]) {
+        npap = launch_spmv_tiled_scalar<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
       } else if (w->stream[0]) {
         npap = stream_grid_for(ctx, m->nrowblk, k_spmv_stream<double>);
         launch_pdl_cfg(ctx, k_spmv_stream<double>, npap, STREAM_THREADS, 0, m->row_ptr, m->col_idx, m->val64.p,
@@ -1428,6 +1530,8 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
       int npap = g;
       if (m->bs == 3 && use_tiled_spmv()) {
         npap = launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+      } else if (w->tiled1[1]) {
+        npap = launch_spmv_tiled_scalar<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
       } else if (w->stream[1]) {
         npap = stream_grid_for(ctx, m->nrowblk, k_spmv_stream<float>);
         launch_pdl_cfg(ctx, k_spmv_stream<float>, npap, STREAM_THREADS, 0, m->row_ptr, m->col_idx, m->val32.p,
@@ -1710,6 +1814,7 @@ void enqueue_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   const int g = w->grid;
   if (mixed) {
     if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+    else if (w->tiled1[1]) launch_spmv_tiled_scalar<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
     else if (w->stream[1])
       launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<float>), STREAM_THREADS, 0, m->row_ptr,
                      m->col_idx, m->val32.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa32.p, w->ap32.p, w->st.p,
@@ -1719,6 +1824,7 @@ void enqueue_spmv(fcu_matrix m, Workspace* w, bool mixed) {
                     w->ap32.p, w->st.p, w->partials.p);
   } else {
     if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
+    else if (w->tiled1[0]) launch_spmv_tiled_scalar<0, double>(m, w, m->val64.p, w->pa64.p, w->ap64.p);
     else if (w->stream[0])
       launch_pdl_cfg(ctx, k_spmv_stream<double>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<double>), STREAM_THREADS, 0, m->row_ptr,
                      m->col_idx, m->val64.p, m->diag_pos, m->rowblk.p, m->nrowblk, w->pa64.p, w->ap64.p, w->st.p,
@@ -1746,6 +1852,14 @@ double time_spmv_launches(fcu_matrix m, Workspace* w, bool mixed, int reps) {
   return reps > 0 ? (double)t / reps : 0.0;
 }
 
+int scalar_tiled_mode() {
+  static int v = [] {
+    const char* e = getenv("FCU_SCALAR_TILED");
+    return e ? atoi(e) : 1;
+  }();
+  return v;
+}
+
 bool tuning_enabled() {
   static int v = [] {
     const char* e = getenv("FCU_TUNE");
@@ -1766,6 +1880,10 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   if (known != ctx->spmv_tune.end()) {
     if (tiled) {
       w->stages[k] = known->second[0];
+    } else if (known->second[1] == 2) {
+      w->tiled1[k] = true;
+      w->stages[k] = known->second[0];
+      scalar_tile_cap(m, scalar_tile_rows(m));  // measured here, never while a graph is being captured
     } else {
       (mixed ? w->vpr32 : w->vpr) = known->second[0];
       w->stream[k] = known->second[1] != 0;
@@ -1802,11 +1920,33 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
     w->stages[k] = best;
     ctx->spmv_tune[key] = {best, 0};
   } else {
-    // Lanes per row change the summation order inside a row, so a shape
-    // replaces the default only when it is clearly (10%) faster: near-ties
-    // then cannot flip the choice, and the iterates, from run to run.
-    // Candidates: the CSR-stream kernel (when the rows are short) and CSR
-    // vectors of 4-32 lanes per row.
+    // The tiled kernel (TMA-staged tiles of rows) replaces the others in
+    // FP64 whenever it fits: by rule, not by timing, so that the choice and
+    // the iterates repeat from run to run; only its ring depth is timed,
+    // which changes no result. FCU_SCALAR_TILED: 0 never, 1 FP64 (default),
+    // 2 both precisions.
+    const int st_mode = scalar_tiled_mode();
+    if (use_tiled_spmv() && (st_mode == 2 || (st_mode == 1 && !mixed)) && scalar_tiled_fits(m, mixed)) {
+      w->tiled1[k] = true;
+      int best_stages = 2;
+      double tiled_ms = 1e30;
+      for (int ns = 2; ns <= MAX_STAGES; ++ns) {
+        w->stages[k] = ns;
+        const double ms = trial();
+        if (ms < tiled_ms) {
+          tiled_ms = ms;
+          best_stages = ns;
+        }
+      }
+      w->stages[k] = best_stages;
+      ctx->spmv_tune[key] = {best_stages, 2};
+      return;
+    }
+    // Otherwise the CSR kernels. Lanes per row change the summation order
+    // inside a row, so a shape replaces the default only when it is clearly
+    // (10%) faster: near-ties then cannot flip the choice, and the iterates,
+    // from run to run. Candidates: the CSR-stream kernel (when the rows are
+    // short) and CSR vectors of 4-32 lanes per row.
     int& v = mixed ? w->vpr32 : w->vpr;
     bool& strm = w->stream[k];
     const bool dflt_stream = strm;
