@@ -710,7 +710,7 @@ __device__ __forceinline__ void decide_after_update(CgState* st, double rz_new, 
 // x += alpha p ; r -= alpha Ap ; z = D^-1 r (stored as T) ; (r.z, r.r).
 // x, r and D^-1 are FP64 in both precisions.
 template <class T>
-__global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x, double* __restrict__ r,
+__global__ void __launch_bounds__(VBLOCK, 5) k_update(i64 n, double* __restrict__ x, double* __restrict__ r,
                                                    const T* __restrict__ p, const T* __restrict__ ap,
                                                    const double* __restrict__ invd, T* __restrict__ z, CgState* st,
                                                    double* partials, int npap) {
@@ -733,6 +733,14 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
     }
   }
   grid_dep_sync();
+  // Ap of the first two elements is loaded before the p.Ap partials are
+  // summed, so that the two round trips overlap
+  T aa[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const i64 i = i0 + k * stride;
+    if (i < n) aa[k] = __ldcg(ap + i);
+  }
   if (block_stopped(st)) return;
   double alpha;
   if (!take_alpha(st, partials, npap, &alpha)) return;
@@ -742,7 +750,7 @@ __global__ void __launch_bounds__(VBLOCK) k_update(i64 n, double* __restrict__ x
     const i64 i = i0 + k * stride;
     if (i < n) {
       x[i] = xa[k] + alpha * (double)pa[k];
-      const double ri = ra[k] - alpha * (double)ap[i];
+      const double ri = ra[k] - alpha * (double)aa[k];
       r[i] = ri;
       const double zi = ri * da[k];
       z[i] = (T)zi;
