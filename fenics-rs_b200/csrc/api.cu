@@ -30,7 +30,7 @@ void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev);
 void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes);
 int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
                    i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
-                   fcu_solve_info* info);
+                   fcu_solve_info* info, const int* fixed_shape = nullptr);
 void batch_config(fcu_matrix m, int precision, int* vpr, int* threads, int* cluster);
 void element_stresses_impl(fcu_space s, double lam, double mu, const double* u_dev, double* stress, double* strain,
                            double* vm, double* trace);

@@ -155,6 +155,7 @@ struct BatchArgs {
   i64* iters;
   i64* updates;
   double* relres;
+  double* resid;  // absolute residual ||r|| per instance
   int* status;
 };
 
@@ -357,6 +358,7 @@ __global__ void __launch_bounds__(BT, 1024 / BT) k_batch_pcg(BatchArgs a) {
       a.iters[inst] = iter;
       a.updates[inst] = updates;
       a.relres[inst] = bnorm > 0.0 ? sqrt(rr) / bnorm : sqrt(rr);
+      a.resid[inst] = sqrt(rr);
       a.status[inst] = status;
     }
   }
@@ -416,7 +418,7 @@ struct BatchWorkspace {
   DBuf<float> z32, p32, ap32;
   DBuf<unsigned> counter;
   DBuf<i64> iters, updates;
-  DBuf<double> relres;
+  DBuf<double> relres, resid;
   DBuf<int> status;
   BatchConfig cfg[2];
   bool tuned[2] = {false, false};
@@ -462,6 +464,7 @@ BatchArgs make_args(fcu_matrix m, BatchWorkspace* w, bool mixed, double tol, i64
   a.iters = w->iters.p;
   a.updates = w->updates.p;
   a.relres = w->relres.p;
+  a.resid = w->resid.p;
   a.status = w->status.p;
   return a;
 }
@@ -564,7 +567,7 @@ BatchConfig autotune(fcu_matrix m, BatchWorkspace* w, bool mixed, double tol) {
 // buffers handled by the caller (api.cu) through staging.
 int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
                    i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
-                   fcu_solve_info* info) {
+                   fcu_solve_info* info, const int* fixed_shape) {
   fcu_ctx ctx = m->ctx;
   const bool mixed = precision == FCU_MIXED;
   if (m->bs != 1) fail(FCU_ERR_UNSUPPORTED, "batched PCG takes scalar (CSR) matrices");
@@ -616,6 +619,7 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
     w->iters.alloc(nb);
     w->updates.alloc(nb);
     w->relres.alloc(nb);
+    w->resid.alloc(nb);
     w->status.alloc(nb);
   }
   const i64 n = m->n;
@@ -639,7 +643,14 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
   CUDA_CHECK(cudaMemcpyAsync(w->b.p, b_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   const int k = mixed ? 1 : 0;
   if (!w->tuned[k]) {
-    w->cfg[k] = autotune(m, w, mixed, tol);
+    if (fixed_shape) {
+      w->cfg[k].vpr = fixed_shape[0];
+      w->cfg[k].threads = fixed_shape[1];
+      w->cfg[k].cluster = fixed_shape[2];
+      if (!pick_kernel(mixed, w->cfg[k])) fail(FCU_ERR_BAD_ARG, "no batched PCG kernel of that shape");
+    } else {
+      w->cfg[k] = autotune(m, w, mixed, tol);
+    }
     w->tuned[k] = true;
   }
   const BatchConfig c = w->cfg[k];
@@ -678,18 +689,19 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   std::vector<i64> it(nb), up(nb);
-  std::vector<double> rel(nb);
+  std::vector<double> rel(nb), res(nb);
   std::vector<int> st(nb);
   download(ctx, it.data(), w->iters.p, nb);
   download(ctx, up.data(), w->updates.p, nb);
   download(ctx, rel.data(), w->relres.p, nb);
+  download(ctx, res.data(), w->resid.p, nb);
   download(ctx, st.data(), w->status.p, nb);
   if (iters_host) std::copy(it.begin(), it.end(), iters_host);
   if (relres_host) std::copy(rel.begin(), rel.end(), relres_host);
   if (status_host) std::copy(st.begin(), st.end(), status_host);
   int worst = FCU_OK;
   i64 max_it = 0, sum_it = 0, sum_up = 0;
-  double max_rel = 0.0;
+  double max_rel = 0.0, max_res = 0.0;
   double bytes = 0.0;
   const double w8 = mixed ? 4.0 : 8.0;
   for (i64 i = 0; i < nb; ++i) {
@@ -698,6 +710,7 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
     sum_it += it[i];
     sum_up += up[i];
     max_rel = std::max(max_rel, rel[i]);
+    max_res = std::max(max_res, res[i]);
     // per iteration: values + columns + row pointers, then the vector passes
     // (direction 3w, SpMV p and Ap 2w, update 40 + 3w bytes per row)
     const double rows = (double)(offsets_host[i + 1] - offsets_host[i]);
@@ -706,7 +719,7 @@ int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* 
   if (info) {
     info->iterations = max_it;
     info->outer_updates = sum_up;
-    info->residual = 0.0;
+    info->residual = max_res;
     info->rel_residual = max_rel;
     info->kernel_ms = ms;
     info->effective_bw_gbps = ms > 0 ? bytes / (ms * 1e-3) / 1e9 : 0.0;

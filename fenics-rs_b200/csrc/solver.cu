@@ -1646,6 +1646,24 @@ void build_rowsum32(fcu_matrix m) {
 
 void tune_spmv(fcu_matrix m, Workspace* w, bool mixed);
 
+int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
+                   i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
+                   fcu_solve_info* info, const int* fixed_shape);
+
+// Scalar systems of at most this many rows go through the batched kernel
+// (see run_pcg): measured faster up to ~17k rows in FP64 and ~33k in mixed
+// precision, slower in FP64 at 33k. FCU_SMALL_BATCHED=0 keeps them on the
+// per-iteration graph.
+constexpr i64 SMALL_SYSTEM_ROWS_FP64 = 20000;
+constexpr i64 SMALL_SYSTEM_ROWS_MIXED = 32768;
+bool small_systems_batched() {
+  static int v = [] {
+    const char* e = getenv("FCU_SMALL_BATCHED");
+    return e ? atoi(e) : 1;
+  }();
+  return v != 0;
+}
+
 // Core PCG driver on device buffers: b_dev, x0_dev (nullable) -> x_dev.
 // inv_diag_dev (nullable) overrides the matrix diagonal (solve_csr_cg_gpu).
 int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_dev, double tol, i64 max_iter,
@@ -1656,6 +1674,24 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
   if (mixed && m->bdinv.p) fail(FCU_ERR_UNSUPPORTED, "block-Jacobi preconditioning runs in FP64");
   if (m->block_jacobi && !inv_diag_dev) refresh_block_jacobi(m);
   if (mixed && m->missing_diag) fail(FCU_ERR_UNSUPPORTED, "the mixed operator needs every diagonal block");
+  // A small scalar system solved from x0 = 0 with the point-Jacobi diagonal
+  // of its own values: one launch of the batched kernel with the system as
+  // its single instance (one cluster of up to 8 CTAs, reductions in
+  // distributed shared memory), instead of three launches per iteration,
+  // whose fixed costs dominate at this size. Same recurrence and stopping
+  // rules (cg.rs:40-149); the kernel shape is fixed by rule, so the
+  // iterates repeat from run to run.
+  if (m->bs == 1 && !x0_dev && !gpu_semantics && !inv_diag_dev && !m->bdinv.p && max_iter > 0 &&
+      m->n > 0 && m->n <= (mixed ? SMALL_SYSTEM_ROWS_MIXED : SMALL_SYSTEM_ROWS_FP64) && small_systems_batched()) {
+    const double mean = (double)m->nnzb / (double)m->n;
+    const int shape[3] = {mean <= 12.0 ? 1 : mean <= 40.0 ? 2 : 4, m->n <= 4096 ? 512 : 1024,
+                          m->n <= 512 ? 1 : m->n <= 1024 ? 2 : m->n <= 2048 ? 4 : 8};
+    const i64 offs[2] = {0, m->n};
+    i64 it = 0;
+    double rel = 0.0;
+    int st = 0;
+    return batch_pcg_impl(m, 1, offs, b_dev, x_dev, tol, max_iter, precision, &it, &rel, &st, info, shape);
+  }
   Workspace* w = ensure_ws(m, mixed);
   const i64 n = m->n, nr = m->nnodes;
   const int g = w->grid;
