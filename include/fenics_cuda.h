@@ -206,7 +206,9 @@ int fcu_assemble_surface_traction(fcu_ctx ctx, fcu_space space, int64_t nf, cons
  * arithmetic; FCU_MIXED runs FP32 SpMV/axpy with FP64 dot accumulation and
  * FP64 residual replacement, and stops on the FP64 residual ||b - A64 x||.
  * Returns FCU_ERR_NO_CONVERGENCE / FCU_ERR_BREAKDOWN like the reference's Err;
- * x and info are filled in every case. */
+ * x and info are filled in every case. Small scalar systems (at most 20,000
+ * rows in FP64, 32,768 in FCU_MIXED) started from x0 = NULL run as a single
+ * instance of the batched solver below, in one launch. */
 int fcu_pcg(fcu_ctx ctx, fcu_matrix m, const double* b, const double* x0, double* x, double tol,
             int64_t max_iter, int precision, fcu_solve_info* info);
 
@@ -230,7 +232,7 @@ int fcu_solve_csr_cg(fcu_ctx ctx, int64_t n, const uint32_t* row_ptr, const uint
  * Per-instance iterations, relative residuals and statuses go to the
  * optional host arrays (nb each). Returns FCU_OK when every instance
  * converged, else the first failing status. info: max iterations, total
- * replacements, max relative residual, device time. */
+ * replacements, max absolute and max relative residual, device time. */
 int fcu_batch_pcg(fcu_ctx ctx, fcu_matrix m, int64_t nb, const int64_t* offsets, const double* b, double* x,
                   double tol, int64_t max_iter, int precision, int64_t* iterations, double* rel_residual,
                   int* status, fcu_solve_info* info);
