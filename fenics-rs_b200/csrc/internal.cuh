@@ -185,7 +185,8 @@ struct fcu_matrix_s {
   bool missing_diag = false;  // a wrapped block row without a diagonal block
   DBuf<int> rowblk;     // row blocks of the CSR-stream SpMV (scalar, built on first use)
   int nrowblk = 0;
-  int tile_cap1[4] = {0, 0, 0, 0};  // scalar tiled SpMV: most entries in a tile of 32, 64, 128, 256 rows
+  int tile_cap1[5] = {0, 0, 0, 0, 0};  // scalar tiled SpMV: most entries in a tile of 32, 64, 128, 256, 512 rows
+  int tile_tr1[2] = {-1, -1};          // scalar tiled SpMV: rows per tile (FP64, FP32), 0 = does not fit
   Workspace* ws = nullptr;
   BatchWorkspace* bws = nullptr;
   ~fcu_matrix_s();

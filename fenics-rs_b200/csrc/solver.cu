@@ -512,7 +512,7 @@ __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int
   constexpr int LPR = 32 * SPMV_CONSUMER_WARPS / TR;  // consumer lanes per block row
   constexpr int VPB = BS * BS;                         // values per stored block
   static_assert(BS == 1 || BS == 3, "block size");
-  static_assert(BS == 1 ? (LPR >= 2 && LPR <= 16) : (LPR == 8 || LPR == 16), "tile rows");
+  static_assert(BS == 1 ? (LPR >= 1 && LPR <= 16) : (LPR == 8 || LPR == 16), "tile rows");
   const size_t stage_bytes = tile_stage_bytes<T, TR, BS>(cap_blocks);
   const i64 ntiles = (nrows + TR - 1) / TR;
   const i64 G = gridDim.x;
@@ -1349,6 +1349,7 @@ size_t tile_stage_bytes_rt(size_t value_bytes, int tr, int cap) {
 size_t scalar_stage_bytes(size_t value_bytes, int tr, int cap) {
   const bool f = value_bytes == 4;
   switch (tr) {
+    case 512: return f ? tile_stage_bytes<float, 512, 1>(cap) : tile_stage_bytes<double, 512, 1>(cap);
     case 256: return f ? tile_stage_bytes<float, 256, 1>(cap) : tile_stage_bytes<double, 256, 1>(cap);
     case 128: return f ? tile_stage_bytes<float, 128, 1>(cap) : tile_stage_bytes<double, 128, 1>(cap);
     case 64: return f ? tile_stage_bytes<float, 64, 1>(cap) : tile_stage_bytes<double, 64, 1>(cap);
@@ -1358,13 +1359,6 @@ size_t scalar_stage_bytes(size_t value_bytes, int tr, int cap) {
 
 int max_block_row(fcu_matrix m) { return m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32); }
 
-// Rows per tile of the scalar tiled SpMV: 512 consumer lanes, 2-16 per row,
-// about four entries per lane at the mean row length.
-int scalar_tile_rows(fcu_matrix m) {
-  const double mean = m->nnodes > 0 ? (double)m->nnzb / (double)m->nnodes : 1.0;
-  return mean <= 8.0 ? 256 : mean <= 16.0 ? 128 : mean <= 48.0 ? 64 : 32;
-}
-
 __global__ void k_tile_cap(const int* __restrict__ rp, i64 nrows, int tr, int* __restrict__ cap) {
   const i64 ntiles = (nrows + tr - 1) / tr;
   for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < ntiles; t += (i64)gridDim.x * blockDim.x) {
@@ -1373,9 +1367,12 @@ __global__ void k_tile_cap(const int* __restrict__ rp, i64 nrows, int tr, int* _
   }
 }
 
-// Most entries in one tile of `tr` rows (scalar CSR), computed once per matrix.
+int tile_slot(int tr) { return tr == 32 ? 0 : tr == 64 ? 1 : tr == 128 ? 2 : tr == 256 ? 3 : 4; }
+
+// Most entries in one tile of `tr` rows (scalar CSR), computed once per matrix
+// (never while a graph is being captured).
 int scalar_tile_cap(fcu_matrix m, int tr) {
-  const int slot = tr == 32 ? 0 : tr == 64 ? 1 : tr == 128 ? 2 : 3;
+  const int slot = tile_slot(tr);
   if (m->tile_cap1[slot] > 0) return m->tile_cap1[slot];
   fcu_ctx ctx = m->ctx;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -1395,16 +1392,31 @@ int scalar_tile_cap(fcu_matrix m, int tr) {
   return m->tile_cap1[slot];
 }
 
-// Whether the scalar tiled SpMV fits: two ring stages of the longest tile,
-// TILED_CTAS_PER_SM CTAs per SM.
-bool scalar_tiled_fits(fcu_matrix m, bool mixed) {
+// Rows per tile of the scalar tiled SpMV, or 0 when it does not fit: the
+// tallest of 512, 256, 128, 64, 32 rows whose ring (two stages of the
+// largest tile, TILED_CTAS_PER_SM CTAs per SM) fits in shared memory. A
+// tile's 512 consumer lanes share its rows (512 / TR lanes per row), and the
+// bytes a tile carries amortise its one round trip of operand gathers, so
+// taller tiles are faster. FP32 takes only 512-row tiles: shorter ones ran
+// slower than the CSR-stream kernel. Computed once per matrix and precision.
+int scalar_tile_rows(fcu_matrix m, bool f32) {
+  int& tr = m->tile_tr1[f32 ? 1 : 0];
+  if (tr >= 0) return tr;
   fcu_ctx ctx = m->ctx;
   int optin = 0, per_sm_max = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
   CUDA_CHECK(cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-  const int tr = scalar_tile_rows(m);
-  const size_t stage = scalar_stage_bytes(mixed ? 4 : 8, tr, scalar_tile_cap(m, tr));
-  return 2 * stage + 1024 <= (size_t)optin && TILED_CTAS_PER_SM * (2 * stage + 2048) <= (size_t)per_sm_max;
+  tr = 0;
+  for (int t : {512, 256, 128, 64, 32}) {
+    if (f32 && t != 512) break;
+    if ((i64)t > 2 * std::max<i64>(m->nnodes, 1) && t > 32) continue;  // tiles far taller than the matrix
+    const size_t stage = scalar_stage_bytes(f32 ? 4 : 8, t, scalar_tile_cap(m, t));
+    if (2 * stage + 1024 <= (size_t)optin && TILED_CTAS_PER_SM * (2 * stage + 2048) <= (size_t)per_sm_max) {
+      tr = t;
+      break;
+    }
+  }
+  return tr;
 }
 
 // Ring depth actually used: the requested depth, lowered until
@@ -1456,11 +1468,11 @@ int launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* a
   return launch_spmv_tiled_tr<DIFF, T, 32>(m, w, val, p, ap);
 }
 
-// Scalar CSR through the tiled kernel: tile rows by mean row length, so that
-// each of the 2-16 lanes of a row sums a few entries.
+// Scalar CSR through the tiled kernel, TR rows per tile (scalar_tile_rows).
 template <int DIFF, class T>
 int launch_spmv_tiled_scalar(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
-  switch (scalar_tile_rows(m)) {
+  switch (scalar_tile_rows(m, sizeof(T) == 4)) {
+    case 512: return launch_spmv_tiled_tr<DIFF, T, 512, 1>(m, w, val, p, ap);
     case 256: return launch_spmv_tiled_tr<DIFF, T, 256, 1>(m, w, val, p, ap);
     case 128: return launch_spmv_tiled_tr<DIFF, T, 128, 1>(m, w, val, p, ap);
     case 64: return launch_spmv_tiled_tr<DIFF, T, 64, 1>(m, w, val, p, ap);
@@ -1927,7 +1939,7 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
     } else if (known->second[1] == 2) {
       w->tiled1[k] = true;
       w->stages[k] = known->second[0];
-      scalar_tile_cap(m, scalar_tile_rows(m));  // measured here, never while a graph is being captured
+      scalar_tile_rows(m, mixed);  // tile sizes measured here, never while a graph is being captured
     } else {
       (mixed ? w->vpr32 : w->vpr) = known->second[0];
       w->stream[k] = known->second[1] != 0;
@@ -1964,13 +1976,12 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
     w->stages[k] = best;
     ctx->spmv_tune[key] = {best, 0};
   } else {
-    // The tiled kernel (TMA-staged tiles of rows) replaces the others in
-    // FP64 whenever it fits: by rule, not by timing, so that the choice and
-    // the iterates repeat from run to run; only its ring depth is timed,
-    // which changes no result. FCU_SCALAR_TILED: 0 never, 1 FP64 (default),
-    // 2 both precisions.
-    const int st_mode = scalar_tiled_mode();
-    if (use_tiled_spmv() && (st_mode == 2 || (st_mode == 1 && !mixed)) && scalar_tiled_fits(m, mixed)) {
+    // The tiled kernel (TMA-staged tiles of rows) replaces the others
+    // whenever its tiles fit (scalar_tile_rows): by rule, not by timing, so
+    // that the choice and the iterates repeat from run to run; only its ring
+    // depth is timed, which changes no result. FCU_SCALAR_TILED=0 turns it
+    // off.
+    if (use_tiled_spmv() && scalar_tiled_mode() != 0 && scalar_tile_rows(m, mixed) > 0) {
       w->tiled1[k] = true;
       int best_stages = 2;
       double tiled_ms = 1e30;
