@@ -1937,9 +1937,10 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
     if (tiled) {
       w->stages[k] = known->second[0];
     } else if (known->second[1] == 2) {
-      w->tiled1[k] = true;
+      // tile sizes are measured here, never while a graph is being captured;
+      // a matrix of the same shape whose tiles do not fit keeps the CSR kernels
+      w->tiled1[k] = scalar_tile_rows(m, mixed) > 0;
       w->stages[k] = known->second[0];
-      scalar_tile_rows(m, mixed);  // tile sizes measured here, never while a graph is being captured
     } else {
       (mixed ? w->vpr32 : w->vpr) = known->second[0];
       w->stream[k] = known->second[1] != 0;
