@@ -185,8 +185,13 @@ struct fcu_matrix_s {
   bool missing_diag = false;  // a wrapped block row without a diagonal block
   DBuf<int> rowblk;     // row blocks of the CSR-stream SpMV (scalar, built on first use)
   int nrowblk = 0;
-  int tile_cap1[5] = {0, 0, 0, 0, 0};  // scalar tiled SpMV: most entries in a tile of 32, 64, 128, 256, 512 rows
-  int tile_tr1[2] = {-1, -1};          // scalar tiled SpMV: rows per tile (FP64, FP32), 0 = does not fit
+  // scalar tiled SpMV, per precision (FP64, FP32): tile row bounds, their
+  // count, the most rows (TR) and entries (cap) a tile may hold; TR = -1 not
+  // yet built, 0 = the tiled kernel does not fit this matrix
+  DBuf<int> tblk[2];
+  int ntblk[2] = {0, 0};
+  int tblk_tr[2] = {-1, -1};
+  int tblk_cap[2] = {0, 0};
   Workspace* ws = nullptr;
   BatchWorkspace* bws = nullptr;
   ~fcu_matrix_s();

@@ -461,6 +461,8 @@ struct TileHeader {
   int rows;      // rows in the tile
   int col_off;   // byte offset of ci[b0] inside the staged column region
   int val_off;   // byte offset of val[9*b0] inside the staged value region
+  int r0;        // first row of the tile
+  int rp_off;    // row pointers staged from rp[r0 - rp_off] (16-byte aligned copy)
 };
 
 __host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
@@ -503,10 +505,11 @@ struct EmitApOwn {
 // predecessor's tail; the producer warp's lanes fetch the row-pointer bounds
 // of the CTA's next 32 tiles in one round of loads. Returns false, having
 // computed nothing, when the solver state says the solve is over.
-template <bool DIFF, class T, int TR, int BS, class GX, class Emit>
+template <bool DIFF, class T, int TR, int BS, bool BLK, class GX, class Emit>
 __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int* __restrict__ ci,
                                            const T* __restrict__ val, i64 nrows, int cap_blocks, int nstage,
-                                           const GX& gx, Emit& emit, CgState* st) {
+                                           const int* __restrict__ tb, i64 ntb, const GX& gx, Emit& emit,
+                                           CgState* st) {
   extern __shared__ __align__(128) unsigned char tile_smem[];
   __shared__ unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
   constexpr int LPR = 32 * SPMV_CONSUMER_WARPS / TR;  // consumer lanes per block row
@@ -514,7 +517,9 @@ __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int
   static_assert(BS == 1 || BS == 3, "block size");
   static_assert(BS == 1 ? (LPR >= 1 && LPR <= 16) : (LPR == 8 || LPR == 16), "tile rows");
   const size_t stage_bytes = tile_stage_bytes<T, TR, BS>(cap_blocks);
-  const i64 ntiles = (nrows + TR - 1) / TR;
+  // tiles: TR consecutive rows each, or (BLK) the ntb row ranges
+  // [tb[t], tb[t + 1]) of at most TR rows and cap_blocks entries
+  const i64 ntiles = BLK ? ntb : (nrows + TR - 1) / TR;
   const i64 G = gridDim.x;
   const int mytiles = blockIdx.x < ntiles ? (int)((ntiles - blockIdx.x + G - 1) / G) : 0;
   const int tid = threadIdx.x;
@@ -528,18 +533,28 @@ __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int
   }
   __syncthreads();
 
-  // producer (warp 0): lane j holds the block bounds of tile k0 + j
-  int pb0 = 0, pb1 = 0;
+  // producer (warp 0): lane j holds the row and block bounds of tile k0 + j
+  int pb0 = 0, pb1 = 0, pr0 = 0, pr1 = 0;
   auto load_desc = [&](int k0) {
     const i64 t = blockIdx.x + (i64)(k0 + lane) * G;
     if (t < ntiles) {
-      const i64 r0 = t * TR;
+      const i64 r0 = BLK ? (i64)tb[t] : t * TR;
+      const i64 r1 = BLK ? (i64)tb[t + 1] : min(r0 + TR, nrows);
+      if (BLK) {
+        pr0 = (int)r0;
+        pr1 = (int)r1;
+      }
       pb0 = rp[r0];
-      pb1 = rp[min(r0 + TR, nrows)];
+      pb1 = rp[r1];
     }
   };
   auto issue = [&](int k) {
     const int b0 = __shfl_sync(FULL, pb0, k & 31), b1 = __shfl_sync(FULL, pb1, k & 31);
+    int tr0 = 0, tr1 = 0;
+    if constexpr (BLK) {
+      tr0 = __shfl_sync(FULL, pr0, k & 31);
+      tr1 = __shfl_sync(FULL, pr1, k & 31);
+    }
     if (lane == 0) {
       const int s = k % nstage;
       unsigned char* base = tile_smem + s * stage_bytes;
@@ -547,21 +562,26 @@ __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int
       unsigned char* rps = base + align128(sizeof(TileHeader));
       unsigned char* cs = rps + align128((TR + 1) * 4 + 16);
       unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
-      const i64 r0 = (blockIdx.x + (i64)k * G) * TR;
-      const int rows = (int)min((i64)TR, nrows - r0);
-      const unsigned rp_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);
+      const i64 r0 = BLK ? (i64)tr0 : (blockIdx.x + (i64)k * G) * TR;
+      const int rows = BLK ? tr1 - tr0 : (int)min((i64)TR, nrows - r0);
+      const int rp_off = BLK ? (int)(r0 & 3) : 0;  // rp + r0 - rp_off is 16-byte aligned
+      const unsigned rp_bytes = (unsigned)(((rows + 1 + rp_off) * 4 + 15) & ~15);
       const uintptr_t c_lo = reinterpret_cast<uintptr_t>(ci + b0) & ~(uintptr_t)15;
       const uintptr_t c_hi = (reinterpret_cast<uintptr_t>(ci + b1) + 15) & ~(uintptr_t)15;
       const uintptr_t v_lo = reinterpret_cast<uintptr_t>(val + VPB * (i64)b0) & ~(uintptr_t)15;
       const uintptr_t v_hi = (reinterpret_cast<uintptr_t>(val + VPB * (i64)b1) + 15) & ~(uintptr_t)15;
       h->b0 = b0;
       h->rows = rows;
+      if (BLK) {
+        h->r0 = (int)r0;
+        h->rp_off = rp_off;
+      }
       h->col_off = (int)(reinterpret_cast<uintptr_t>(ci + b0) - c_lo);
       h->val_off = (int)(reinterpret_cast<uintptr_t>(val + VPB * (i64)b0) - v_lo);
       const unsigned cb = (unsigned)(c_hi - c_lo), vb = (unsigned)(v_hi - v_lo);
       fence_proxy_async();
       mbar_arrive_expect_tx(&full[s], rp_bytes + cb + vb);
-      bulk_load(rps, rp + r0, rp_bytes, &full[s]);
+      bulk_load(rps, rp + (r0 - rp_off), rp_bytes, &full[s]);
       if (cb) bulk_load(cs, reinterpret_cast<const void*>(c_lo), cb, &full[s]);
       if (vb) bulk_load(vs, reinterpret_cast<const void*>(v_lo), vb, &full[s]);
     }
@@ -611,13 +631,13 @@ __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int
     }
     unsigned char* base = tile_smem + s * stage_bytes;
     const TileHeader* h = reinterpret_cast<const TileHeader*>(base);
-    const int* rps = reinterpret_cast<const int*>(base + align128(sizeof(TileHeader)));
+    const int* rps = reinterpret_cast<const int*>(base + align128(sizeof(TileHeader))) + (BLK ? h->rp_off : 0);
     const unsigned char* cs = base + align128(sizeof(TileHeader)) + align128((TR + 1) * 4 + 16);
     const unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
     const int* cis = reinterpret_cast<const int*>(cs + h->col_off);
     const T* vls = reinterpret_cast<const T*>(vs + h->val_off);
     const int b0 = h->b0;
-    const i64 row = (blockIdx.x + (i64)k * G) * TR + row_in_tile;
+    const i64 row = BLK ? (i64)h->r0 + row_in_tile : (blockIdx.x + (i64)k * G) * TR + row_in_tile;
     const bool valid = row_in_tile < h->rows;
     if constexpr (BS == 1) {
       // scalar row: lane `sub` sums entries sub, sub + LPR, ... (difference
@@ -683,10 +703,12 @@ __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int
 template <int DIFF, class T, int TR, int BS = 3>
 __global__ void __launch_bounds__(SPMV_THREADS)
     k_spmv_tiled(const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val, i64 nrows,
-                 int cap_blocks, int nstage, const T* __restrict__ p, T* __restrict__ ap, CgState* st,
-                 double* partials) {
+                 int cap_blocks, int nstage, const int* __restrict__ tb, i64 ntb, const T* __restrict__ p,
+                 T* __restrict__ ap, CgState* st, double* partials) {
   EmitApOwn<T, BS> em{ap};
-  if (!tiled_rows<DIFF != 0, T, TR, BS>(rp, ci, val, nrows, cap_blocks, nstage, XPlain<T>{p}, em, st)) return;
+  if (!tiled_rows<DIFF != 0, T, TR, BS, BS == 1>(rp, ci, val, nrows, cap_blocks, nstage, tb, ntb, XPlain<T>{p}, em,
+                                                 st))
+    return;
   store_pap_partial(em.dot, partials);
 }
 
@@ -1359,63 +1381,52 @@ size_t scalar_stage_bytes(size_t value_bytes, int tr, int cap) {
 
 int max_block_row(fcu_matrix m) { return m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32); }
 
-__global__ void k_tile_cap(const int* __restrict__ rp, i64 nrows, int tr, int* __restrict__ cap) {
-  const i64 ntiles = (nrows + tr - 1) / tr;
-  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < ntiles; t += (i64)gridDim.x * blockDim.x) {
-    const i64 r0 = t * tr, r1 = std::min<i64>(r0 + tr, nrows);
-    atomicMax(cap, rp[r1] - rp[r0]);
-  }
-}
-
-int tile_slot(int tr) { return tr == 32 ? 0 : tr == 64 ? 1 : tr == 128 ? 2 : tr == 256 ? 3 : 4; }
-
-// Most entries in one tile of `tr` rows (scalar CSR), computed once per matrix
-// (never while a graph is being captured).
-int scalar_tile_cap(fcu_matrix m, int tr) {
-  const int slot = tile_slot(tr);
-  if (m->tile_cap1[slot] > 0) return m->tile_cap1[slot];
+// Rows per tile of the scalar tiled SpMV (TR), or 0 when it does not fit.
+// TR = 512 / lanes per row, the lanes chosen by mean row length (1 up to 12
+// entries, 2 up to 24, 4 up to 48, else 8). Tiles are row ranges of at most
+// TR rows and at most `cap` entries, cut greedily, with cap as large as two
+// ring stages of two CTAs per SM allow: every tile then carries about as
+// many bytes as the ring holds, which amortises its one round trip of
+// operand gathers (a matrix whose longest row exceeds cap does not fit).
+// Built once per matrix and precision, never while a graph is captured.
+int scalar_tile_rows(fcu_matrix m, bool f32) {
+  const int k = f32 ? 1 : 0;
+  if (m->tblk_tr[k] >= 0) return m->tblk_tr[k];
   fcu_ctx ctx = m->ctx;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   CUDA_CHECK(cudaStreamIsCapturing(ctx->stream, &cs));
-  if (cs != cudaStreamCaptureStatusNone) fail(FCU_ERR_CUDA, "tile sizes of the scalar tiled SpMV requested during capture");
-  DBuf<int> cap;
-  cap.alloc(1);
-  CUDA_CHECK(cudaMemsetAsync(cap.p, 0, sizeof(int), ctx->stream));
-  const i64 ntiles = (m->nnodes + tr - 1) / tr;
-  k_tile_cap<<<grid_for(std::max<i64>(ntiles, 1), 256, ctx->num_sms * 4), 256, 0, ctx->stream>>>(m->row_ptr, m->nnodes,
-                                                                                                 tr, cap.p);
-  LAUNCH_CHECK(ctx);
-  int h = 0;
-  CUDA_CHECK(cudaMemcpyAsync(&h, cap.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-  m->tile_cap1[slot] = std::max(h, 1);
-  return m->tile_cap1[slot];
-}
-
-// Rows per tile of the scalar tiled SpMV, or 0 when it does not fit: the
-// tallest of 512, 256, 128, 64, 32 rows whose ring (two stages of the
-// largest tile, TILED_CTAS_PER_SM CTAs per SM) fits in shared memory. A
-// tile's 512 consumer lanes share its rows (512 / TR lanes per row), and the
-// bytes a tile carries amortise its one round trip of operand gathers, so
-// taller tiles are faster. FP32 takes only 512-row tiles: shorter ones ran
-// slower than the CSR-stream kernel. Computed once per matrix and precision.
-int scalar_tile_rows(fcu_matrix m, bool f32) {
-  int& tr = m->tile_tr1[f32 ? 1 : 0];
-  if (tr >= 0) return tr;
-  fcu_ctx ctx = m->ctx;
+  if (cs != cudaStreamCaptureStatusNone) fail(FCU_ERR_CUDA, "tiles of the scalar tiled SpMV requested during capture");
+  m->tblk_tr[k] = 0;
+  if (m->nnodes <= 0) return 0;
+  const double mean = (double)m->nnzb / (double)m->nnodes;
+  const int lpr = mean <= 12.0 ? 1 : mean <= 24.0 ? 2 : mean <= 48.0 ? 4 : 8;
+  const int tr = 512 / lpr;
   int optin = 0, per_sm_max = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
   CUDA_CHECK(cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-  tr = 0;
-  for (int t : {512, 256, 128, 64, 32}) {
-    if (f32 && t != 512) break;
-    if ((i64)t > 2 * std::max<i64>(m->nnodes, 1) && t > 32) continue;  // tiles far taller than the matrix
-    const size_t stage = scalar_stage_bytes(f32 ? 4 : 8, t, scalar_tile_cap(m, t));
-    if (2 * stage + 1024 <= (size_t)optin && TILED_CTAS_PER_SM * (2 * stage + 2048) <= (size_t)per_sm_max) {
-      tr = t;
-      break;
-    }
+  const size_t budget = std::min((size_t)optin - 1024, (size_t)per_sm_max / TILED_CTAS_PER_SM - 2048) / 2;
+  const size_t wv = f32 ? 4 : 8;
+  int cap = (int)((budget - scalar_stage_bytes(wv, tr, 0)) / (4 + wv)) - 64;
+  while (cap > 0 && scalar_stage_bytes(wv, tr, cap) > budget) cap -= 16;
+  if (cap <= 0) return 0;
+  std::vector<int> rp(m->nnodes + 1);
+  CUDA_CHECK(cudaMemcpyAsync(rp.data(), m->row_ptr, (m->nnodes + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  std::vector<int> b;
+  b.push_back(0);
+  for (i64 r = 0; r < m->nnodes;) {
+    if (rp[r + 1] - rp[r] > cap) return 0;  // a row longer than a tile holds
+    i64 e = r;
+    while (e < m->nnodes && e - r < tr && (i64)rp[e + 1] - rp[r] <= cap) ++e;
+    b.push_back((int)e);
+    r = e;
   }
+  m->ntblk[k] = (int)b.size() - 1;
+  upload(ctx, m->tblk[k], b.data(), b.size());
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  m->tblk_cap[k] = cap;
+  m->tblk_tr[k] = tr;
   return tr;
 }
 
@@ -1435,7 +1446,10 @@ int fitted_stages(fcu_ctx ctx, int requested, size_t stage) {
 template <int DIFF, class T, int TR, int BS = 3>
 int launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
   fcu_ctx ctx = m->ctx;
-  const int cap = BS == 3 ? TR * max_block_row(m) : scalar_tile_cap(m, TR);
+  const int kp = sizeof(T) == 4 ? 1 : 0;
+  const int cap = BS == 3 ? TR * max_block_row(m) : m->tblk_cap[kp];
+  const int* tb = BS == 3 ? nullptr : m->tblk[kp].p;
+  const i64 ntb = BS == 3 ? 0 : m->ntblk[kp];
   const size_t stage = tile_stage_bytes<T, TR, BS>(cap);
   const int nstage = fitted_stages(ctx, w->stages[sizeof(T) == 4 ? 1 : 0], stage);
   const size_t smem = nstage * stage;
@@ -1453,11 +1467,11 @@ int launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T
   // The grid sets the order in which p.Ap is reduced, so it does not follow
   // the ring depth: TILED_CTAS_PER_SM CTAs per SM whenever they fit, which
   // keeps the iterates identical for every depth the tuner may pick.
-  const i64 ntiles = (m->nnodes + TR - 1) / TR;
+  const i64 ntiles = BS == 3 ? (m->nnodes + TR - 1) / TR : ntb;
   const int grid =
       (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)std::min(per_sm, TILED_CTAS_PER_SM) * ctx->num_sms));
-  launch_pdl_cfg(ctx, kern, grid, SPMV_THREADS, smem, m->row_ptr, m->col_idx, val, m->nnodes, cap, nstage, p, ap,
-                 w->st.p, w->partials.p);
+  launch_pdl_cfg(ctx, kern, grid, SPMV_THREADS, smem, m->row_ptr, m->col_idx, val, m->nnodes, cap, nstage, tb, ntb,
+                 p, ap, w->st.p, w->partials.p);
   return grid;
 }
 
