@@ -1382,8 +1382,8 @@ size_t scalar_stage_bytes(size_t value_bytes, int tr, int cap) {
 int max_block_row(fcu_matrix m) { return m->space ? m->space->max_row : (m->max_row_own ? m->max_row_own : 32); }
 
 // Rows per tile of the scalar tiled SpMV (TR), or 0 when it does not fit.
-// TR = 512 / lanes per row, the lanes chosen by mean row length (1 up to 12
-// entries, 2 up to 24, 4 up to 48, else 8). Tiles are row ranges of at most
+// TR = 512 / lanes per row, the lanes chosen by mean row length (1 up to 16
+// entries, 2 up to 32, 4 up to 64, else 8: about 7-16 entries per lane). Tiles are row ranges of at most
 // TR rows and at most `cap` entries, cut greedily, with cap as large as two
 // ring stages of two CTAs per SM allow: every tile then carries about as
 // many bytes as the ring holds, which amortises its one round trip of
@@ -1399,7 +1399,7 @@ int scalar_tile_rows(fcu_matrix m, bool f32) {
   m->tblk_tr[k] = 0;
   if (m->nnodes <= 0) return 0;
   const double mean = (double)m->nnzb / (double)m->nnodes;
-  const int lpr = mean <= 12.0 ? 1 : mean <= 24.0 ? 2 : mean <= 48.0 ? 4 : 8;
+  const int lpr = mean <= 16.0 ? 1 : mean <= 32.0 ? 2 : mean <= 64.0 ? 4 : 8;
   const int tr = 512 / lpr;
   int optin = 0, per_sm_max = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
