@@ -400,9 +400,10 @@ __global__ void __launch_bounds__(VBLOCK) k_direction(i64 n, T* __restrict__ p, 
 }
 
 // --- block and scalar SpMV with TMA-staged tiles --------------------------------
-// (3x3-block CSR, and scalar CSR in FP64, where each stored "block" is one
-// entry and 2-16 lanes share a row.)
-// A persistent CTA walks tiles of TR consecutive block rows. One thread streams
+// (3x3-block CSR with tiles of TR consecutive block rows; scalar CSR, where
+// each stored "block" is one entry and 1-8 lanes share a row, with tiles
+// that are row ranges cut to an entry budget, listed per matrix.)
+// A persistent CTA walks its tiles in turn. One thread streams
 // each tile's row pointers, column indices and block values into shared memory
 // with bulk asynchronous copies (cp.async.bulk, completion counted on an
 // mbarrier), two stages deep, while the CTA's warps compute the previous tile
