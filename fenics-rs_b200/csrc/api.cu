@@ -346,6 +346,7 @@ void ctx_release(fcu_ctx c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   c->temp.release();
+  for (void* p : c->pinned_pool) cudaFreeHost(p);
   cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -104,6 +104,10 @@ struct fcu_ctx_s {
   // stored blocks, longest row, precision): a later matrix of the same shape
   // (a new solve on the same mesh) takes them without timing candidates.
   std::map<std::array<i64, 5>, std::array<int, 2>> spmv_tune;
+  // Pinned solver state records of released matrices, reused by later ones
+  // (pinned allocation and release are slow and synchronising), freed with
+  // the context.
+  std::vector<void*> pinned_pool;
   unsigned char* temp_bytes(size_t b) {
     if (temp.n < b) temp.alloc(b);
     return temp.p;

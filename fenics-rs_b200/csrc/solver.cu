@@ -1174,6 +1174,7 @@ void build_row_blocks(fcu_ctx ctx, const int* rp_dev, i64 nrows, DBuf<int>& rb, 
 // ---------------------------------------------------------------------------
 
 struct Workspace {
+  fcu_ctx ctx = nullptr;
   i64 n = 0;
   DBuf<double> x, r, b, invd, partials;
   DBuf<double> z64, pa64, pb64, ap64;  // FP64 path: z, p (two buffers), Ap
@@ -1195,7 +1196,10 @@ struct Workspace {
       if (g) cudaGraphExecDestroy(g);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
-    if (host_st) cudaFreeHost(host_st);
+    if (host_st) {
+      if (ctx) ctx->pinned_pool.push_back(host_st);
+      else cudaFreeHost(host_st);
+    }
   }
 };
 
@@ -1292,7 +1296,13 @@ Workspace* ensure_ws(fcu_matrix m, bool mixed) {
     w->partials.alloc(PARTIAL_REGIONS * MAXG);
     w->st.alloc(1);
     CUDA_CHECK(cudaMemsetAsync(w->st.p, 0, sizeof(CgState), ctx->stream));
-    CUDA_CHECK(cudaMallocHost(&w->host_st, 2 * sizeof(CgState)));
+    w->ctx = ctx;
+    if (!ctx->pinned_pool.empty()) {
+      w->host_st = static_cast<CgState*>(ctx->pinned_pool.back());
+      ctx->pinned_pool.pop_back();
+    } else {
+      CUDA_CHECK(cudaMallocHost(&w->host_st, 2 * sizeof(CgState)));
+    }
     for (auto& e : w->ev) CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     w->vpr = pick_vpr(m);
     w->vpr32 = w->vpr;
