@@ -191,8 +191,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
         // stage element rows of contributions ch .. ch+31
         const int t = ch + lane;
         int a_own = 0;
+        // P2 rows of more than 32 slots (vertex rows) with at most 32
+        // contributions reuse the element rows staged by the first slot group
+        const bool restage = !(IS_P2 && g0 > 0 && nct <= 32);
         if (IS_P2) {
-          if (t < nct) {
+          if (restage && t < nct) {
             int cc = contrib[cs + t];
             const double2* g = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
 #pragma unroll
@@ -204,7 +207,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
             sa_all[wib][lane] = cc & 15;
           }
           __syncwarp();
-          const int nt = min(32, nct - ch);
+          const int nt = restage ? min(32, nct - ch) : 0;
           for (int q = lane; q < nt * K; q += 32) {
             const int tt = q / K, b = q - tt * K;
             const int a = sa_all[wib][tt];
