@@ -144,6 +144,17 @@ __global__ void k_p2_metric_records(const int* __restrict__ cn, const double* __
   }
 }
 
+// Header of a row-gather row, spread over the warp: lane k < 5 holds
+// row_ptr[row], row_ptr[row + 1], contrib_ptr[row], contrib_ptr[row + 1],
+// diag_pos[row] (read back with shuffles). The kernels fetch the next row's
+// header while they sum the current row.
+__device__ __forceinline__ int row_header(const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr,
+                                          const int* __restrict__ diag_pos, i64 row, i64 nrows, int lane) {
+  if (row >= nrows || lane >= 5) return 0;
+  const int* src = lane < 2 ? row_ptr : lane < 4 ? contrib_ptr : diag_pos;
+  return src[row + (lane == 1 || lane == 3 ? 1 : 0)];
+}
+
 template <int K, int DIM, bool IS_P2>
 __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
@@ -164,11 +175,18 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
   }
   double(*stage)[KS] = stage_all[wib];
   const i64 nwarps = (i64)gridDim.x * WARPS;
-  for (i64 row = (i64)blockIdx.x * WARPS + wib; row < nrows; row += nwarps) {
-    const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
-    const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
+  const i64 row0 = (i64)blockIdx.x * WARPS + wib;
+  int hdr = row_header(row_ptr, contrib_ptr, diag_pos, row0, nrows, lane);
+  for (i64 row = row0; row < nrows; row += nwarps) {
+    const int rs = __shfl_sync(FULL, hdr, 0), L = __shfl_sync(FULL, hdr, 1) - rs;
+    const int cs = __shfl_sync(FULL, hdr, 2), nct = __shfl_sync(FULL, hdr, 3) - cs;
+    const int dl = __shfl_sync(FULL, hdr, 4) - rs;  // slot of the diagonal
+    hdr = row_header(row_ptr, contrib_ptr, diag_pos, row + nwarps, nrows, lane);
     const i64 ebase = (i64)K * cs;
-    const int dl = diag_pos[row] - rs;  // slot of the diagonal
+    // the first group's slot counts and the first chunk's contributions are
+    // fetched together with the entry list
+    const int cnt_first = lane < L ? (int)slot_cnt[rs + lane] : 0;
+    const int cc_first = lane < nct ? contrib[cs + lane] : 0;
     // The row's (contribution, column) entry list, staged once per row with a
     // coalesced copy when it fits (at most 32 contributions).
     const bool staged = nct <= 32;
@@ -178,7 +196,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
     int run = 0;  // entries consumed by earlier slot groups
     for (int g0 = 0; g0 < L; g0 += 32) {
       const int s = g0 + lane;
-      const int cnt = (s < L) ? (int)slot_cnt[rs + s] : 0;
+      const int cnt = g0 == 0 ? cnt_first : (s < L) ? (int)slot_cnt[rs + s] : 0;
       int tot;
       const int off = warp_excl_scan(cnt, lane, &tot);
       i64 e = ebase + run + off;
@@ -196,7 +214,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
         const bool restage = !(IS_P2 && g0 > 0 && nct <= 32);
         if (IS_P2) {
           if (restage && t < nct) {
-            int cc = contrib[cs + t];
+            const int cc = ch == 0 ? cc_first : contrib[cs + t];
             const double2* g = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
@@ -219,7 +237,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_scalar(
           }
         } else {
           if (t < nct) {
-            int cc = contrib[cs + t];
+            const int cc = ch == 0 ? cc_first : contrib[cs + t];
             a_own = cc & 15;
             p1_element_row<K, DIM>(X, cn, cc >> 4, cc & 15, coef ? coef[cc >> 4] : 1.0, stage[lane]);
           }
@@ -269,11 +287,16 @@ __global__ void __launch_bounds__(EWARPS * 32, 4) k_assemble_elasticity(
   double(*st)[17] = st_all[wib];
   double* out = out_all[wib];
   const i64 nwarps = (i64)gridDim.x * EWARPS;
-  for (i64 row = (i64)blockIdx.x * EWARPS + wib; row < nrows; row += nwarps) {
-    const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
-    const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
+  const i64 row0 = (i64)blockIdx.x * EWARPS + wib;
+  int hdr = row_header(row_ptr, contrib_ptr, diag_pos, row0, nrows, lane);
+  for (i64 row = row0; row < nrows; row += nwarps) {
+    const int rs = __shfl_sync(FULL, hdr, 0), L = __shfl_sync(FULL, hdr, 1) - rs;
+    const int cs = __shfl_sync(FULL, hdr, 2), nct = __shfl_sync(FULL, hdr, 3) - cs;
+    const int dl = __shfl_sync(FULL, hdr, 4) - rs;
+    hdr = row_header(row_ptr, contrib_ptr, diag_pos, row + nwarps, nrows, lane);
     const i64 ebase = 4 * (i64)cs;
-    const int dl = diag_pos[row] - rs;
+    const int cnt_first = lane < L ? (int)slot_cnt[rs + lane] : 0;
+    const int cc_first = lane < nct ? contrib[cs + lane] : 0;
     const bool staged = nct <= 32;
     if (staged)
       for (int q = lane; q < 4 * nct; q += 32) ent_all[wib][q] = slot_ent[ebase + q];
@@ -281,7 +304,7 @@ __global__ void __launch_bounds__(EWARPS * 32, 4) k_assemble_elasticity(
     int run = 0;
     for (int g0 = 0; g0 < L; g0 += 32) {
       const int s = g0 + lane;
-      const int cnt = (s < L) ? (int)slot_cnt[rs + s] : 0;
+      const int cnt = g0 == 0 ? cnt_first : (s < L) ? (int)slot_cnt[rs + s] : 0;
       int tot;
       const int off = warp_excl_scan(cnt, lane, &tot);
       i64 e = ebase + run + off;
@@ -296,7 +319,7 @@ __global__ void __launch_bounds__(EWARPS * 32, 4) k_assemble_elasticity(
         const int t = ch + lane;
         int a_own = 0;
         if (t < nct) {
-          const int cc = contrib[cs + t];
+          const int cc = ch == 0 ? cc_first : contrib[cs + t];
           const int c = cc >> 4, a = cc & 15;
           a_own = a;
           int v[4];
@@ -400,11 +423,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
   __shared__ unsigned short ent_all[WARPS][32 * K];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const i64 nwarps = (i64)gridDim.x * WARPS;
-  for (i64 row = (i64)blockIdx.x * WARPS + wib; row < nrows; row += nwarps) {
-    const int rs = row_ptr[row], L = row_ptr[row + 1] - rs;
-    const int cs = contrib_ptr[row], nct = contrib_ptr[row + 1] - cs;
+  const i64 row0 = (i64)blockIdx.x * WARPS + wib;
+  int hdr = row_header(row_ptr, contrib_ptr, diag_pos, row0, nrows, lane);
+  for (i64 row = row0; row < nrows; row += nwarps) {
+    const int rs = __shfl_sync(FULL, hdr, 0), L = __shfl_sync(FULL, hdr, 1) - rs;
+    const int cs = __shfl_sync(FULL, hdr, 2), nct = __shfl_sync(FULL, hdr, 3) - cs;
+    const int dl = __shfl_sync(FULL, hdr, 4) - rs;
+    hdr = row_header(row_ptr, contrib_ptr, diag_pos, row + nwarps, nrows, lane);
     const i64 ebase = (i64)K * cs;
-    const int dl = diag_pos[row] - rs;
+    const int cnt_first = lane < L ? (int)slot_cnt[rs + lane] : 0;
+    const int cc_first = lane < nct ? contrib[cs + lane] : 0;
     const bool staged = nct <= 32;
     if (staged)
       for (int q = lane; q < K * nct; q += 32) ent_all[wib][q] = slot_ent[ebase + q];
@@ -412,7 +440,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
     int run = 0;
     for (int g0 = 0; g0 < L; g0 += 32) {
       const int s = g0 + lane;
-      const int cnt = (s < L) ? (int)slot_cnt[rs + s] : 0;
+      const int cnt = g0 == 0 ? cnt_first : (s < L) ? (int)slot_cnt[rs + s] : 0;
       int tot;
       const int off = warp_excl_scan(cnt, lane, &tot);
       i64 e = ebase + run + off;
@@ -424,7 +452,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_assemble_mass(
       for (int ch = 0; ch < nct; ch += 32) {
         const int t = ch + lane;
         if (t < nct) {
-          const int cc = contrib[cs + t];
+          const int cc = ch == 0 ? cc_first : contrib[cs + t];
           const int c = cc >> 4;
           int v[DIM + 1];
 #pragma unroll
