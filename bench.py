@@ -674,7 +674,7 @@ def run_reference(args, cfg):
     }
 
 
-PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5")
+PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5", "p2_cube40")
 
 
 def profile_case(name):
@@ -688,7 +688,10 @@ def profile_case(name):
       batch_c5         the C5 batch of 256 Poisson problems, mixed PCG capped
                        at 60 iterations per instance, 3 launches of the
                        persistent batch kernel (shape fixed by FCU_BATCH_* if
-                       set, else tuned first)"""
+                       set, else tuned first)
+      p2_cube40        P2 stiffness on the unit cube 40^3 x 6 tets (384,000
+                       cells, 531,441 dofs), random kappa, assembled 3 times
+                       (the C3 kernel on a quarter of its cells)"""
     import torch
     import fenics_cuda as fcu
     ctx = fcu.Context(0)
@@ -710,6 +713,15 @@ def profile_case(name):
             M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
             M.block_jacobi(True)
             M.pcg(b, tol=1e-30, max_iter=12, raise_on_error=False)
+        ctx.synchronize()
+        M.close(); V.close()
+    elif name == "p2_cube40":
+        mesh = fcu.unit_cube(40, 40, 40)
+        kap = np.exp(np.random.default_rng(3).standard_normal(mesh.nc))
+        V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P2)
+        M = fcu.Matrix(ctx, V)
+        for _ in range(3):
+            M.assemble_stiffness(kap)
         ctx.synchronize()
         M.close(); V.close()
     elif name == "batch_c5":
