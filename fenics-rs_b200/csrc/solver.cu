@@ -388,15 +388,33 @@ __global__ void __launch_bounds__(VBLOCK) k_spmv_ap(const int* __restrict__ rp, 
   store_pap_partial(em.dot, partials);
 }
 
-// p = z + beta p (in place), for the unfused iteration.
+// p = z + beta p (in place), for the unfused iteration. FP32 directions go
+// four floats per load when both arrays are 16-byte aligned (on the
+// 421,443-dof elasticity system: 34.65 -> 34.05 us per mixed iteration; two
+// doubles per load made the FP64 iteration 0.8% slower, so FP64 keeps one
+// element per load); the arithmetic per element is the same either way.
+__device__ __forceinline__ float4 axpy4(float4 a, float b, float4 c) {
+  return make_float4(a.x + b * c.x, a.y + b * c.y, a.z + b * c.z, a.w + b * c.w);
+}
+
 template <class T>
 __global__ void __launch_bounds__(VBLOCK) k_direction(i64 n, T* __restrict__ p, const T* __restrict__ z,
                                                       const CgState* st) {
   grid_dep_sync();
   if (st->done || st->pause) return;
   const T beta = (T)st->beta;
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
-    p[i] = z[i] + beta * p[i];
+  const i64 t0 = blockIdx.x * (i64)blockDim.x + threadIdx.x, stride = (i64)gridDim.x * blockDim.x;
+  i64 head = 0;
+  if constexpr (sizeof(T) == 4) {
+    if (((reinterpret_cast<uintptr_t>(p) | reinterpret_cast<uintptr_t>(z)) & 15) == 0) {
+      const i64 nv = n / 4;
+      float4* pv = reinterpret_cast<float4*>(p);
+      const float4* zv = reinterpret_cast<const float4*>(z);
+      for (i64 i = t0; i < nv; i += stride) pv[i] = axpy4(zv[i], beta, pv[i]);
+      head = nv * 4;
+    }
+  }
+  for (i64 i = head + t0; i < n; i += stride) p[i] = z[i] + beta * p[i];
 }
 
 // --- block and scalar SpMV with TMA-staged tiles --------------------------------
