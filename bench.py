@@ -445,7 +445,9 @@ def run_workloads(ctx, stream, peak):
     ms_s, _ = _best_ms(stream, lambda: V.element_stresses(210e9, 0.3, x, von_mises=cvm), k=3)
     ms_v, _ = _best_ms(stream, lambda: V.vertex_von_mises(cvm, out=vvm), k=3)
     sbytes = mesh.nc * (16 + 8) + mesh.nv * (24 + 24)
-    vbytes = mesh.nc * (16 + 16 + 8) + mesh.nv * (24 + 8)
+    # vertex average: per cell its 4 contribution entries (16 B), von Mises value and cached volume
+    # (8 B each); per vertex its row bound (4 B) and the result (8 B)
+    vbytes = mesh.nc * (16 + 8 + 8) + mesh.nv * (4 + 8)
     c2p["stress_recovery"] = {
         "element_von_mises": {"ms": ms_s, "gbs": sbytes / (ms_s * 1e-3) / 1e9, "bytes": sbytes,
                               "frac_of_hbm": sbytes / (ms_s * 1e-3) / 1e9 / peak},

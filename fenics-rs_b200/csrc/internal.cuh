@@ -152,6 +152,7 @@ struct fcu_space_s {
   DBuf<unsigned short> slot_cnt;   // nnzb: contributions to each slot
   DBuf<unsigned short> slot_ent;   // k*ncontrib: (t_local << 4) | b, per slot in cell order
   DBuf<int> tpos;          // nnzb: position of the transposed entry (built on demand)
+  DBuf<double> cell_vol;   // nc: |det J| / 6 per tet (built by the first vertex average)
 };
 
 struct fcu_matrix_s {

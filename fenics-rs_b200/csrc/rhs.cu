@@ -531,21 +531,32 @@ __global__ void k_element_stresses(const double* __restrict__ X, const int* __re
   }
 }
 
+// |det J| / 6 of every tet: the weights of the vertex average, computed on a
+// space's first vertex average and kept with the space (its mesh does not
+// change), with the expression the average used per cell before.
+__global__ void k_cell_volumes(const double* __restrict__ X, const int* __restrict__ cells, i64 nc,
+                               double* __restrict__ vol) {
+  for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
+    int vv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) vv[i] = cells[4 * c + i];
+    vol[c] = (1.0 / 6.0) * fabs(tet_geometry(X, vv).det);
+  }
+}
+
 // One thread per vertex: sum over its cells in ascending order (the row's
 // contribution list) of vm * vol and vol, then the quotient (kept as the sum
 // when the volume is ~0, as the reference leaves it).
 __global__ void k_vertex_von_mises(const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
-                                   const double* __restrict__ X, const int* __restrict__ cells,
-                                   const double* __restrict__ cell_vm, i64 nv, double* __restrict__ out) {
+                                   const double* __restrict__ cell_vol, const double* __restrict__ cell_vm, i64 nv,
+                                   double* __restrict__ out) {
   for (i64 v = blockIdx.x * (i64)blockDim.x + threadIdx.x; v < nv; v += (i64)gridDim.x * blockDim.x) {
     double sv = 0.0, sw = 0.0;
-    for (int q = contrib_ptr[v]; q < contrib_ptr[v + 1]; ++q) {
+    const int q1 = contrib_ptr[v + 1];
+#pragma unroll 4
+    for (int q = contrib_ptr[v]; q < q1; ++q) {
       const int c = contrib[q] >> 4;
-      int vv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) vv[i] = cells[4 * (i64)c + i];
-      const Geo3 g3 = tet_geometry(X, vv);
-      const double vol = (1.0 / 6.0) * fabs(g3.det);
+      const double vol = cell_vol[c];
       sv += cell_vm[c] * vol;
       sw += vol;
     }
@@ -567,7 +578,13 @@ void element_stresses_impl(fcu_space s, double lam, double mu, const double* u_d
 void vertex_von_mises_impl(fcu_space s, const double* cell_vm_dev, double* out_dev) {
   fcu_mesh m = s->mesh;
   fcu_ctx ctx = m->ctx;
+  if (!s->cell_vol.p) {
+    s->cell_vol.alloc(m->nc);
+    k_cell_volumes<<<grid_for(m->nc, 128, ctx->num_sms * 16), 128, 0, ctx->stream>>>(m->coords.p, m->cells.p, m->nc,
+                                                                                     s->cell_vol.p);
+    LAUNCH_CHECK(ctx);
+  }
   k_vertex_von_mises<<<grid_for(m->nv, 128, ctx->num_sms * 16), 128, 0, ctx->stream>>>(
-      s->contrib_ptr.p, s->contrib.p, m->coords.p, m->cells.p, cell_vm_dev, m->nv, out_dev);
+      s->contrib_ptr.p, s->contrib.p, s->cell_vol.p, cell_vm_dev, m->nv, out_dev);
   LAUNCH_CHECK(ctx);
 }
