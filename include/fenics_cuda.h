@@ -369,7 +369,8 @@ int fcu_element_stresses(fcu_ctx ctx, fcu_space space, double E, double nu, cons
                          double* stress, double* strain, double* von_mises, double* trace);
 /* compute_vertex_von_mises (elasticity.rs:323-360): volume-weighted average of
  * the cells' von Mises stress at each vertex (nv), cells summed in ascending
- * order; vertices with no volume keep the (zero) sum. */
+ * order; vertices with no volume keep the (zero) sum. The first call on a
+ * space computes its cell volumes (nc doubles) and keeps them with the space. */
 int fcu_vertex_von_mises(fcu_ctx ctx, fcu_space space, const double* cell_von_mises,
                          double* vertex_von_mises);
 
