@@ -28,6 +28,7 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
             int precision, bool gpu_semantics, const double* inv_diag_dev, fcu_solve_info* info);
 void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev);
 void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes);
+void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_bytes, double* ms, double* bytes);
 int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
                    i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
                    fcu_solve_info* info, const int* fixed_shape = nullptr);
@@ -482,6 +483,64 @@ int fcu_ctx_synchronize(fcu_ctx ctx) {
 void* fcu_ctx_stream(fcu_ctx ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int64_t fcu_ctx_kernel_launches(fcu_ctx ctx) { return ctx ? ctx->launches : 0; }
+
+// ---------------------------------------------------------------------------
+// device buffers and devices
+// ---------------------------------------------------------------------------
+
+int fcu_buffer_alloc(fcu_ctx ctx, size_t bytes, void** out) {
+  if (!out) return FCU_ERR_BAD_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    check_ctx(ctx);
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes ? bytes : 1, ctx->stream);
+    if (e != cudaSuccess) fail(FCU_ERR_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    *out = p;
+  });
+}
+
+int fcu_buffer_free(fcu_ctx ctx, void* p) {
+  return guarded(ctx, [&] {
+    check_ctx(ctx);
+    if (p) CUDA_CHECK(cudaFreeAsync(p, ctx->stream));
+  });
+}
+
+int fcu_buffer_copy(fcu_ctx ctx, void* dst, const void* src, size_t bytes) {
+  return guarded(ctx, [&] {
+    check_ctx(ctx);
+    if (!bytes) return;
+    if (!dst || !src) fail(FCU_ERR_BAD_ARG, "null copy argument");
+    CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+    if (!is_device_ptr(dst) || !is_device_ptr(src)) sync(ctx);
+  });
+}
+
+int fcu_buffer_memset(fcu_ctx ctx, void* p, int value, size_t bytes) {
+  return guarded(ctx, [&] {
+    check_ctx(ctx);
+    if (!bytes) return;
+    if (!p || !is_device_ptr(p)) fail(FCU_ERR_BAD_ARG, "memset target is not device memory");
+    CUDA_CHECK(cudaMemsetAsync(p, value, bytes, ctx->stream));
+  });
+}
+
+int fcu_device_count(int* count) {
+  if (!count) return FCU_ERR_BAD_ARG;
+  *count = 0;
+  return guarded(nullptr, [&] { CUDA_CHECK(cudaGetDeviceCount(count)); });
+}
+
+int fcu_device_name(int device, char* name, size_t len) {
+  if (!name || !len) return FCU_ERR_BAD_ARG;
+  return guarded(nullptr, [&] {
+    cudaDeviceProp prop;
+    CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
+    std::strncpy(name, prop.name, len - 1);
+    name[len - 1] = 0;
+  });
+}
 
 // ---------------------------------------------------------------------------
 // meshes
@@ -1431,6 +1490,16 @@ int fcu_time_spmv(fcu_ctx ctx, fcu_matrix m, int precision, int reps, double* ms
     if (!m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
     if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
     time_spmv_impl(m, precision, reps, ms_per_launch, bytes_per_launch);
+  });
+}
+
+int fcu_time_spmv_cold(fcu_ctx ctx, fcu_matrix m, int precision, int reps, size_t flush_bytes,
+                       double* ms_per_launch, double* bytes_per_launch) {
+  return guarded(ctx, [&] {
+    if (!m || !ms_per_launch || !bytes_per_launch || reps < 0) fail(FCU_ERR_BAD_ARG, "bad arguments");
+    if (!m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
+    time_spmv_cold_impl(m, precision, reps, flush_bytes, ms_per_launch, bytes_per_launch);
   });
 }
 

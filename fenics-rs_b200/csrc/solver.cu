@@ -2085,6 +2085,42 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
   *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
 }
 
+// The same with L2 flushed before each launch: a memset of `flush_bytes`
+// evicts the matrix and p, then one SpMV is timed by events on either side.
+// The memset is queued before the first event, so the launch never waits on
+// the host. Returns the mean single-launch time.
+void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_bytes, double* ms, double* bytes) {
+  const bool mixed = precision == FCU_MIXED;
+  Workspace* w = ensure_ws(m, mixed);
+  if (mixed) build_rowsum32(m);
+  tune_spmv(m, w, mixed);
+  spmv_timing_state(m, w, mixed);
+  fcu_ctx ctx = m->ctx;
+  if (!flush_bytes) flush_bytes = 256ull << 20;
+  DBuf<unsigned char> flush;
+  flush.alloc(flush_bytes);
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  double total = 0.0;
+  for (int r = 0; r < reps; ++r) {
+    CUDA_CHECK(cudaMemsetAsync(flush.p, r & 0xff, flush_bytes, ctx->stream));
+    CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+    enqueue_spmv(m, w, mixed);
+    CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+    CUDA_CHECK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CUDA_CHECK(cudaEventElapsedTime(&t, e0, e1));
+    total += t;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = reps > 0 ? total / reps : 0.0;
+  const double bs2 = (double)m->bs * m->bs;
+  const double wv = mixed ? 4.0 : 8.0;
+  *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free CSR PCG (fcu_solve_csr_cg_noalloc).
 //
@@ -2107,9 +2143,12 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
 //  - the array is shared by all calls on a device, so calls that overlap in
 //    time on one device (from several host threads) race and corrupt each
 //    other's results. Callers must not overlap them;
-//  - the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress, which may load this module onto that device. Make
-//    that first call before any stream capture begins on the device;
+//  - every call looks up the array's device address on the current device
+//    with cudaGetSymbolAddress (no address is cached, so a call made after a
+//    cudaDeviceReset, which may reload the module at another address, still
+//    gets the right one). The first call on a device may load this module
+//    onto that device: make that first call before any stream capture
+//    begins on the device;
 //  - the solver state (grid-reduction arrival counters included) must start
 //    at zero. Each call writes a fresh state block over the array's header
 //    on the caller's stream before its first kernel. The vectors need no
@@ -2139,23 +2178,15 @@ static __device__ __align__(256) double g_noalloc_scratch[NA_WORDS];
 
 namespace {
 
-constexpr int NA_MAX_DEVICES = 64;
-std::atomic<double*> g_noalloc_addr[NA_MAX_DEVICES];
-
-// Device address of the scratch array on the current device (looked up on
-// the first call per device; the lookup is idempotent, so concurrent first
-// calls agree).
-double* noalloc_scratch(int dev) {
-  if (dev < 0 || dev >= NA_MAX_DEVICES) fail(FCU_ERR_UNSUPPORTED, "device ordinal too large for the no-alloc solver");
-  double* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
-  if (p) return p;
+// Device address of the scratch array on the current device, looked up on
+// every call: cheap once the module is loaded, allocates nothing, and never
+// stale (a cached address would outlive a cudaDeviceReset).
+double* noalloc_scratch() {
   void* a = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
   if (e != cudaSuccess) fail(FCU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   if (!a) fail(FCU_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
-  p = static_cast<double*>(a);
-  g_noalloc_addr[dev].store(p, std::memory_order_release);
-  return p;
+  return static_cast<double*>(a);
 }
 
 // Same acceptance rule as the u32 -> i32 conversion of fcu_solve_csr_cg:
@@ -2232,7 +2263,7 @@ int run_pcg_noalloc(i64 n, const uint32_t* row_ptr, const uint32_t* col_idx, con
     require_device_ptr(vals, dev, "vals");
   }
 
-  double* base = noalloc_scratch(dev);
+  double* base = noalloc_scratch();
   NoAllocHeader* hdr = reinterpret_cast<NoAllocHeader*>(base);
   double* partials = base + NA_HEADER_WORDS;
   double* r = partials + NA_PARTIAL_WORDS;

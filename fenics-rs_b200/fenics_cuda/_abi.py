@@ -115,6 +115,13 @@ SIGNATURES = {
     "fcu_spmv": (cint, [vp, vp, vp, vp]),
     "fcu_adjoint_gradient": (cint, [vp, vp, dbl, dbl, vp, vp, vp, vp]),
     "fcu_time_spmv": (cint, [vp, vp, cint, cint, C.POINTER(dbl), C.POINTER(dbl)]),
+    "fcu_time_spmv_cold": (cint, [vp, vp, cint, cint, C.c_size_t, C.POINTER(dbl), C.POINTER(dbl)]),
+    "fcu_buffer_alloc": (cint, [vp, C.c_size_t, C.POINTER(vp)]),
+    "fcu_buffer_free": (cint, [vp, vp]),
+    "fcu_buffer_copy": (cint, [vp, vp, vp, C.c_size_t]),
+    "fcu_buffer_memset": (cint, [vp, vp, cint, C.c_size_t]),
+    "fcu_device_count": (cint, [C.POINTER(cint)]),
+    "fcu_device_name": (cint, [cint, C.c_char_p, C.c_size_t]),
 }
 
 _lib = None

@@ -256,8 +256,10 @@ int fcu_batch_config(fcu_matrix m, int precision, int* lanes_per_row, int* threa
  *    synchronises it before returning;
  *  - the array is shared by every call on a device: calls that overlap in
  *    time on one device race. Callers must not overlap them;
- *  - the first call on a device looks up the array's address (and may load
- *    the module there); make it before any stream capture begins;
+ *  - every call looks up the array's address on the current device (no
+ *    address is cached, so calls after a cudaDeviceReset stay valid); the
+ *    first call on a device may load the module there, so make it before any
+ *    stream capture begins;
  *  - each call resets the solver state itself (it must start at zero);
  *  - info->kernel_ms is the host wall time of the call;
  *  - errors: fcu_last_error(NULL). Results and semantics as fcu_solve_csr_cg. */
@@ -374,6 +376,23 @@ int fcu_element_stresses(fcu_ctx ctx, fcu_space space, double E, double nu, cons
 int fcu_vertex_von_mises(fcu_ctx ctx, fcu_space space, const double* cell_von_mises,
                          double* vertex_von_mises);
 
+/* ---- device buffers and devices (no reference counterpart) ------------------ */
+/* For callers with no CUDA allocator of their own, such as the Python mirror
+ * of the Rust API; a Rust caller may equally pass memory from its own arena.
+ * Buffers come from the device's memory pool, allocated and released in
+ * order on the context's stream. */
+int fcu_buffer_alloc(fcu_ctx ctx, size_t bytes, void** out);
+int fcu_buffer_free(fcu_ctx ctx, void* p);
+/* Copy `bytes` between host and device memory, in any direction, on the
+ * context's stream. Returns when the copy is complete if either side is host
+ * memory; device-to-device copies are asynchronous. */
+int fcu_buffer_copy(fcu_ctx ctx, void* dst, const void* src, size_t bytes);
+/* Set `bytes` of device memory to the byte `value` (asynchronous). */
+int fcu_buffer_memset(fcu_ctx ctx, void* p, int value, size_t bytes);
+int fcu_device_count(int* count);
+/* The device's name, NUL-terminated and truncated to `len` bytes. */
+int fcu_device_name(int device, char* name, size_t len);
+
 /* ---- diagnostics (no reference counterpart) -------------------------------- */
 /* Average device time of one launch of the SpMV kernel the PCG of `precision`
  * runs on m (Ap = A p with the device p.Ap reduction), over `reps`
@@ -382,6 +401,13 @@ int fcu_vertex_von_mises(fcu_ctx ctx, fcu_space space, const double* cell_von_mi
  * pointers + one read of p + one write of Ap). */
 int fcu_time_spmv(fcu_ctx ctx, fcu_matrix m, int precision, int reps, double* ms_per_launch,
                   double* bytes_per_launch);
+/* As fcu_time_spmv, with the L2 cache flushed before every timed launch: a
+ * write of `flush_bytes` (at least the L2 size; 0 picks 256 MiB) to a buffer
+ * the call allocates, then one launch bracketed by CUDA events. Returns the
+ * mean of the `reps` single-launch times, so the matrix and the operand
+ * vector come from HBM as they do inside a solve whose operator exceeds L2. */
+int fcu_time_spmv_cold(fcu_ctx ctx, fcu_matrix m, int precision, int reps, size_t flush_bytes,
+                       double* ms_per_launch, double* bytes_per_launch);
 
 #ifdef __cplusplus
 }

@@ -5,7 +5,8 @@ process and after every other test has used the library. Everything goes
 through the C ABI: the library's fcu_solve_csr_cg (host arrays, through a
 context) is the comparison, the no-alloc entry point gets device arrays on
 the current torch stream. The matrix is the 7-point Laplacian that
-fenics-gpu/src/gpu.rs:1610-1663 solves with solve_csr_cg_gpu.
+crates/fenics-solver/src/gpu.rs:1610-1663 solves with solve_csr_cg_gpu, and
+the CPU oracle's restatement of cg.rs:40-149 checks the solution.
 """
 import ctypes as C
 
@@ -86,6 +87,25 @@ def test_noalloc_matches_existing_entry_two_calls(fcu, ctx, system):
         assert info.iterations == info_ref.iterations
         assert info.rel_residual < RTOL
         assert _close(xd.cpu().numpy(), x_ref)
+
+
+def test_noalloc_matches_oracle_cg(fcu, system):
+    """x and the iteration count against the oracle's CG (cg.rs:40-149) on the
+    same Laplacian (symmetric, so its CSR arrays are its CSC arrays)."""
+    import torch
+    import oracle as O
+    rp, ci, v, inv, dev = system
+    n = len(inv)
+    A = O.Csc(n, rp.astype(np.int64), ci.astype(np.int64), v)
+    b = np.random.default_rng(11).standard_normal(n)
+    x_o, it_o, _ = O.solve_cg(A, b, None, RTOL, MAX_ITER)
+    for _ in range(2):
+        xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rc, info = _noalloc(fcu, n, dev, torch.from_numpy(b).cuda(), xd)
+        assert rc == 0, fcu._abi.lib().fcu_last_error(None)
+        assert abs(info.iterations - it_o) <= 1
+        x = xd.cpu().numpy()
+        assert np.linalg.norm(x - x_o) <= 1e-8 * np.linalg.norm(x_o)
 
 
 def test_noalloc_allocates_no_device_memory(fcu, system):
