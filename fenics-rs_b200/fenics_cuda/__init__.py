@@ -526,10 +526,17 @@ class Matrix:
         _check(self.ctx, _L().fcu_spmv(self.ctx.h, self.h, px, py))
         return y
 
-    def time_spmv(self, precision=FCU_FP64, reps=20):
-        """(ms per launch, algorithmic bytes per launch) of the PCG SpMV kernel."""
+    def time_spmv(self, precision=FCU_FP64, reps=20, cold=False, flush_bytes=0):
+        """(ms per launch, algorithmic bytes per launch) of the PCG SpMV kernel:
+        the mean of `reps` back-to-back launches, or with cold=True the mean
+        of `reps` single launches each after an L2 flush of `flush_bytes`
+        (0: 256 MiB)."""
         ms, by = C.c_double(), C.c_double()
-        _check(self.ctx, _L().fcu_time_spmv(self.ctx.h, self.h, precision, reps, C.byref(ms), C.byref(by)))
+        if cold:
+            rc = _L().fcu_time_spmv_cold(self.ctx.h, self.h, precision, reps, flush_bytes, C.byref(ms), C.byref(by))
+        else:
+            rc = _L().fcu_time_spmv(self.ctx.h, self.h, precision, reps, C.byref(ms), C.byref(by))
+        _check(self.ctx, rc)
         return ms.value, by.value
 
     def pcg(self, b, x=None, x0=None, tol=1e-8, max_iter=10000, precision=FCU_FP64, raise_on_error=True):

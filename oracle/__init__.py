@@ -85,6 +85,7 @@ def _load() -> C.CDLL:
         "orc_p2_grads": (None, [f64p, f64p]),
         "orc_p2_mass_products": (None, [f64p]),
         "orc_cg_fixed_iters_mt": (dbl, [vp, f64p, i64, f64p, C.c_int]),
+        "orc_solve_cg_mt": (C.c_int, [vp, f64p, vp, dbl, i64, C.c_int, f64p, C.POINTER(i64), C.POINTER(dbl)]),
         "orc_assemble_mass": (vp, [i64, f64p, i64, i64p, vp, C.c_int, dbl, vp]),
     }
     for name, (res, args) in sig.items():
@@ -394,6 +395,25 @@ def solve_cg(A: Csc, b, x0=None, tol=1e-10, max_iter=1000):
     x0a = None if x0 is None else _f64(x0)
     with _Handle(A) as h:
         st = lib().orc_solve_cg(h, _f64(b), _ptr(x0a), tol, max_iter, x, C.byref(it), C.byref(res))
+    if st == 1:
+        raise CgError(f"Breakdown in CG: curvature p^T A p is near zero at iteration {it.value}")
+    if st == 2:
+        raise CgError(f"CG failed to converge within {max_iter} iterations")
+    return x, it.value, res.value
+
+
+def solve_cg_mt(A: Csc, b, x0=None, tol=1e-10, max_iter=1000, threads: int = 0):
+    """solve_cg's recurrence and stopping rules (cg.rs:40-149) with the SpMV,
+    vector loops and dot products on `threads` OpenMP threads (0 = all): a
+    multi-threaded CSR variant, labelled as such (the reference's CG is
+    sequential). A must be symmetric. Returns (x, iterations, absolute
+    residual); raises CgError like solve_cg."""
+    x = np.empty(A.n)
+    it = i64(0)
+    res = dbl(0.0)
+    x0a = None if x0 is None else _f64(x0)
+    with _Handle(A) as h:
+        st = lib().orc_solve_cg_mt(h, _f64(b), _ptr(x0a), tol, max_iter, threads, x, C.byref(it), C.byref(res))
     if st == 1:
         raise CgError(f"Breakdown in CG: curvature p^T A p is near zero at iteration {it.value}")
     if st == 2:

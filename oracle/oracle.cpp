@@ -1043,18 +1043,19 @@ int orc_solve_cg(void* h, const double* b, const double* x0, double tol, i64 max
   return 2;
 }
 
-// Timed-baseline helper: run exactly `iters` PCG iterations (no convergence
-// test) and return the final relative residual. Same arithmetic as
-// orc_solve_cg's loop.
-// Multi-threaded variant for the CPU baseline (labelled as such; the
-// reference's cg.rs is sequential): the same Jacobi-PCG recurrence with a
-// row-gather SpMV (the CSC of a symmetric matrix read as its CSR) and the
-// vector loops and dot products split over `threads` OpenMP threads.
-double orc_cg_fixed_iters_mt(void* h, const double* b, i64 iters, double* x, int threads) {
-  const orc_csc* A = (const orc_csc*)h;
+// Multi-threaded Jacobi-PCG (labelled as such wherever it is used; the
+// reference's cg.rs is sequential): the recurrence and stopping rules of
+// cg.rs:40-149 (x0 = 0 or given, the test ||r||/||b|| < tol after the x/r
+// update, breakdown when |p.Ap| < 1e-30), with a row-gather SpMV (the CSC of
+// a symmetric matrix read as its CSR) and the vector loops and dot products
+// split over `threads` OpenMP threads, so sums are ordered per thread block.
+// tol < 0 runs exactly max_iter iterations with no test (the timed-sample
+// form). Returns 0 converged, 1 breakdown, 2 iteration limit.
+static int cg_mt(const orc_csc* A, const double* b, const double* x0, double tol, i64 max_iter, int threads,
+                 double* x, i64* iters, double* res) {
   const i64 n = A->n;
   const int nt = nthreads_or_default(threads);
-  std::vector<double> inv(n, 1.0), r(b, b + n), z(n), p(n), ap(n);
+  std::vector<double> inv(n, 1.0), r(n), z(n), p(n), ap(n);
 #pragma omp parallel for schedule(static) num_threads(nt)
   for (i64 col = 0; col < n; ++col)
     for (i64 q = A->colptr[col]; q < A->colptr[col + 1]; ++q)
@@ -1068,22 +1069,43 @@ double orc_cg_fixed_iters_mt(void* h, const double* b, i64 iters, double* x, int
     for (i64 i = 0; i < n; ++i) s += u[i] * v[i];
     return s;
   };
-#pragma omp parallel for schedule(static) num_threads(nt)
-  for (i64 i = 0; i < n; ++i) {
-    x[i] = 0.0;
-    z[i] = r[i] * inv[i];
-    p[i] = z[i];
-  }
-  const double bn = std::sqrt(dot(b, b));
-  double rz = dot(r.data(), z.data()), rn = bn;
-  for (i64 it = 1; it <= iters; ++it) {
+  auto matvec = [&](const double* in, double* out) {
 #pragma omp parallel for schedule(static) num_threads(nt)
     for (i64 row = 0; row < n; ++row) {
       double s = 0.0;
-      for (i64 q = A->colptr[row]; q < A->colptr[row + 1]; ++q) s += A->vals[q] * p[A->rowidx[q]];
-      ap[row] = s;
+      for (i64 q = A->colptr[row]; q < A->colptr[row + 1]; ++q) s += A->vals[q] * in[A->rowidx[q]];
+      out[row] = s;
     }
-    const double alpha = rz / dot(p.data(), ap.data());
+  };
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (i64 i = 0; i < n; ++i) x[i] = x0 ? x0[i] : 0.0;
+  if (x0) {
+    matvec(x, ap.data());
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (i64 i = 0; i < n; ++i) r[i] = b[i] - ap[i];
+  } else {
+    std::copy(b, b + n, r.begin());
+  }
+  const double bn = std::sqrt(dot(b, b));
+  double rn = std::sqrt(dot(r.data(), r.data()));
+  *iters = 0;
+  *res = rn;
+  if (tol >= 0.0 && (rn < tol || (bn > 0.0 && rn / bn < tol))) return 0;
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (i64 i = 0; i < n; ++i) {
+    z[i] = r[i] * inv[i];
+    p[i] = z[i];
+  }
+  double rz = dot(r.data(), z.data());
+  for (i64 it = 1; it <= max_iter; ++it) {
+    matvec(p.data(), ap.data());
+    const double pap = dot(p.data(), ap.data());
+    if (tol >= 0.0 && std::fabs(pap) < 1e-30) {
+      *iters = it;
+      *res = rn;
+      return 1;
+    }
+    const double alpha = rz / pap;
 #pragma omp parallel for schedule(static) num_threads(nt)
     for (i64 i = 0; i < n; ++i) {
       x[i] += alpha * p[i];
@@ -1091,13 +1113,32 @@ double orc_cg_fixed_iters_mt(void* h, const double* b, i64 iters, double* x, int
       z[i] = r[i] * inv[i];
     }
     rn = std::sqrt(dot(r.data(), r.data()));
+    *iters = it;
+    *res = rn;
+    if (tol >= 0.0 && (bn > 0.0 ? rn / bn : rn) < tol) return 0;
     const double rzn = dot(r.data(), z.data());
     const double beta = rzn / rz;
     rz = rzn;
 #pragma omp parallel for schedule(static) num_threads(nt)
     for (i64 i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
   }
+  return 2;
+}
+
+// Timed-sample form: exactly `iters` iterations, final relative residual.
+double orc_cg_fixed_iters_mt(void* h, const double* b, i64 iters, double* x, int threads) {
+  const orc_csc* A = (const orc_csc*)h;
+  i64 it = 0;
+  double rn = 0.0;
+  cg_mt(A, b, nullptr, -1.0, iters, threads, x, &it, &rn);
+  const double bn = std::sqrt(dotv(b, b, A->n));
   return bn > 0.0 ? rn / bn : rn;
+}
+
+// To tolerance (cg.rs stopping rules), multi-threaded.
+int orc_solve_cg_mt(void* h, const double* b, const double* x0, double tol, i64 max_iter, int threads, double* x,
+                    i64* iters, double* res) {
+  return cg_mt((const orc_csc*)h, b, x0, tol, max_iter, threads, x, iters, res);
 }
 
 double orc_cg_fixed_iters(void* h, const double* b, i64 iters, double* x) {

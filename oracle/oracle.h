@@ -50,6 +50,8 @@ void orc_p2_basis(const double* xi, double* phi);
 void orc_p2_grads(const double* xi, double* g);
 void orc_p2_mass_products(double* out);
 double orc_cg_fixed_iters_mt(void* h, const double* b, i64 iters, double* x, int threads);
+int orc_solve_cg_mt(void* h, const double* b, const double* x0, double tol, i64 max_iter, int threads, double* x,
+                    i64* iters, double* res);
 void* orc_assemble_mass(i64 ndofs, const double* coords, i64 nc, const i64* cells, const i64* cell_dofs, int kind,
                         double density, const double* coef);
 #ifdef __cplusplus

@@ -1,109 +1,291 @@
-"""Checks at the benchmark's full sizes, through size-independent properties
-(the oracle is too slow here; the small-size parity tests compare with it
-directly):
+"""Parity with the oracle at the benchmark configurations' full sizes.
 
-- C2 elasticity (421,443 dofs): the assembled matrix is symmetric and holds
-  the three rigid translations in its kernel row by row (elasticity.rs:133-136
-  gives a symmetric element matrix with zero row sums per component); the
-  FP64 and mixed solutions both satisfy the FP64 residual bound, and agree.
-- C3 P2 Poisson (2,146,689 dofs, random kappa): every stiffness row sums to
-  zero (constants are in the kernel of the Laplacian).
-- C5 batch (256 instances, 5.8M dofs): every instance reaches its own
-  FP64 residual bound.
+Every configuration the benchmark measures is compared here with the CPU
+restatement of the reference path (oracle/), on the same inputs, through the
+C ABI:
+
+- C1, 2D P1 Poisson 64x64 (4,225 dofs): stiffness, load, Dirichlet system and
+  the FP64 PCG solution against poisson.rs:23-121,222-263 and cg.rs:40-149.
+- C2, vector-P1 elasticity 128x32x32 (421,443 dofs): the raw stiffness, the
+  body force and the eliminated system against elasticity.rs:73-227; the FP64
+  and mixed 1e-8 solutions against a tight FP64 reference solution, whose
+  residual is measured on the oracle's own matrix and which agrees with the
+  oracle's CG at 1e-13.
+- C3, P2 Poisson 64^3 with a random per-cell kappa (2,146,689 dofs): dof map,
+  boundary dofs, stiffness and load against the oracle's P2 restatement.
+- C4, adjoint sensitivities 96x32x32 (316,899 dofs): the gradient kernel
+  against the oracle's adjoint gradient on the same u and lambda, the
+  compliance identity, and the end-to-end gradient against one computed
+  entirely on the CPU (oracle assembly, oracle CG, oracle gradient).
+- C5, the 256-instance batch: the assembled block-diagonal matrix against the
+  oracle's, and 16 instances (the largest among them) solved by the batched
+  kernel against the oracle's CG on that instance alone.
+
+Bars: patterns, dof maps, boundary sets and load vectors bit-exact; FP64
+matrix entries within 1e-12 of each column's largest magnitude; solution
+tolerances stated at each assertion.
 """
+import math
+
 import numpy as np
 import pytest
 
+import oracle as O
+
 pytestmark = pytest.mark.gpu
 
-
-def _c2(fcu, ctx):
-    mesh = fcu.box_beam(4.0, 1.0, 1.0, 128, 32, 32)
-    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
-    M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
-    return mesh, V, M
+PI = math.pi
 
 
-def test_c2_matrix_symmetric_and_translations_in_kernel(fcu, ctx):
-    mesh, V, M = _c2(fcu, ctx)
-    A = M.export_csc().to_scipy().tocsr()
-    assert A.shape == (421443, 421443)
-    scale = abs(A).max()
-    assert abs(A - A.T).max() <= 1e-12 * scale
-    for c in range(3):
-        t = np.zeros(A.shape[0])
-        t[c::3] = 1.0
-        assert np.max(np.abs(A @ t)) <= 1e-9 * scale
+def _assert_csc_equal(A, B, tol=1e-12):
+    """A from the device, B from the oracle: pattern bit-exact, values within
+    tol of the column's largest magnitude."""
+    assert A.n == B.n
+    assert np.array_equal(A.colptr, B.colptr), "column pointers differ"
+    assert np.array_equal(A.rowidx, B.rowidx), "row indices differ"
+    scale = np.maximum.reduceat(np.abs(B.vals), B.colptr[:-1])
+    colscale = np.repeat(scale, np.diff(B.colptr))
+    dev = np.abs(A.vals - B.vals) / np.maximum(colscale, 1e-300)
+    assert dev.max() <= tol, f"max deviation {dev.max():.3e} of the column scale"
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# ---------------------------------------------------------------------------
+# C1
+# ---------------------------------------------------------------------------
+
+def test_c1_poisson_64_matches_oracle(fcu, ctx):
+    om = O.unit_square(64, 64)
+    mesh = fcu.Mesh(om.coords, om.cells)
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
+    M = fcu.Matrix(ctx, V).assemble_stiffness(None)
+    K = O.assemble_stiffness_2d(om)
+    _assert_csc_equal(M.export_csc(), K)
+    assert K.nnz == 29057
+    f = lambda x, y: 2.0 * PI * PI * np.sin(PI * x) * np.sin(PI * y)
+    b = fcu.assemble_rhs_2d(mesh, f, ctx)
+    bo = O.assemble_rhs_2d(om, f)
+    assert np.array_equal(b, bo)
+    # the benchmark's device-evaluated source: device sin vs libm sin
+    bs = V.rhs_source(fcu.FCU_SRC_SIN_PRODUCT, params=(2 * PI ** 2, PI))
+    assert np.max(np.abs(bs - bo)) <= 1e-14 * np.max(np.abs(bo))
+    bd = V.boundary_dofs()
+    assert np.array_equal(bd, O.boundary_dofs_2d(om)) and len(bd) == 256
+    Kb, fb = O.apply_dirichlet_bc(K, bo, bd, np.zeros(len(bd)))
+    M.apply_dirichlet(b, bd, np.zeros(len(bd)))
+    _assert_csc_equal(M.export_csc(), Kb)
+    assert Kb.nnz == 27537
+    assert np.array_equal(b, fb)
+    x, info = M.pcg(b, tol=1e-10, max_iter=10000, precision=fcu.FCU_FP64)
+    xo, it_o, _ = O.solve_cg(Kb, fb, None, 1e-10, 10000)
+    assert abs(info.iterations - it_o) <= 1, (info.iterations, it_o)
+    assert _rel(x, xo) <= 1e-9
+    # tight solve against a direct solve (scipy SuperLU)
+    import scipy.sparse.linalg as sla
+    xd = sla.spsolve(Kb.to_scipy().tocsc(), fb)
+    xt, _ = M.pcg(b, tol=1e-13, max_iter=10000, precision=fcu.FCU_FP64)
+    assert _rel(xt, xd) <= 1e-8
     M.close()
     V.close()
 
 
-def test_c2_fp64_and_mixed_solutions(fcu, ctx):
-    mesh, V, M = _c2(fcu, ctx)
-    A_raw = M.export_csc().to_scipy().tocsr()
-    clamp = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
-    dofs = (3 * clamp[:, None] + np.arange(3)).ravel().astype(np.int64)
+# ---------------------------------------------------------------------------
+# C2
+# ---------------------------------------------------------------------------
+
+@pytest.fixture(scope="module")
+def c2_oracle():
+    om = O.box_beam(4.0, 1.0, 1.0, 128, 32, 32)
+    K = O.assemble_elasticity_3d(om, 210e9, 0.3)
+    f = O.body_force_3d(om, [0.0, 0.0, -7.8e4])
+    dofs = O.clamp_dofs(om)
+    Kb, fb = O.apply_dirichlet_bc(K, f, dofs, np.zeros(len(dofs)))
+    return om, K, f, dofs, Kb, fb
+
+
+def test_c2_elasticity_system_matches_oracle(fcu, ctx, c2_oracle):
+    om, K, f, dofs, Kb, fb = c2_oracle
+    V = fcu.FunctionSpace(ctx, fcu.Mesh(om.coords, om.cells), fcu.FCU_SPACE_P1_VEC3)
+    M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+    assert V.ndofs == 421443
+    _assert_csc_equal(M.export_csc(), K)
+    assert K.nnz == 18280521
+    b = V.body_force([0.0, 0.0, -7.8e4])
+    assert np.array_equal(b, f)
+    M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
+    _assert_csc_equal(M.export_csc(), Kb)
+    assert Kb.nnz == 18141489
+    assert np.array_equal(b, fb)
+    M.close()
+    V.close()
+
+
+def test_c2_solutions_against_fp64_reference(fcu, ctx, c2_oracle):
+    """Both benchmark modes at 1e-8 against a 1e-13 FP64 reference solution."""
+    om, K, f, dofs, Kb, fb = c2_oracle
+    V = fcu.FunctionSpace(ctx, fcu.Mesh(om.coords, om.cells), fcu.FCU_SPACE_P1_VEC3)
+    M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
     b = V.body_force([0.0, 0.0, -7.8e4])
     M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
-    A = M.export_csc().to_scipy().tocsr()
-    xs = {}
+    bn = np.linalg.norm(fb)
+
+    def true_rel(x):  # residual on the oracle's matrix
+        return float(np.linalg.norm(fb - O.spmv(Kb, x)) / bn)
+
+    x_ref, info_ref = M.pcg(b, tol=1e-13, max_iter=200000, precision=fcu.FCU_FP64)
+    assert true_rel(x_ref) < 1e-12
+    # independent check of the reference solution: the oracle's CG (same
+    # recurrence, multi-threaded loops) to the same tolerance on the CPU
+    x_cpu, it_cpu, _ = O.solve_cg_mt(Kb, fb, None, 1e-13, 200000)
+    assert _rel(x_ref, x_cpu) <= 1e-9, _rel(x_ref, x_cpu)
+    assert abs(info_ref.iterations - it_cpu) <= max(5, 0.01 * it_cpu)
     for prec in (fcu.FCU_FP64, fcu.FCU_MIXED):
-        x, info = M.pcg(b, tol=1e-8, max_iter=100000, precision=prec)
-        rel = np.linalg.norm(b - A @ x) / np.linalg.norm(b)
+        x, info = M.pcg(b, tol=1e-8, max_iter=200000, precision=prec)
+        r = true_rel(x)
         if prec == fcu.FCU_MIXED:
-            # decided on the FP64 residual b - A64 x: reported = true, below tol
-            assert rel < 1e-8 * 1.0001
-            assert abs(info.rel_residual - rel) <= 1e-3 * rel
+            assert r < 1e-8 * 1.0001          # decided on the FP64 residual
         else:
-            # cg.rs stops on the recurrence residual; the true one drifts slightly
-            assert info.rel_residual < 1e-8
-            assert rel < 2e-8
-        xs[prec] = x
-    d = np.linalg.norm(xs[fcu.FCU_MIXED] - xs[fcu.FCU_FP64]) / np.linalg.norm(xs[fcu.FCU_FP64])
-    assert d < 1e-4
-    # clamped dofs stay zero; the beam sags (body force along -z)
-    assert np.all(xs[fcu.FCU_FP64][dofs] == 0.0)
-    assert xs[fcu.FCU_FP64][2::3].min() < 0.0
-    del A_raw
+            assert info.rel_residual < 1e-8   # cg.rs stops on the recurrence residual
+            assert r < 2e-8
+        # measured: FP64 ~1e-6 and mixed ~1e-6 relative L2 error at a 1e-8
+        # residual (the smooth bending modes converge last)
+        assert _rel(x, x_ref) < 2e-5, (prec, _rel(x, x_ref))
+        assert np.all(x[dofs] == 0.0)
     M.close()
     V.close()
 
 
-def test_c3_p2_rows_sum_to_zero(fcu, ctx):
-    mesh = fcu.unit_cube(64, 64, 64)
-    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P2)
-    assert V.ndofs == 2146689
-    kappa = np.exp(np.random.default_rng(3).standard_normal(mesh.nc))
+# ---------------------------------------------------------------------------
+# C3
+# ---------------------------------------------------------------------------
+
+def test_c3_p2_poisson_matches_oracle(fcu, ctx):
+    om = O.unit_cube(64, 64, 64)
+    kappa = np.exp(np.random.default_rng(3).standard_normal(om.nc))
+    cd, ev = O.p2_dofmap(om)
+    nd = om.nv + len(ev)
+    assert nd == 2146689
+    V = fcu.FunctionSpace(ctx, fcu.Mesh(om.coords, om.cells), fcu.FCU_SPACE_P2)
+    assert V.ndofs == nd
+    dcd, dev = V.p2_dofmap()
+    assert np.array_equal(dcd, cd) and np.array_equal(dev, ev)
+    bd = V.boundary_dofs()
+    assert np.array_equal(bd, O.p2_boundary_dofs(om)) and len(bd) == 98306
     M = fcu.Matrix(ctx, V).assemble_stiffness(kappa)
-    A = M.export_csc().to_scipy().tocsr()
-    assert A.nnz == 60859905
-    rows = np.asarray(A @ np.ones(A.shape[0]))
-    assert np.max(np.abs(rows)) <= 1e-10 * abs(A).max()
-    assert abs(A - A.T).max() <= 1e-12 * abs(A).max()
+    A = M.export_csc()
+    del dcd, dev
+    K = O.assemble_p2_stiffness_3d(om, cd, nd, kappa)
+    assert K.nnz == 60859905
+    _assert_csc_equal(A, K)
+    del A, K
+    b = V.rhs_source(fcu.FCU_SRC_CONSTANT, (1.0,))
+    assert np.array_equal(b, O.assemble_p2_rhs_3d(om, cd, nd, np.ones(4 * om.nc)))
     M.close()
     V.close()
 
 
-def test_c5_full_batch_converges_per_instance(fcu, ctx):
+# ---------------------------------------------------------------------------
+# C4
+# ---------------------------------------------------------------------------
+
+def test_c4_adjoint_gradient_full_size(fcu, ctx):
+    L = 3.0
+    om = O.box_beam(L, 1.0, 1.0, 96, 32, 32)
+    mesh = fcu.Mesh(om.coords, om.cells)
+    theta = np.random.default_rng(4).uniform(0.01, 1.0, om.nc)
+    facets = fcu.facets_on_plane(mesh, 0, L, ctx)
+    assert len(facets) == 2 * 32 * 32
+    ov = O.boundary_facets_3d(om)[0]
+    assert np.array_equal(facets, ov[np.all(np.abs(om.coords[ov][..., 0] - L) < 1e-9, axis=1)])
+    Vt = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+    load = fcu.traction_load(Vt, facets, (0.0, 0.0, -1.0))
+    Vt.close()
+    assert np.array_equal(load, O.surface_traction_3d(om, facets, lambda x, y, z: (0 * x, 0 * y, -1.0 + 0 * z)))
+    dofs = O.clamp_dofs(om)
+    adj = fcu.ElasticityAdjoint(mesh, 0.3, load, dofs, objective="compliance", ctx=ctx, tol=1e-13,
+                                max_iter=200000, precision=fcu.FCU_FP64)
+    J = adj.forward(theta)
+    g = adj.backward()
+    # the kernel against the oracle's gradient on the same u (lambda = u)
+    go = O.adjoint_grad(om, 0.3, 1.0, theta, adj.u, adj.u)
+    assert np.max(np.abs(g - go)) <= 1e-12 * np.max(np.abs(go))
+    # compliance identity: sum_e theta_e dJ/dtheta_e = -3 u^T K u = -3 J
+    assert abs(np.dot(theta, g) + 3.0 * J) <= 1e-9 * abs(J)
+    # end to end against the CPU: oracle assembly, oracle CG, oracle gradient
+    K = O.assemble_elasticity_3d(om, 1.0, 0.3, cell_E=theta ** 3)
+    Kb, fb = O.apply_dirichlet_bc(K, load, dofs, np.zeros(len(dofs)))
+    del K
+    u_cpu, _, _ = O.solve_cg_mt(Kb, fb, None, 1e-13, 200000)
+    g_cpu = O.adjoint_grad(om, 0.3, 1.0, theta, u_cpu, u_cpu)
+    assert np.max(np.abs(g - g_cpu)) <= 1e-8 * np.max(np.abs(g_cpu)), \
+        np.max(np.abs(g - g_cpu)) / np.max(np.abs(g_cpu))
+    adj.close()
+    # tip objective: lambda from a second solve
+    verts, cells, _ = fcu.extract_boundary_facets(mesh, ctx)
+    tipc = cells[np.all(np.abs(om.coords[verts][..., 0] - L) < 1e-9, axis=1)]
+    tipv = np.unique(om.cells[tipc])
+    cz = np.zeros(3 * om.nv)
+    cz[3 * tipv + 2] = 1.0 / len(tipv)
+    adj = fcu.ElasticityAdjoint(mesh, 0.3, load, dofs, objective=cz, ctx=ctx, tol=1e-13, max_iter=200000,
+                                precision=fcu.FCU_FP64)
+    adj.forward(theta)
+    g2 = adj.backward()
+    cb = cz.copy()
+    cb[dofs] = 0.0
+    lam_cpu, _, _ = O.solve_cg_mt(Kb, cb, None, 1e-13, 200000)
+    g2_cpu = O.adjoint_grad(om, 0.3, 1.0, theta, u_cpu, lam_cpu)
+    assert np.max(np.abs(g2 - g2_cpu)) <= 1e-8 * np.max(np.abs(g2_cpu))
+    adj.close()
+
+
+# ---------------------------------------------------------------------------
+# C5
+# ---------------------------------------------------------------------------
+
+def test_c5_batch_matches_oracle(fcu, ctx):
     rng = np.random.default_rng(2024)
     ns = rng.integers(32, 257, size=256)
-    meshes = [fcu.unit_square(int(n), int(n)) for n in ns]
-    kap = [np.exp(rng.standard_normal(m.nc)) for m in meshes]
-    fs = [rng.uniform(-1.0, 1.0, m.nv) for m in meshes]
-    mesh, offs = fcu.concat_meshes(meshes)
+    oms = [O.unit_square(int(n), int(n)) for n in ns]
+    kap = [np.exp(rng.standard_normal(m.nc)) for m in oms]
+    fs = [rng.uniform(-1.0, 1.0, m.nv) for m in oms]
+    mesh, offs = fcu.concat_meshes([fcu.Mesh(m.coords, m.cells) for m in oms])
     V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
     M = fcu.Matrix(ctx, V).assemble_stiffness(np.concatenate(kap))
+    # the whole block-diagonal matrix against the oracle on the concatenated mesh
+    K = O.assemble_stiffness_2d(O.Mesh(mesh.coords, mesh.cells), kappa=np.concatenate(kap))
+    _assert_csc_equal(M.export_csc(), K)
+    del K
     b = V.rhs_source(fcu.FCU_SRC_NODAL, nodal=np.concatenate(fs))
+    b_raw = b.copy()
     bd = V.boundary_dofs()
     M.apply_dirichlet(b, bd, np.zeros(len(bd)))
-    A = M.export_csc().to_scipy().tocsr()
-    x, it, rel, st, info = M.batch_pcg(offs, b, tol=1e-8, precision=fcu.FCU_MIXED)
-    assert np.all(st == 0)
-    r = b - A @ x
-    for i in range(len(meshes)):
+    res = {p: M.batch_pcg(offs, b, tol=1e-8, max_iter=100000, precision=p) for p in (fcu.FCU_FP64, fcu.FCU_MIXED)}
+    for p, (x, it, rel, st, info) in res.items():
+        assert np.all(st == 0)
+    x64, it64, _, _, _ = res[fcu.FCU_FP64]
+    xm, _, _, _, _ = res[fcu.FCU_MIXED]
+    # 16 instances, the four largest among them, each solved alone by the oracle
+    pick = list(np.argsort(-ns, kind="stable")[:4]) + list(rng.choice(256, 12, replace=False))
+    for i in pick:
+        om = oms[i]
         sl = slice(offs[i], offs[i + 1])
-        true_rel = np.linalg.norm(r[sl]) / np.linalg.norm(b[sl])
-        assert true_rel < 1e-8 * 1.0001
-        assert abs(rel[i] - true_rel) <= 1e-3 * true_rel
+        Ki = O.assemble_stiffness_2d(om, kappa=kap[i])
+        # the nodal load b = M f through the 3-point rule (f at the edge midpoints)
+        c = om.cells
+        f0, f1, f2 = fs[i][c[:, 0]], fs[i][c[:, 1]], fs[i][c[:, 2]]
+        fq = np.stack([0.5 * f0 + 0.5 * f1, 0.5 * f1 + 0.5 * f2, 0.5 * f0 + 0.5 * f2], 1).ravel()
+        bi = O.assemble_rhs_2d_values(om, fq)
+        assert np.max(np.abs(b_raw[sl] - bi)) <= 1e-15 * np.max(np.abs(bi))
+        bdi = O.boundary_dofs_2d(om)
+        Kbi, fbi = O.apply_dirichlet_bc(Ki, bi, bdi, np.zeros(len(bdi)))
+        xo, it_o, _ = O.solve_cg(Kbi, fbi, None, 1e-8, 100000)
+        assert abs(int(it64[i]) - it_o) <= max(2, 0.01 * it_o), (i, int(it64[i]), it_o)
+        assert _rel(x64[sl], xo) <= 1e-6, (i, _rel(x64[sl], xo))
+        r = np.linalg.norm(fbi - O.spmv(Kbi, xm[sl])) / np.linalg.norm(fbi)
+        assert r < 1e-8 * 1.0001
+        assert _rel(xm[sl], xo) <= 1e-6, (i, _rel(xm[sl], xo))
     M.close()
     V.close()
