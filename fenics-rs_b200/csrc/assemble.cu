@@ -144,6 +144,79 @@ __global__ void k_p2_metric_records(const int* __restrict__ cn, const double* __
   }
 }
 
+// P2 stiffness, three rows per warp (the kernel fcu_assemble_stiffness runs on
+// P2 spaces whose rows have at most 255 slots). Lanes 10g .. 10g+9 own row g
+// of the warp's three consecutive rows, lane 10g+b local column b. At each
+// step every group takes its row's next contribution (cell c with the row's
+// dof at local index a, ascending cell order), forms the element entry
+// K_e[a][b] = sum_m S_c[m] R[m][a][b] from the cell's metric record, and adds
+// it to the row's accumulator of slot cmap[t][b] in shared memory. The ten
+// columns of one cell are ten distinct dofs, so the ten lanes of a group
+// update ten distinct slots: no atomics, and every slot sums its
+// contributions in ascending cell order, as the triplet assembly does. The
+// three rows' slots are contiguous in the pattern, so the warp writes them
+// with coalesced stores. One element entry costs one metric record read
+// (shared by the group), six reference-tensor reads from shared memory, six
+// FMAs and one shared-memory add; no per-entry summation lists are read.
+constexpr int P2W = 8;  // warps per block
+
+__global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
+    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+    const unsigned char* __restrict__ cmap, const double* __restrict__ p2geo, i64 nrows, int stride,
+    double* __restrict__ v64, float* __restrict__ v32) {
+  extern __shared__ double p2sh[];
+  double* R = p2sh;  // 6 x 10 x 10
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (int q = threadIdx.x; q < 600; q += blockDim.x) R[q] = (&c_p2_R[0][0][0])[q];
+  __syncthreads();
+  const int g = lane / 10, b = lane - 10 * g;  // g == 3 on lanes 30 and 31
+  double* acc = p2sh + 600 + (i64)wib * 3 * stride;
+  double* my = acc + (g < 3 ? g : 0) * stride;
+  const i64 nwarps = (i64)gridDim.x * P2W;
+  for (i64 r0 = ((i64)blockIdx.x * P2W + wib) * 3; r0 < nrows; r0 += nwarps * 3) {
+    const i64 row = r0 + g;
+    int L = 0, cs = 0, nct = 0;
+    if (g < 3 && row < nrows) {
+      L = row_ptr[row + 1] - row_ptr[row];
+      cs = contrib_ptr[row];
+      nct = contrib_ptr[row + 1] - cs;
+    }
+    for (int q = b; q < L; q += 10) my[q] = 0.0;
+    const int steps = __reduce_max_sync(FULL, nct);
+    __syncwarp();
+    for (int t = 0; t < steps; ++t) {
+      if (t < nct) {
+        const i64 ci = (i64)cs + t;
+        const int cc = contrib[ci];
+        const double2* rec = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
+        const double2 s01 = rec[0], s23 = rec[1], s45 = rec[2];
+        const int sl = cmap[ci * 10 + b];
+        const double* Rab = R + (cc & 15) * 10 + b;
+        double v = s01.x * Rab[0];
+        v += s01.y * Rab[100];
+        v += s23.x * Rab[200];
+        v += s23.y * Rab[300];
+        v += s45.x * Rab[400];
+        v += s45.y * Rab[500];
+        my[sl] += v;
+      }
+      __syncwarp();
+    }
+    const i64 rend = r0 + 3 < nrows ? r0 + 3 : nrows;
+    const int base = row_ptr[r0];
+    const int tot = row_ptr[rend] - base;
+    const int off1 = row_ptr[r0 + 1 < rend ? r0 + 1 : rend] - base;
+    const int off2 = row_ptr[r0 + 2 < rend ? r0 + 2 : rend] - base;
+    for (int q = lane; q < tot; q += 32) {
+      const int gg = q >= off2 ? 2 : (q >= off1 ? 1 : 0);
+      const double v = acc[gg * stride + q - (gg == 2 ? off2 : gg == 1 ? off1 : 0)];
+      v64[base + q] = v;
+      v32[base + q] = (float)v;
+    }
+    __syncwarp();
+  }
+}
+
 // Header of a row-gather row, spread over the warp: lane k < 5 holds
 // row_ptr[row], row_ptr[row + 1], contrib_ptr[row], contrib_ptr[row + 1],
 // diag_pos[row] (read back with shuffles). The kernels fetch the next row's
@@ -392,6 +465,139 @@ __global__ void __launch_bounds__(EWARPS * 32, 4) k_assemble_elasticity(
         v32[base + q] = (float)v;
       }
       __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Vector-P1 elasticity, block-parallel form (the kernels fcu_assemble_elasticity
+// runs). Two passes:
+//
+//  1. k_elast_records, one thread per cell: the cell's four basis gradients
+//     g_b = J^{-T} grad(phi_b) and its scale s_c = |det J| / 6 (times E_c),
+//     stored as four 32-byte groups {g_b.x, g_b.y, g_b.z, s_c}. Each cell's
+//     geometry is computed once (the row-gather kernel above computes it once
+//     per vertex, four times).
+//  2. k_elast_blocks, one thread per block: for an upper off-diagonal block
+//     (i, j), j > i, the thread sums M = sum_c s_c g_a g_b^T over the cells
+//     that hold the edge (ascending cell order, a and b the local indices of
+//     i and j), forms K_ij = lam M + mu M^T + mu tr(M) I, and writes K_ij
+//     and its transpose K_ji; for a diagonal block (i, i) it sums the
+//     symmetric D = sum_c s_c g_a g_a^T over the cells around i and writes
+//     (lam + mu) D + mu tr(D) I. Every value is written once, with no atomics,
+//     and the assembled matrix is exactly symmetric.
+//
+// Both passes read and write with plain coalesced or 32-byte vector accesses;
+// the records of the cells around a window of rows stay in L2 between the
+// threads that share them.
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_elast_records(const int* __restrict__ cn, const double* __restrict__ X,
+                                                       const unsigned char* __restrict__ valid,
+                                                       const double* __restrict__ cellE, i64 nc,
+                                                       double* __restrict__ rec) {
+  for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
+    const int4 q = reinterpret_cast<const int4*>(cn)[c];
+    const int v[4] = {q.x, q.y, q.z, q.w};
+    double2* o = reinterpret_cast<double2*>(rec + 16 * c);
+    if (!valid[c]) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) o[k] = make_double2(0.0, 0.0);
+      continue;
+    }
+    const Geo3 g = tet_geometry(X, v);
+    double sc = (1.0 / 6.0) * fabs(g.det);
+    if (cellE) sc *= cellE[c];
+    o[0] = make_double2(-g.G[0][0] - g.G[0][1] - g.G[0][2], -g.G[1][0] - g.G[1][1] - g.G[1][2]);
+    o[1] = make_double2(-g.G[2][0] - g.G[2][1] - g.G[2][2], sc);
+#pragma unroll
+    for (int b = 1; b < 4; ++b) {
+      o[2 * b] = make_double2(g.G[0][b - 1], g.G[1][b - 1]);
+      o[2 * b + 1] = make_double2(g.G[2][b - 1], sc);
+    }
+  }
+}
+
+__device__ __forceinline__ void load_rec(const double* __restrict__ rec, unsigned c, unsigned a, double& x, double& y,
+                                         double& z, double& s) {
+  const double2* r = reinterpret_cast<const double2*>(rec + 16 * (i64)c + 4 * a);
+  const double2 p = __ldg(r), q = __ldg(r + 1);
+  x = p.x;
+  y = p.y;
+  z = q.x;
+  s = q.y;
+}
+
+__global__ void __launch_bounds__(256) k_elast_blocks(i64 nup, const int* __restrict__ up_ptr,
+                                                      const unsigned* __restrict__ up_ent,
+                                                      const int* __restrict__ up_slot,
+                                                      const int* __restrict__ up_tslot, i64 nn,
+                                                      const int* __restrict__ contrib_ptr,
+                                                      const int* __restrict__ contrib,
+                                                      const int* __restrict__ diag_pos,
+                                                      const double* __restrict__ rec, double lam, double mu,
+                                                      double* __restrict__ v64, float* __restrict__ v32) {
+  const i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+  if (t < nup) {
+    double M[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) M[k] = 0.0;
+    const int e1 = up_ptr[t + 1];
+    for (int e = up_ptr[t]; e < e1; ++e) {
+      const unsigned ent = up_ent[e];
+      const unsigned c = ent >> 4, a = (ent >> 2) & 3u, b = ent & 3u;
+      double hx, hy, hz, s, gx, gy, gz, s2;
+      load_rec(rec, c, a, hx, hy, hz, s);
+      load_rec(rec, c, b, gx, gy, gz, s2);
+      hx *= s;
+      hy *= s;
+      hz *= s;
+      M[0] += hx * gx; M[1] += hx * gy; M[2] += hx * gz;
+      M[3] += hy * gx; M[4] += hy * gy; M[5] += hy * gz;
+      M[6] += hz * gx; M[7] += hz * gy; M[8] += hz * gz;
+    }
+    const double tr = mu * (M[0] + M[4] + M[8]);
+    double K[9];
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+      for (int b2 = 0; b2 < 3; ++b2)
+        K[3 * a2 + b2] = lam * M[3 * a2 + b2] + mu * M[3 * b2 + a2] + (a2 == b2 ? tr : 0.0);
+    const i64 p = up_slot[t], q = up_tslot[t];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      v64[9 * p + k] = K[k];
+      v32[9 * p + k] = (float)K[k];
+    }
+    if (q < 0) return;  // the pattern is symmetric, so this does not happen
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+      for (int b2 = 0; b2 < 3; ++b2) {
+        v64[9 * q + 3 * b2 + a2] = K[3 * a2 + b2];
+        v32[9 * q + 3 * b2 + a2] = (float)K[3 * a2 + b2];
+      }
+  } else if (t - nup < nn) {
+    const i64 i = t - nup;
+    double d00 = 0.0, d11 = 0.0, d22 = 0.0, d01 = 0.0, d02 = 0.0, d12 = 0.0;
+    const int c1 = contrib_ptr[i + 1];
+    for (int k = contrib_ptr[i]; k < c1; ++k) {
+      const unsigned cc = (unsigned)contrib[k];
+      double gx, gy, gz, s;
+      load_rec(rec, cc >> 4, cc & 15u, gx, gy, gz, s);
+      const double hx = s * gx, hy = s * gy, hz = s * gz;
+      d00 += hx * gx; d11 += hy * gy; d22 += hz * gz;
+      d01 += hx * gy; d02 += hx * gz; d12 += hy * gz;
+    }
+    const double tr = mu * (d00 + d11 + d22);
+    const double lm = lam + mu;
+    const double K[9] = {lm * d00 + tr, lm * d01, lm * d02, lm * d01, lm * d11 + tr, lm * d12,
+                         lm * d02, lm * d12, lm * d22 + tr};
+    const i64 p = diag_pos[i];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      v64[9 * p + k] = K[k];
+      v32[9 * p + k] = (float)K[k];
     }
   }
 }
@@ -716,6 +922,25 @@ void ensure_p2_tables(fcu_ctx ctx) {
 // Host entry points (called from api.cu)
 // ---------------------------------------------------------------------------
 
+// FCU_ELAST_ROWGATHER=1 selects the row-gather elasticity kernel (kept as the
+// comparison for the block-parallel one).
+// FCU_P2_ROWGATHER=1 selects the slot-list P2 kernel (kept as the comparison).
+bool p2_row_gather() {
+  static const bool v = [] {
+    const char* e = getenv("FCU_P2_ROWGATHER");
+    return e && atoi(e) != 0;
+  }();
+  return v;
+}
+
+bool elasticity_row_gather() {
+  static const bool v = [] {
+    const char* e = getenv("FCU_ELAST_ROWGATHER");
+    return e && atoi(e) != 0;
+  }();
+  return v;
+}
+
 int assembly_blocks(fcu_ctx ctx, i64 rows, int warps = WARPS) {
   i64 need = (rows + warps - 1) / warps;
   i64 cap = (i64)ctx->num_sms * 8;
@@ -734,6 +959,22 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
     k_p2_metric_records<<<grid_for(me->nc, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
         s->cell_nodes.p, me->coords.p, coef_dev, me->nc, geo.p);
     LAUNCH_CHECK(ctx);
+    if (s->cmap.p && !p2_row_gather()) {
+      const int stride = s->max_row | 1;  // odd, so the three rows' accumulators start in different banks
+      const size_t smem = (600 + (size_t)P2W * 3 * stride) * sizeof(double);
+      static bool attr_set[64] = {};
+      if (smem > 48 * 1024 && !attr_set[ctx->device & 63]) {
+        CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        attr_set[ctx->device & 63] = true;
+      }
+      const i64 groups = (s->nnodes + 3 * P2W - 1) / (3 * P2W);
+      const int nbp = (int)std::max<i64>(1, std::min<i64>(groups, (i64)ctx->num_sms * 8));
+      k_assemble_p2_rows<<<nbp, P2W * 32, smem, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                                s->cmap.p, geo.p, s->nnodes, stride, m->val64.p,
+                                                                m->val32.p);
+      LAUNCH_CHECK(ctx);
+      return;
+    }
     k_assemble_scalar<10, 3, true><<<nb, WARPS * 32, 0, ctx->stream>>>(
         s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p, me->coords.p,
         coef_dev, geo.p, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
@@ -756,12 +997,29 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
   const double Eref = cellE_dev ? 1.0 : E;
   const double lam = (Eref * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
   const double mu = Eref / (2.0 * (1.0 + nu));
-  const int nb = assembly_blocks(ctx, s->nnodes, EWARPS);
-  k_assemble_elasticity<<<nb, EWARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
-                                                            s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p,
-                                                            s->mesh->coords.p, cellE_dev, lam, mu, s->diag_pos.p, s->nnodes,
-                                                            m->val64.p, m->val32.p);
-  LAUNCH_CHECK(ctx);
+  if (elasticity_row_gather()) {
+    const int nb = assembly_blocks(ctx, s->nnodes, EWARPS);
+    k_assemble_elasticity<<<nb, EWARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                              s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p,
+                                                              s->mesh->coords.p, cellE_dev, lam, mu, s->diag_pos.p,
+                                                              s->nnodes, m->val64.p, m->val32.p);
+    LAUNCH_CHECK(ctx);
+    return;
+  }
+  fcu_mesh me = s->mesh;
+  if (!s->cell_rec.p) s->cell_rec.alloc((size_t)me->nc * 16);
+  if (me->nc) {
+    k_elast_records<<<grid_for(me->nc, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
+        s->cell_nodes.p, me->coords.p, me->valid.p, cellE_dev, me->nc, s->cell_rec.p);
+    LAUNCH_CHECK(ctx);
+  }
+  const i64 work = s->nup + s->nnodes;
+  if (work) {
+    k_elast_blocks<<<(unsigned)((work + 255) / 256), 256, 0, ctx->stream>>>(
+        s->nup, s->up_ptr.p, s->up_ent.p, s->up_slot.p, s->up_tslot.p, s->nnodes, s->contrib_ptr.p, s->contrib.p,
+        s->diag_pos.p, s->cell_rec.p, lam, mu, m->val64.p, m->val32.p);
+    LAUNCH_CHECK(ctx);
+  }
 }
 
 void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev) {

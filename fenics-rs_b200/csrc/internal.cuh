@@ -153,6 +153,20 @@ struct fcu_space_s {
   DBuf<unsigned short> slot_ent;   // k*ncontrib: (t_local << 4) | b, per slot in cell order
   DBuf<int> tpos;          // nnzb: position of the transposed entry (built on demand)
   DBuf<double> cell_vol;   // nc: |det J| / 6 per tet (built by the first vertex average)
+  // Vector P1: the upper off-diagonal blocks (i, j), j > i, as a flat list.
+  // Block u sits at slot up_slot[u], its transpose at up_tslot[u]; the cells
+  // that couple i and j are up_ent[up_ptr[u] .. up_ptr[u+1]), each packed as
+  // (cell << 4) | (a << 2) | b with a, b the local indices of i and j, in
+  // ascending cell order.
+  i64 nup = 0;
+  DBuf<int> up_ptr, up_slot, up_tslot;
+  DBuf<unsigned> up_ent;
+  DBuf<double> cell_rec;   // vector P1: per-cell gradient records (16 doubles each)
+  // P2 scalar: for contribution t of a row (position in `contrib`) and local
+  // column b, the slot of dof cell_nodes[cell][b] within the row, as an
+  // offset from the row's first slot (rows of at most 255 slots; empty when
+  // a longer row exists).
+  DBuf<unsigned char> cmap;
 };
 
 struct fcu_matrix_s {

@@ -198,6 +198,88 @@ __global__ void k_slot_entries(const unsigned long long* __restrict__ keys, cons
   }
 }
 
+// Upper off-diagonal block lists (vector P1). On the sorted (row, col)
+// pairs: one flag per cell entry with col > row; on the slots: one flag per
+// slot with col > row.
+__global__ void k_up_entry_flags(const unsigned long long* __restrict__ keys, const unsigned* __restrict__ vals,
+                                 i64 nE, i64 nn, unsigned long long sentinel, int* __restrict__ f) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nE; t += (i64)gridDim.x * blockDim.x) {
+    const unsigned long long key = keys[t];
+    f[t] = (key != sentinel && vals[t] != 0xFFFFFFFFu && key % nn > key / nn) ? 1 : 0;
+  }
+}
+
+__global__ void k_up_slot_flags(const unsigned long long* __restrict__ keys, const int* __restrict__ slot_first,
+                                i64 nnzb, i64 nn, int* __restrict__ f) {
+  for (i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x; s < nnzb; s += (i64)gridDim.x * blockDim.x) {
+    const unsigned long long key = keys[slot_first[s]];
+    f[s] = key % nn > key / nn ? 1 : 0;
+  }
+}
+
+__global__ void k_up_fill_slots(const int* __restrict__ sflag, const int* __restrict__ sid,
+                                const int* __restrict__ slot_first, const int* __restrict__ epos, i64 nnzb,
+                                int* __restrict__ up_slot, int* __restrict__ up_ptr) {
+  for (i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x; s < nnzb; s += (i64)gridDim.x * blockDim.x) {
+    if (!sflag[s]) continue;
+    const int u = sid[s];
+    up_slot[u] = (int)s;
+    up_ptr[u] = epos[slot_first[s]];
+  }
+}
+
+__global__ void k_up_fill_entries(const unsigned* __restrict__ vals, const int* __restrict__ eflag,
+                                  const int* __restrict__ epos, i64 nE, unsigned* __restrict__ ent) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nE; t += (i64)gridDim.x * blockDim.x) {
+    if (!eflag[t]) continue;
+    ent[epos[t]] = vals[t];  // the emission index cell*16 + a*4 + b (k = 4) is the packed entry
+  }
+}
+
+// Position of the transposed block of each upper block (binary search in row j).
+__global__ void k_up_tslot(const int* __restrict__ row_ptr, const int* __restrict__ col_idx,
+                           const int* __restrict__ up_slot, const unsigned long long* __restrict__ keys,
+                           const int* __restrict__ slot_first, i64 nup, i64 nn, int* __restrict__ up_tslot) {
+  for (i64 u = blockIdx.x * (i64)blockDim.x + threadIdx.x; u < nup; u += (i64)gridDim.x * blockDim.x) {
+    const int p = up_slot[u];
+    const unsigned long long key = keys[slot_first[p]];
+    const int i = (int)(key / nn), j = (int)(key % nn);
+    int lo = row_ptr[j], hi = row_ptr[j + 1];
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (col_idx[mid] < i) lo = mid + 1;
+      else hi = mid;
+    }
+    up_tslot[u] = (lo < row_ptr[j + 1] && col_idx[lo] == i) ? lo : -1;
+  }
+}
+
+// Per-contribution slot map (P2 scalar): entry (i, j) of cell c with local
+// indices (a, b) is column b of contribution (c, a) of row i.
+__global__ void k_contrib_slot_map(const unsigned long long* __restrict__ keys, const unsigned* __restrict__ vals,
+                                   const int* __restrict__ slot_incl, i64 nE, i64 nn, int k,
+                                   unsigned long long sentinel, const int* __restrict__ row_ptr,
+                                   const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+                                   unsigned char* __restrict__ cmap) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nE; t += (i64)gridDim.x * blockDim.x) {
+    const unsigned long long key = keys[t];
+    if (key == sentinel) continue;
+    const unsigned v = vals[t];
+    if (v == 0xFFFFFFFFu) continue;
+    const i64 i = (i64)(key / nn);
+    const i64 kk = (i64)k * k;
+    const int c = (int)(v / kk);
+    const int b = (int)(v % k);
+    int lo = contrib_ptr[i], hi = contrib_ptr[i + 1];
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((contrib[mid] >> 4) < c) lo = mid + 1;
+      else hi = mid;
+    }
+    cmap[(i64)lo * k + b] = (unsigned char)(slot_incl[t] - 1 - row_ptr[i]);
+  }
+}
+
 __global__ void k_u32_to_u16(const unsigned* __restrict__ a, i64 n, unsigned short* __restrict__ b,
                              int* __restrict__ overflow) {
   for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n; t += (i64)gridDim.x * blockDim.x) {
@@ -402,6 +484,42 @@ void build_space_pattern(fcu_space s) {
   if (read_scalar(ctx, overflow.p))
     fail(FCU_ERR_UNSUPPORTED, "a node has more than 4095 incident cells or a slot more than 65535 contributions");
 
+  // --- upper off-diagonal block lists (vector P1 stiffness) -------------------
+  if (s->kind == FCU_SPACE_P1_VEC3) {
+    if (nc >= (1ll << 28)) fail(FCU_ERR_UNSUPPORTED, "mesh too large for the packed block lists");
+    DBuf<int> ef, epos, sf, sid;
+    ef.alloc(nE);
+    epos.alloc(nE);
+    sf.alloc(nnzb);
+    sid.alloc(nnzb);
+    k_up_entry_flags<<<grid_for(nE, 256, cap), 256, 0, ctx->stream>>>(keys_s.p, vals_s.p, nE, nn, sentinel, ef.p);
+    LAUNCH_CHECK(ctx);
+    exclusive_scan(ctx, ef.p, epos.p, nE);
+    const i64 nent = (i64)read_scalar(ctx, epos.p + nE - 1) + read_scalar(ctx, ef.p + nE - 1);
+    k_up_slot_flags<<<grid_for(nnzb, 256, cap), 256, 0, ctx->stream>>>(keys_s.p, slot_first.p, nnzb, nn, sf.p);
+    LAUNCH_CHECK(ctx);
+    exclusive_scan(ctx, sf.p, sid.p, nnzb);
+    const i64 nup = (i64)read_scalar(ctx, sid.p + nnzb - 1) + read_scalar(ctx, sf.p + nnzb - 1);
+    s->nup = nup;
+    s->up_slot.alloc(nup);
+    s->up_tslot.alloc(nup);
+    s->up_ptr.alloc(nup + 1);
+    s->up_ent.alloc(nent);
+    const int nent32 = (int)nent;
+    CUDA_CHECK(cudaMemcpyAsync(s->up_ptr.p + nup, &nent32, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    if (nup) {
+      k_up_fill_slots<<<grid_for(nnzb, 256, cap), 256, 0, ctx->stream>>>(sf.p, sid.p, slot_first.p, epos.p, nnzb,
+                                                                          s->up_slot.p, s->up_ptr.p);
+      LAUNCH_CHECK(ctx);
+      k_up_fill_entries<<<grid_for(nE, 256, cap), 256, 0, ctx->stream>>>(vals_s.p, ef.p, epos.p, nE, s->up_ent.p);
+      LAUNCH_CHECK(ctx);
+      k_up_tslot<<<grid_for(nup, 256, cap), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col_idx.p, s->up_slot.p,
+                                                                   keys_s.p, slot_first.p, nup, nn, s->up_tslot.p);
+      LAUNCH_CHECK(ctx);
+    }
+    CUDA_CHECK(cudaStreamSynchronize(ctx->stream));  // nent32 is a host temporary
+  }
+
   // --- host-side statistics -----------------------------------------------
   std::vector<int> rp(nn + 1), cp(nn + 1);
   CUDA_CHECK(cudaMemcpyAsync(rp.data(), s->row_ptr.p, (nn + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -418,6 +536,15 @@ void build_space_pattern(fcu_space s) {
   s->max_row = mr;
   s->max_contrib = mc;
   s->nnz_ref = (nnzb - empty_rows) * (i64)s->bs * s->bs;
+
+  // --- per-contribution slot map (P2 stiffness) --------------------------------
+  if ((s->kind == FCU_SPACE_P2 || s->kind == FCU_SPACE_P2_NODES) && mr <= 255 && ncontrib > 0) {
+    s->cmap.alloc((i64)k * ncontrib);
+    k_contrib_slot_map<<<grid_for(nE, 256, cap), 256, 0, ctx->stream>>>(keys_s.p, vals_s.p, slot_incl.p, nE, nn, k,
+                                                                        sentinel, s->row_ptr.p, s->contrib_ptr.p,
+                                                                        s->contrib.p, s->cmap.p);
+    LAUNCH_CHECK(ctx);
+  }
 }
 
 void build_transpose_positions(fcu_space s) {

@@ -18,7 +18,7 @@ meaning and error behaviour follow GlassOnTin/fenics-rs:
                            solve_vibration_modes(_with_inner)
 
 All compute runs in CUDA kernels on the device; there is no CPU fallback (a
-missing library or device raises). Arrays may be numpy (host) or torch CUDA
+missing library or device raises). Arrays may be numpy (host), DeviceArray (device memory the library allocates), or torch CUDA
 tensors (device); device arrays are used in place.
 """
 from __future__ import annotations
@@ -66,7 +66,7 @@ def _L():
 
 
 # ---------------------------------------------------------------------------
-# pointers: numpy (host) or torch CUDA tensors (device)
+# pointers: numpy (host), DeviceArray or any CUDA tensor with data_ptr() (device)
 # ---------------------------------------------------------------------------
 
 def _is_torch(a) -> bool:
@@ -77,12 +77,100 @@ def _ptr(a, dtype=None):
     """(address, keepalive) of a contiguous array, converting numpy dtypes."""
     if a is None:
         return None, None
+    if isinstance(a, DeviceArray):
+        if dtype is not None and np.dtype(dtype) != a.dtype:
+            raise TypeError(f"device array of {a.dtype} where {np.dtype(dtype)} is expected")
+        return a.ptr, a
     if _is_torch(a):
         if not a.is_contiguous():
             raise ValueError("torch tensors must be contiguous")
         return a.data_ptr(), a
     arr = np.ascontiguousarray(a, dtype=dtype) if dtype is not None else np.ascontiguousarray(a)
     return arr.ctypes.data, arr
+
+
+class DeviceArray:
+    """A one-dimensional array in device memory, allocated by the library
+    (fcu_buffer_alloc on the context's stream) for callers that have no CUDA
+    array type of their own; the mirror of a Rust caller passing memory from
+    its own arena. Every function of this module accepts it wherever it
+    accepts a host array, and then leaves the data on the device."""
+
+    def __init__(self, ctx: "Context", n: int, dtype=np.float64):
+        self.ctx = ctx
+        self.dtype = np.dtype(dtype)
+        self.n = int(n)
+        h = C.c_void_p()
+        _check(ctx, _L().fcu_buffer_alloc(ctx.h, self.nbytes, C.byref(h)))
+        self.ptr = h.value
+
+    @classmethod
+    def from_numpy(cls, ctx: "Context", a, dtype=None) -> "DeviceArray":
+        a = np.ascontiguousarray(a, dtype=dtype)
+        d = cls(ctx, a.size, a.dtype)
+        d.copy_from(a)
+        return d
+
+    @property
+    def nbytes(self) -> int:
+        return self.n * self.dtype.itemsize
+
+    @property
+    def shape(self):
+        return (self.n,)
+
+    def __len__(self):
+        return self.n
+
+    def copy_from(self, a):
+        """Copy from a host array or another device array of the same size."""
+        if isinstance(a, DeviceArray):
+            src, keep = a.ptr, a
+        else:
+            keep = np.ascontiguousarray(a, dtype=self.dtype)
+            src = keep.ctypes.data
+        if (keep.nbytes if not isinstance(keep, DeviceArray) else keep.nbytes) != self.nbytes:
+            raise ValueError("size mismatch")
+        _check(self.ctx, _L().fcu_buffer_copy(self.ctx.h, C.c_void_p(self.ptr), C.c_void_p(src), self.nbytes))
+        return self
+
+    def zero_(self):
+        _check(self.ctx, _L().fcu_buffer_memset(self.ctx.h, C.c_void_p(self.ptr), 0, self.nbytes))
+        return self
+
+    def numpy(self) -> np.ndarray:
+        """Host copy (waits for the context's stream)."""
+        out = np.empty(self.n, self.dtype)
+        _check(self.ctx, _L().fcu_buffer_copy(self.ctx.h, C.c_void_p(out.ctypes.data), C.c_void_p(self.ptr),
+                                               self.nbytes))
+        return out
+
+    def clone(self) -> "DeviceArray":
+        return DeviceArray(self.ctx, self.n, self.dtype).copy_from(self)
+
+    def free(self):
+        if self.ptr and self.ctx.h:
+            _L().fcu_buffer_free(self.ctx.h, C.c_void_p(self.ptr))
+        self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    rc = _L().fcu_device_count(C.byref(n))
+    return n.value if rc == _abi.FCU_OK else 0
+
+
+def device_name(device: int = 0) -> str:
+    buf = C.create_string_buffer(256)
+    if _L().fcu_device_name(device, buf, 256) != _abi.FCU_OK:
+        return f"cuda:{device}"
+    return buf.value.decode()
 
 
 def _check(ctx: "Context", rc: int):
@@ -822,10 +910,7 @@ def _device_vector(ctx: Context, n: int):
     """A device vector for the drivers: the load vector and the solution stay
     on the device from assembly to the end of the solve. It is allocated on
     the context's stream, the stream the library's kernels use it on."""
-    import torch
-    dev = torch.device("cuda", ctx.device)
-    with torch.cuda.stream(torch.cuda.ExternalStream(ctx.stream, device=dev)):
-        return torch.empty(n, dtype=torch.float64, device=dev)
+    return DeviceArray(ctx, n)
 
 
 def _solve_poisson(mesh: Mesh, source, boundary_value, tol, max_iter, ctx, precision):
@@ -840,7 +925,7 @@ def _solve_poisson(mesh: Mesh, source, boundary_value, tol, max_iter, ctx, preci
                                     np.float64), (len(bd),)).copy()
     M.apply_dirichlet(b, bd, bv)
     x, info = M.pcg(b, x=_device_vector(ctx, V.ndofs), tol=tol, max_iter=max_iter, precision=precision)
-    return PoissonSolution(x.cpu().numpy(), info.iterations, info.residual)
+    return PoissonSolution(x.numpy(), info.iterations, info.residual)
 
 
 def solve_poisson_2d(mesh: Mesh, source, boundary_value, tol, max_iter, ctx=None, precision=FCU_FP64):
@@ -1020,12 +1105,15 @@ def shard_instances(costs, world: int) -> list:
 
 
 def solve_poisson_batch_sharded(meshes, kappas=None, nodal_sources=None, tol=1e-8, max_iter=100000, ctx=None,
-                                precision=FCU_MIXED, rank=0, world=1, group=None, solve=None):
+                                precision=FCU_MIXED, rank=0, world=1, group=None, solve=None, all_gather=None):
     """The batch split over ranks (one GPU each): rank r solves its shard with
     the batched solver, then every rank receives every instance's result
     through one all_gather of Python objects. The solve itself exchanges
     nothing. `solve` replaces solve_poisson_batch (same arguments), e.g. for
-    host-side tests. Returns (solutions, iterations, rel_residuals, statuses)
+    host-side tests. `all_gather(parts, obj)` fills `parts` (one slot per
+    rank) with every rank's obj; by default torch.distributed's
+    all_gather_object on `group` (the process-group plumbing, imported only
+    when world > 1). Returns (solutions, iterations, rel_residuals, statuses)
     in instance order."""
     meshes = list(meshes)
     mine = shard_instances(batch_costs(meshes), world)[rank]
@@ -1039,9 +1127,12 @@ def solve_poisson_batch_sharded(meshes, kappas=None, nodal_sources=None, tol=1e-
             local[i] = (np.asarray(res.solutions[j]), int(res.iterations[j]), float(res.rel_residuals[j]),
                         int(res.statuses[j]))
     if world > 1:
-        import torch.distributed as dist
         parts = [None] * world
-        dist.all_gather_object(parts, local, group=group)
+        if all_gather is None:
+            import torch.distributed as dist
+            dist.all_gather_object(parts, local, group=group)
+        else:
+            all_gather(parts, local)
         merged = {}
         for part in parts:
             merged.update(part)
@@ -1070,7 +1161,7 @@ def solve_elasticity_3d(mesh: Mesh, material: ElasticMaterial, body_force, bc: V
     d, v = bc.arrays()
     M.apply_dirichlet(f, d, v)
     xd, info = M.pcg(f, x=_device_vector(ctx, V.ndofs), tol=tol, max_iter=max_iter, precision=precision)
-    x = xd.cpu().numpy()
+    x = xd.numpy()
     return ElasticitySolution(x, mesh.coords + x.reshape(-1, 3), info.iterations, info.residual)
 
 
@@ -1236,7 +1327,12 @@ class TransientHeatSolver:
 
     def step(self, mass_mat, stiff_mat, u_n, f_n, f_next):
         st = self._prepare(mass_mat, stiff_mat)
-        out = np.empty(len(u_n)) if not _is_torch(u_n) else u_n.new_empty(u_n.shape)
+        if isinstance(u_n, DeviceArray):
+            out = DeviceArray(self.ctx, len(u_n))
+        elif _is_torch(u_n):
+            out = u_n.new_empty(u_n.shape)
+        else:
+            out = np.empty(len(u_n))
         self.last_info = st.step(u_n, f_n, f_next, out, self.tol, self.max_iter, self.precision)
         return out
 
@@ -1265,7 +1361,6 @@ def solve_transient_heat_2d(mesh: Mesh, diffusivity, u_initial, bcs, dt, num_ste
     the state before and after every step. heat_source(t, point) is called
     per vertex like the reference's closure (or once per time with the
     (nv, 2) coordinates when vectorized_source); None means no source."""
-    import torch
     ctx = ctx or default_context()
     n = mesh.num_vertices()
     if len(u_initial) != n:
@@ -1280,9 +1375,8 @@ def solve_transient_heat_2d(mesh: Mesh, diffusivity, u_initial, bcs, dt, num_ste
         vals.extend(float(v) for v in bc.values)
     if dofs:
         st.set_dirichlet(np.asarray(dofs, np.int64), np.asarray(vals, np.float64))
-    dev = torch.device("cuda", ctx.device)
-    u = torch.as_tensor(np.asarray(u_initial, dtype=np.float64)).to(dev)
-    un = torch.empty_like(u)
+    u = DeviceArray.from_numpy(ctx, u_initial, np.float64)
+    un = DeviceArray(ctx, n)
     coords = mesh.coords
 
     def source(t):
@@ -1301,8 +1395,8 @@ def solve_transient_heat_2d(mesh: Mesh, diffusivity, u_initial, bcs, dt, num_ste
             u, un = un, u
             times.append(t_next)
             if keep_history:
-                history.append(u.cpu().numpy())
-        final = u.cpu().numpy()
+                history.append(u.numpy())
+        final = u.numpy()
     finally:
         st.close()
         M.close()
@@ -1322,14 +1416,6 @@ class VibrationMode:
     mode_shape: np.ndarray
 
 
-class _DeviceArray:
-    """A raw device pointer exposed through __cuda_array_interface__."""
-
-    def __init__(self, ptr: int, n: int, readonly: bool):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, readonly),
-                                         "version": 3, "strides": None}
-
-
 def _vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, ctx, precision, inner_tol,
                      inner_max_iter, inner):
     ctx = ctx or default_context()
@@ -1344,18 +1430,18 @@ def _vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, ctx, pre
     err = []
     cb = _abi.INNER_SOLVE()
     if inner is not None:
-        import torch
-        dev = torch.device("cuda", ctx.device)
+        L = _L()
 
         def trampoline(user, nn, b, x0, x):
             try:
-                bh = torch.as_tensor(_DeviceArray(b, nn, False), device=dev).cpu().numpy()
-                x0h = torch.as_tensor(_DeviceArray(x0, nn, False), device=dev).cpu().numpy()
+                # b, x0 and x are device arrays; the library's stream is idle
+                bh, x0h = np.empty(nn), np.empty(nn)
+                _check(ctx, L.fcu_buffer_copy(ctx.h, C.c_void_p(bh.ctypes.data), C.c_void_p(b), 8 * nn))
+                _check(ctx, L.fcu_buffer_copy(ctx.h, C.c_void_p(x0h.ctypes.data), C.c_void_p(x0), 8 * nn))
                 res = np.ascontiguousarray(inner(bh, x0h), dtype=np.float64)
                 if res.shape != (nn,):
                     raise ValueError(f"inner solve returned shape {res.shape}, expected ({nn},)")
-                torch.as_tensor(_DeviceArray(x, nn, False), device=dev).copy_(torch.from_numpy(res))
-                torch.cuda.synchronize(dev)
+                _check(ctx, L.fcu_buffer_copy(ctx.h, C.c_void_p(x), C.c_void_p(res.ctypes.data), 8 * nn))
                 return 0
             except Exception as e:  # the reference's `?` on the closure's Err
                 err.append(e)
@@ -1420,8 +1506,7 @@ class GpuBsr3Context:
         self.M = Matrix.from_bsr3(self.ctx, n_nodes, row_ptr, cols, vals_flat, dinv_flat)
 
     def device_name(self) -> str:
-        import torch
-        return torch.cuda.get_device_name(self.ctx.device)
+        return device_name(self.ctx.device)
 
     def nnz_blocks(self) -> int:
         return self._nnzb
@@ -1466,10 +1551,9 @@ def solve_bsr3_pcg_gpu(n_nodes, row_ptr, cols, vals_flat, dinv_flat, b, x0=None,
     wall = (time.perf_counter() - t0) * 1e3
     nnzb = int(np.asarray(row_ptr)[-1])
     flops = (nnzb * 18.0 + n * 16.0) * info.iterations
-    import torch
     return GpuSolveResult(x, int(info.iterations), float(info.rel_residual), wall, float(info.kernel_ms),
                           flops / max(info.kernel_ms * 1e-3, 1e-12) / 1e9, float(info.effective_bw_gbps),
-                          [torch.cuda.get_device_name(ctx.device)])
+                          [device_name(ctx.device)])
 
 
 def bsr3_row_split(n_nodes, row_ptr, parts):
@@ -1495,8 +1579,7 @@ def spmv_bsr3_multi_gpu(n_nodes, row_ptr, cols, vals_flat, x, max_gpus):
     g = min(max_gpus, visible devices) contiguous ranges (bsr3_row_split), each
     range's product computed on its device, concatenated on the host. Returns
     (y, device names)."""
-    import torch
-    nd = max(1, min(int(max_gpus), torch.cuda.device_count()))
+    nd = max(1, min(int(max_gpus), device_count()))
     cols = np.asarray(cols, np.uint32)
     vals_flat = np.asarray(vals_flat, np.float64)
     y = np.zeros(3 * int(n_nodes))
@@ -1507,7 +1590,7 @@ def spmv_bsr3_multi_gpu(n_nodes, row_ptr, cols, vals_flat, x, max_gpus):
         part = M.spmv(x)
         y[3 * r0:3 * r1] = part[3 * r0:3 * r1]
         M.close()
-        names.append(torch.cuda.get_device_name(ctx.device))
+        names.append(device_name(ctx.device))
         if slot:
             ctx.close()
     return y, names

@@ -68,3 +68,21 @@ def test_concat_meshes_layout(fcu):
     assert np.array_equal(O.boundary_dofs_2d(om), want)
     with pytest.raises(ValueError):
         fcu.concat_meshes([])
+
+
+def test_package_imports_without_torch():
+    """The product package allocates and copies device memory through the
+    library's own C ABI (DeviceArray), so it imports and loads with torch
+    unavailable, as a Rust caller would run it."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.modules['torch'] = None\n"
+            "sys.path.insert(0, %r)\n"
+            "import fenics_cuda as f\n"
+            "f._abi.lib()\n"
+            "assert f.DeviceArray and f.device_count() >= 0\n"
+            "bad = [m for m in sys.modules if m == 'torch' or m.startswith('torch.')]\n"
+            "assert all(sys.modules[m] is None for m in bad), bad\n"
+            "print('ok')\n") % os.path.join(ROOT, "fenics-rs_b200")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stderr
