@@ -430,6 +430,10 @@ def run_cuda(args, cfg):
                                    "peak": peak, "unit": "GB/s", "frac": sp["frac_cold"],
                                    "bytes_per_launch": sp["bytes"],
                                    "traffic": _profile_traffic("spmv_bsr3_fp32_elasticity_c2p.txt")}
+    if dist and not args.no_extra:
+        c5 = run_c5_sharded(ctx, stream, rank, world, tdist)
+        if rank == 0:
+            res["c5_sharded"] = c5
     if rank == 0 and not args.no_cpu_baseline:
         res["cpu_baseline"] = cpu_baseline_leg(cfg, x_ref)
     if dist:
@@ -437,6 +441,46 @@ def run_cuda(args, cfg):
         tdist.destroy_process_group()
     ctx.close()
     return res if rank == 0 else None
+
+
+def run_c5_sharded(ctx, stream, rank, world, tdist):
+    """The 256-instance batch (C5) split over the ranks by instance
+    (shard_instances: largest estimated cost first onto the least-loaded
+    rank). Each rank assembles and solves its shard with the batched PCG on
+    its own GPU; nothing is exchanged during the solve. Device time per rank
+    by CUDA events, the maximum over ranks by one all_reduce; the solve is
+    timed after one untimed warm-up (tuning and graph capture)."""
+    import torch
+    import fenics_cuda as fcu
+    rng = np.random.default_rng(2024)
+    ns = rng.integers(32, 257, size=256)
+    meshes = [fcu.unit_square(int(n), int(n)) for n in ns]
+    kap = [np.exp(rng.standard_normal(m.nc)) for m in meshes]
+    fs = [rng.uniform(-1.0, 1.0, m.nv) for m in meshes]
+    mine = fcu.shard_instances(fcu.batch_costs(meshes), world)[rank]
+    mesh, offs = fcu.concat_meshes([meshes[i] for i in mine])
+    V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1)
+    M = fcu.Matrix(ctx, V).assemble_stiffness(np.concatenate([kap[i] for i in mine]))
+    b = V.rhs_source(fcu.FCU_SRC_NODAL, nodal=np.concatenate([fs[i] for i in mine]))
+    bd = V.boundary_dofs()
+    M.apply_dirichlet(b, bd, np.zeros(len(bd)))
+    M.batch_pcg(offs, b, tol=1e-8, max_iter=100000, precision=fcu.FCU_MIXED)
+    tdist.barrier()
+    torch.cuda.synchronize()
+    ms, (x, it, rel, st, info) = _events_ms(
+        stream, lambda: M.batch_pcg(offs, b, tol=1e-8, max_iter=100000, precision=fcu.FCU_MIXED))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = torch.tensor([ms, float(V.ndofs), float((st != 0).sum())], dtype=torch.float64, device=dev)
+    tmax = t.clone()
+    tdist.all_reduce(tmax, op=tdist.ReduceOp.MAX)
+    tsum = t.clone()
+    tdist.all_reduce(tsum, op=tdist.ReduceOp.SUM)
+    M.close()
+    V.close()
+    return {"workload": "the 256-problem C5 batch split over the ranks by instance, mixed PCG to 1e-8",
+            "ms_max_over_ranks": float(tmax[0]), "dofs_total": int(tsum[1]),
+            "dof_per_s": float(tsum[1]) / (float(tmax[0]) * 1e-3), "unconverged": int(tsum[2]),
+            "instances_on_rank0": len(mine), "scaling": "strong"}
 
 
 def _events_ms(stream, fn):
@@ -788,7 +832,8 @@ def run_reference(args, cfg):
     }
 
 
-PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5", "p2_cube40")
+PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5", "p2_cube40",
+                 "spmv_c2p", "spmv_c2")
 
 
 def profile_case(name):
@@ -805,11 +850,29 @@ def profile_case(name):
                        set, else tuned first)
       p2_cube40        P2 stiffness on the unit cube 40^3 x 6 tets (384,000
                        cells, 531,441 dofs), random kappa, assembled 3 times
-                       (the C3 kernel on a quarter of its cells)"""
+                       (the C3 kernel on a quarter of its cells)
+      spmv_c2p         the mixed PCG's FP32 block SpMV on the C2' system
+                       (1,568,403 dofs, operator larger than L2), 3 launches
+                       each after an L2 flush, shape tuning off
+      spmv_c2          the same on the C2 system (421,443 dofs)"""
     import torch
+    if name in ("spmv_c2p", "spmv_c2"):
+        os.environ["FCU_TUNE"] = "0"   # no shape-tuning launches before the captured ones
     import fenics_cuda as fcu
     ctx = fcu.Context(0)
-    if name in ("elasticity_c2", "mass_c2", "block_update_c2"):
+    if name in ("spmv_c2p", "spmv_c2"):
+        cfg = CONFIGS["c2p" if name == "spmv_c2p" else "c2"]
+        mesh = fcu.box_beam(cfg["L"], cfg["W"], cfg["H"], cfg["nx"], cfg["ny"], cfg["nz"])
+        V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+        M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+        cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+        dofs = (3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64)
+        b = V.body_force([0.0, 0.0, -7.8e4])
+        M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
+        M.time_spmv(fcu.FCU_MIXED, reps=3, cold=True)
+        ctx.synchronize()
+        M.close(); V.close()
+    elif name in ("elasticity_c2", "mass_c2", "block_update_c2"):
         mesh = fcu.box_beam(4.0, 1.0, 1.0, 128, 32, 32)
         V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
         if name in ("elasticity_c2", "mass_c2"):

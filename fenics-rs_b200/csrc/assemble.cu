@@ -160,6 +160,18 @@ __global__ void k_p2_metric_records(const int* __restrict__ cn, const double* __
 // FMAs and one shared-memory add; no per-entry summation lists are read.
 constexpr int P2W = 8;  // warps per block
 
+__device__ __forceinline__ void p2_record(const double* __restrict__ p2geo, int cc, double2& s01, double2& s23,
+                                          double2& s45) {
+  const double2* rec = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
+  s01 = __ldg(rec);
+  s23 = __ldg(rec + 1);
+  s45 = __ldg(rec + 2);
+}
+
+// PF: software pipeline over the steps (the next step's metric record and
+// slot, and the contribution two steps ahead, are loaded before the current
+// step's arithmetic), so a step does not wait for its own loads.
+template <bool PF>
 __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
     const unsigned char* __restrict__ cmap, const double* __restrict__ p2geo, i64 nrows, int stride,
@@ -183,24 +195,63 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     }
     for (int q = b; q < L; q += 10) my[q] = 0.0;
     const int steps = __reduce_max_sync(FULL, nct);
-    __syncwarp();
-    for (int t = 0; t < steps; ++t) {
-      if (t < nct) {
-        const i64 ci = (i64)cs + t;
-        const int cc = contrib[ci];
-        const double2* rec = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
-        const double2 s01 = rec[0], s23 = rec[1], s45 = rec[2];
-        const int sl = cmap[ci * 10 + b];
-        const double* Rab = R + (cc & 15) * 10 + b;
-        double v = s01.x * Rab[0];
-        v += s01.y * Rab[100];
-        v += s23.x * Rab[200];
-        v += s23.y * Rab[300];
-        v += s45.x * Rab[400];
-        v += s45.y * Rab[500];
-        my[sl] += v;
+    if (PF) {
+      // step t uses (cc0, s01.., sl0); cc1 is step t+1's contribution
+      int cc0 = nct > 0 ? contrib[cs] : 0;
+      int cc1 = nct > 1 ? contrib[cs + 1] : 0;
+      double2 s01 = make_double2(0.0, 0.0), s23 = s01, s45 = s01;
+      int sl0 = 0;
+      if (nct > 0) {
+        p2_record(p2geo, cc0, s01, s23, s45);
+        sl0 = cmap[(i64)cs * 10 + b];
       }
       __syncwarp();
+      for (int t = 0; t < steps; ++t) {
+        double2 n01 = s01, n23 = s23, n45 = s45;
+        int nsl = 0, ncc = 0;
+        if (t + 1 < nct) {
+          p2_record(p2geo, cc1, n01, n23, n45);
+          nsl = cmap[((i64)cs + t + 1) * 10 + b];
+        }
+        if (t + 2 < nct) ncc = contrib[cs + t + 2];
+        if (t < nct) {
+          const double* Rab = R + (cc0 & 15) * 10 + b;
+          double v = s01.x * Rab[0];
+          v += s01.y * Rab[100];
+          v += s23.x * Rab[200];
+          v += s23.y * Rab[300];
+          v += s45.x * Rab[400];
+          v += s45.y * Rab[500];
+          my[sl0] += v;
+        }
+        cc0 = cc1;
+        cc1 = ncc;
+        s01 = n01;
+        s23 = n23;
+        s45 = n45;
+        sl0 = nsl;
+        __syncwarp();
+      }
+    } else {
+      __syncwarp();
+      for (int t = 0; t < steps; ++t) {
+        if (t < nct) {
+          const i64 ci = (i64)cs + t;
+          const int cc = contrib[ci];
+          double2 s01, s23, s45;
+          p2_record(p2geo, cc, s01, s23, s45);
+          const int sl = cmap[ci * 10 + b];
+          const double* Rab = R + (cc & 15) * 10 + b;
+          double v = s01.x * Rab[0];
+          v += s01.y * Rab[100];
+          v += s23.x * Rab[200];
+          v += s23.y * Rab[300];
+          v += s45.x * Rab[400];
+          v += s45.y * Rab[500];
+          my[sl] += v;
+        }
+        __syncwarp();
+      }
     }
     const i64 rend = r0 + 3 < nrows ? r0 + 3 : nrows;
     const int base = row_ptr[r0];
@@ -933,6 +984,15 @@ bool p2_row_gather() {
   return v;
 }
 
+// FCU_P2_PIPELINE=0 turns the P2 kernel's step pipeline off (comparison).
+bool p2_pipelined() {
+  static const bool v = [] {
+    const char* e = getenv("FCU_P2_PIPELINE");
+    return !e || atoi(e) != 0;
+  }();
+  return v;
+}
+
 bool elasticity_row_gather() {
   static const bool v = [] {
     const char* e = getenv("FCU_ELAST_ROWGATHER");
@@ -964,14 +1024,22 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
       const size_t smem = (600 + (size_t)P2W * 3 * stride) * sizeof(double);
       static bool attr_set[64] = {};
       if (smem > 48 * 1024 && !attr_set[ctx->device & 63]) {
-        CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        227 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        227 * 1024));
         attr_set[ctx->device & 63] = true;
       }
       const i64 groups = (s->nnodes + 3 * P2W - 1) / (3 * P2W);
       const int nbp = (int)std::max<i64>(1, std::min<i64>(groups, (i64)ctx->num_sms * 8));
-      k_assemble_p2_rows<<<nbp, P2W * 32, smem, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
-                                                                s->cmap.p, geo.p, s->nnodes, stride, m->val64.p,
-                                                                m->val32.p);
+      if (p2_pipelined())
+        k_assemble_p2_rows<true><<<nbp, P2W * 32, smem, ctx->stream>>>(
+            s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->cmap.p, geo.p, s->nnodes, stride, m->val64.p,
+            m->val32.p);
+      else
+        k_assemble_p2_rows<false><<<nbp, P2W * 32, smem, ctx->stream>>>(
+            s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->cmap.p, geo.p, s->nnodes, stride, m->val64.p,
+            m->val32.p);
       LAUNCH_CHECK(ctx);
       return;
     }
