@@ -256,6 +256,7 @@ def run_cuda(args, cfg):
     b_d = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
     x_d = torch.empty(n, dtype=torch.float64, device=f"cuda:{dev}")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")  # 256 MiB > L2
+    torch.cuda.synchronize()  # the inputs above were written on torch's stream, the library runs on its own
 
     def step(precision):
         M.assemble_elasticity(210e9, 0.3)
@@ -313,8 +314,14 @@ def run_cuda(args, cfg):
     # (PCG to 1e-13 on the same eliminated system; its true residual is
     # measured here with the FP64 SpMV, and in the cpu_baseline leg on the
     # oracle's own matrix)
+    # (on b scaled by 2^40, exact: unscaled, p^T A p of this system falls
+    # below cg.rs's absolute breakdown bound 1e-30 before a 1e-13 residual)
     x_ref_d = torch.empty_like(b_d)
-    _, info_ref = M.pcg(b_d, x=x_ref_d, tol=1e-13, max_iter=1000000, precision=fcu.FCU_FP64)
+    with torch.cuda.stream(stream):
+        b_scaled = b_d * 2.0 ** 40
+    _, info_ref = M.pcg(b_scaled, x=x_ref_d, tol=1e-13, max_iter=1000000, precision=fcu.FCU_FP64)
+    ctx.synchronize()
+    x_ref_d /= 2.0 ** 40
     ax = torch.empty_like(b_d)
     M.spmv(x_ref_d, ax)
     ctx.synchronize()

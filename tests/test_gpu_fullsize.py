@@ -135,11 +135,18 @@ def test_c2_solutions_against_fp64_reference(fcu, ctx, c2_oracle):
     def true_rel(x):  # residual on the oracle's matrix
         return float(np.linalg.norm(fb - O.spmv(Kb, x)) / bn)
 
-    x_ref, info_ref = M.pcg(b, tol=1e-13, max_iter=200000, precision=fcu.FCU_FP64)
+    # The tight solves run on b scaled by 2^40 (exact; the iterates scale
+    # exactly too): with E = 210e9 the inverse diagonal is ~1e-9, so at a
+    # 1e-13 residual p^T A p falls below cg.rs's absolute breakdown bound
+    # |p^T A p| < 1e-30 (cg.rs:102-107) on the unscaled system.
+    S = 2.0 ** 40
+    x_ref, info_ref = M.pcg(b * S, tol=1e-13, max_iter=200000, precision=fcu.FCU_FP64)
+    x_ref /= S
     assert true_rel(x_ref) < 1e-12
     # independent check of the reference solution: the oracle's CG (same
     # recurrence, multi-threaded loops) to the same tolerance on the CPU
-    x_cpu, it_cpu, _ = O.solve_cg_mt(Kb, fb, None, 1e-13, 200000)
+    x_cpu, it_cpu, _ = O.solve_cg_mt(Kb, fb * S, None, 1e-13, 200000)
+    x_cpu /= S
     assert _rel(x_ref, x_cpu) <= 1e-9, _rel(x_ref, x_cpu)
     assert abs(info_ref.iterations - it_cpu) <= max(5, 0.01 * it_cpu)
     for prec in (fcu.FCU_FP64, fcu.FCU_MIXED):
