@@ -653,6 +653,110 @@ __global__ void __launch_bounds__(256) k_elast_blocks(i64 nup, const int* __rest
   }
 }
 
+// Vector-P1 elasticity, row form over the gradient records: LPR lanes per
+// block row (16 when every row has at most 16 blocks, as on the Kuhn box
+// meshes, else 32), one off-diagonal block per lane. A lane sums
+// M = sum_c s_c g_a g_b^T over the block's cell list (sl_ent, ascending cell
+// order) reading two 32-byte gradient records per cell, forms
+// K = lam M + mu M^T + mu tr(M) I, and stages it in shared memory; each chunk
+// of LPR blocks is then written with contiguous stores. The diagonal block
+// comes from the row-sum identity: every cell's gradients sum to zero, so
+// sum_j M_ij = 0 and M_ii = -sum_{j != i} M_ij (symmetrised), summed over the
+// row's lanes through shared memory. Relative to the summed-per-cell diagonal
+// this moves the diagonal by a few ulps of the row's largest block.
+template <int LPR>
+__global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_ptr, const int* __restrict__ diag_pos,
+                                                    const int* __restrict__ sl_ptr,
+                                                    const unsigned* __restrict__ sl_ent,
+                                                    const double* __restrict__ rec, i64 nrows, double lam, double mu,
+                                                    double* __restrict__ v64, float* __restrict__ v32) {
+  constexpr int RPW = 32 / LPR;
+  constexpr int W = 8;
+  __shared__ double out_all[W][32 * 9];
+  __shared__ double ms_all[W][32 * 9];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int sub = lane % LPR, seg = lane / LPR;
+  double* out = out_all[wib];
+  double* ms = ms_all[wib];
+  const i64 nwarps = (i64)gridDim.x * W;
+  for (i64 r0 = ((i64)blockIdx.x * W + wib) * RPW; r0 < nrows; r0 += nwarps * RPW) {
+    const i64 row = r0 + seg;
+    const bool valid = row < nrows;
+    int rs = 0, L = 0, dl = -1;
+    if (valid) {
+      rs = row_ptr[row];
+      L = row_ptr[row + 1] - rs;
+      dl = diag_pos[row] - rs;
+    }
+    double S[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S[k] = 0.0;
+    const int nch = __reduce_max_sync(FULL, (L + LPR - 1) / LPR);
+    for (int ch = 0; ch < nch; ++ch) {
+      const int q = ch * LPR + sub;
+      if (q < L && q != dl) {
+        double M[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) M[k] = 0.0;
+        const int e1 = sl_ptr[rs + q + 1];
+        for (int e = sl_ptr[rs + q]; e < e1; ++e) {
+          const unsigned ent = sl_ent[e];
+          const unsigned c = ent >> 4, a = (ent >> 2) & 3u, b = ent & 3u;
+          double hx, hy, hz, sc, gx, gy, gz, s2;
+          load_rec(rec, c, a, hx, hy, hz, sc);
+          load_rec(rec, c, b, gx, gy, gz, s2);
+          hx *= sc;
+          hy *= sc;
+          hz *= sc;
+          M[0] += hx * gx; M[1] += hx * gy; M[2] += hx * gz;
+          M[3] += hy * gx; M[4] += hy * gy; M[5] += hy * gz;
+          M[6] += hz * gx; M[7] += hz * gy; M[8] += hz * gz;
+        }
+        const double tr = mu * (M[0] + M[4] + M[8]);
+        double* o = out + 9 * lane;
+#pragma unroll
+        for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+          for (int b2 = 0; b2 < 3; ++b2) {
+            o[3 * a2 + b2] = lam * M[3 * a2 + b2] + mu * M[3 * b2 + a2] + (a2 == b2 ? tr : 0.0);
+            S[3 * a2 + b2] += M[3 * a2 + b2];
+          }
+      }
+      __syncwarp();
+      const int n = L - ch * LPR < LPR ? L - ch * LPR : LPR;
+      const i64 base = 9 * ((i64)rs + ch * LPR);
+      for (int idx = sub; idx < 9 * n; idx += LPR) {
+        const int blk = idx / 9;
+        if (ch * LPR + blk == dl) continue;
+        const double v = out[9 * seg * LPR + idx];
+        v64[base + idx] = v;
+        v32[base + idx] = (float)v;
+      }
+      __syncwarp();
+    }
+    // diagonal block: M_ii = -sum_j M_ij, symmetrised
+#pragma unroll
+    for (int k = 0; k < 9; ++k) ms[9 * lane + k] = S[k];
+    __syncwarp();
+    double t = 0.0;
+    if (sub < 9)
+      for (int l = 0; l < LPR; ++l) t += ms[9 * (seg * LPR + l) + sub];
+    __syncwarp();
+    if (sub < 9) out[9 * seg * LPR + sub] = t;
+    __syncwarp();
+    if (valid && sub < 9 && dl >= 0) {
+      const double* T = out + 9 * seg * LPR;
+      const int a2 = sub / 3, b2 = sub - 3 * (sub / 3);
+      const double d = -0.5 * (T[3 * a2 + b2] + T[3 * b2 + a2]);
+      const double tr = -(T[0] + T[4] + T[8]);
+      const double v = (lam + mu) * d + (a2 == b2 ? mu * tr : 0.0);
+      v64[9 * ((i64)rs + dl) + sub] = v;
+      v32[9 * ((i64)rs + dl) + sub] = (float)v;
+    }
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Mass matrices (mass.rs:10-250). Entry (a, b) of cell c is s_c F[a][b]:
 // s_c = rho * measure (area |det|/2, volume |det|/6; the P2 products already
@@ -973,8 +1077,6 @@ void ensure_p2_tables(fcu_ctx ctx) {
 // Host entry points (called from api.cu)
 // ---------------------------------------------------------------------------
 
-// FCU_ELAST_ROWGATHER=1 selects the row-gather elasticity kernel (kept as the
-// comparison for the block-parallel one).
 // FCU_P2_ROWGATHER=1 selects the slot-list P2 kernel (kept as the comparison).
 bool p2_row_gather() {
   static const bool v = [] {
@@ -993,10 +1095,13 @@ bool p2_pipelined() {
   return v;
 }
 
-bool elasticity_row_gather() {
-  static const bool v = [] {
-    const char* e = getenv("FCU_ELAST_ROWGATHER");
-    return e && atoi(e) != 0;
+// FCU_ELAST_KERNEL selects the elasticity kernel: 0 = row form over the
+// gradient records (default), 1 = block-parallel form, 2 = row-gather with
+// per-contribution geometry (kept as comparisons).
+int elasticity_kernel() {
+  static const int v = [] {
+    const char* e = getenv("FCU_ELAST_KERNEL");
+    return e ? atoi(e) : 0;
   }();
   return v;
 }
@@ -1065,7 +1170,8 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
   const double Eref = cellE_dev ? 1.0 : E;
   const double lam = (Eref * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
   const double mu = Eref / (2.0 * (1.0 + nu));
-  if (elasticity_row_gather()) {
+  const int mode = elasticity_kernel();
+  if (mode == 2) {
     const int nb = assembly_blocks(ctx, s->nnodes, EWARPS);
     k_assemble_elasticity<<<nb, EWARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                               s->slot_cnt.p, s->slot_ent.p, s->cell_nodes.p,
@@ -1080,6 +1186,19 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
     k_elast_records<<<grid_for(me->nc, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
         s->cell_nodes.p, me->coords.p, me->valid.p, cellE_dev, me->nc, s->cell_rec.p);
     LAUNCH_CHECK(ctx);
+  }
+  if (mode == 0) {
+    const i64 rows_per_block = 8 * (s->max_row <= 16 ? 2 : 1);
+    const i64 need = (s->nnodes + rows_per_block - 1) / rows_per_block;
+    const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
+    if (s->max_row <= 16)
+      k_elast_rows<16><<<nbr, 256, 0, ctx->stream>>>(s->row_ptr.p, s->diag_pos.p, s->sl_ptr.p, s->sl_ent.p,
+                                                      s->cell_rec.p, s->nnodes, lam, mu, m->val64.p, m->val32.p);
+    else
+      k_elast_rows<32><<<nbr, 256, 0, ctx->stream>>>(s->row_ptr.p, s->diag_pos.p, s->sl_ptr.p, s->sl_ent.p,
+                                                      s->cell_rec.p, s->nnodes, lam, mu, m->val64.p, m->val32.p);
+    LAUNCH_CHECK(ctx);
+    return;
   }
   const i64 work = s->nup + s->nnodes;
   if (work) {

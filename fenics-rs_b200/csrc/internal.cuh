@@ -162,6 +162,11 @@ struct fcu_space_s {
   DBuf<int> up_ptr, up_slot, up_tslot;
   DBuf<unsigned> up_ent;
   DBuf<double> cell_rec;   // vector P1: per-cell gradient records (16 doubles each)
+  // Vector P1: for every stored off-diagonal block (i, j) in CSR order, the
+  // cells that couple i and j, packed as up_ent is, at sl_ent[sl_ptr[p] ..
+  // sl_ptr[p+1]) (diagonal slots have empty lists).
+  DBuf<int> sl_ptr;
+  DBuf<unsigned> sl_ent;
   // P2 scalar: for contribution t of a row (position in `contrib`) and local
   // column b, the slot of dof cell_nodes[cell][b] within the row, as an
   // offset from the row's first slot (rows of at most 255 slots; empty when

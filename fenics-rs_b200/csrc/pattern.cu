@@ -209,6 +209,20 @@ __global__ void k_up_entry_flags(const unsigned long long* __restrict__ keys, co
   }
 }
 
+__global__ void k_off_entry_flags(const unsigned long long* __restrict__ keys, const unsigned* __restrict__ vals,
+                                  i64 nE, i64 nn, unsigned long long sentinel, int* __restrict__ f) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nE; t += (i64)gridDim.x * blockDim.x) {
+    const unsigned long long key = keys[t];
+    f[t] = (key != sentinel && vals[t] != 0xFFFFFFFFu && key % nn != key / nn) ? 1 : 0;
+  }
+}
+
+__global__ void k_slot_list_ptr(const int* __restrict__ slot_first, const int* __restrict__ epos, i64 nnzb,
+                                int* __restrict__ sl_ptr) {
+  for (i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x; s < nnzb; s += (i64)gridDim.x * blockDim.x)
+    sl_ptr[s] = epos[slot_first[s]];
+}
+
 __global__ void k_up_slot_flags(const unsigned long long* __restrict__ keys, const int* __restrict__ slot_first,
                                 i64 nnzb, i64 nn, int* __restrict__ f) {
   for (i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x; s < nnzb; s += (i64)gridDim.x * blockDim.x) {
@@ -518,6 +532,21 @@ void build_space_pattern(fcu_space s) {
       LAUNCH_CHECK(ctx);
     }
     CUDA_CHECK(cudaStreamSynchronize(ctx->stream));  // nent32 is a host temporary
+
+    // lists of every off-diagonal block, in CSR order
+    k_off_entry_flags<<<grid_for(nE, 256, cap), 256, 0, ctx->stream>>>(keys_s.p, vals_s.p, nE, nn, sentinel, ef.p);
+    LAUNCH_CHECK(ctx);
+    exclusive_scan(ctx, ef.p, epos.p, nE);
+    const i64 noff = (i64)read_scalar(ctx, epos.p + nE - 1) + read_scalar(ctx, ef.p + nE - 1);
+    s->sl_ptr.alloc(nnzb + 1);
+    s->sl_ent.alloc(noff);
+    const int noff32 = (int)noff;
+    CUDA_CHECK(cudaMemcpyAsync(s->sl_ptr.p + nnzb, &noff32, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    k_slot_list_ptr<<<grid_for(nnzb, 256, cap), 256, 0, ctx->stream>>>(slot_first.p, epos.p, nnzb, s->sl_ptr.p);
+    LAUNCH_CHECK(ctx);
+    k_up_fill_entries<<<grid_for(nE, 256, cap), 256, 0, ctx->stream>>>(vals_s.p, ef.p, epos.p, nE, s->sl_ent.p);
+    LAUNCH_CHECK(ctx);
+    CUDA_CHECK(cudaStreamSynchronize(ctx->stream));  // noff32 is a host temporary
   }
 
   // --- host-side statistics -----------------------------------------------
