@@ -315,11 +315,19 @@ def run_cuda(args, cfg):
     # measured here with the FP64 SpMV, and in the cpu_baseline leg on the
     # oracle's own matrix)
     # (on b scaled by 2^40, exact: unscaled, p^T A p of this system falls
-    # below cg.rs's absolute breakdown bound 1e-30 before a 1e-13 residual)
+    # below cg.rs's absolute breakdown bound 1e-30 before a 1e-13 residual;
+    # two restarts from the iterate recompute the residual as b - A x, since
+    # one pass's recurrence residual drifts from the true one)
     x_ref_d = torch.empty_like(b_d)
+    x_tmp_d = torch.empty_like(b_d)
     with torch.cuda.stream(stream):
         b_scaled = b_d * 2.0 ** 40
     _, info_ref = M.pcg(b_scaled, x=x_ref_d, tol=1e-13, max_iter=1000000, precision=fcu.FCU_FP64)
+    ref_iters = info_ref.iterations
+    for _ in range(2):
+        _, info2 = M.pcg(b_scaled, x0=x_ref_d, x=x_tmp_d, tol=1e-13, max_iter=1000000, precision=fcu.FCU_FP64)
+        ref_iters += info2.iterations
+        x_ref_d, x_tmp_d = x_tmp_d, x_ref_d
     ctx.synchronize()
     x_ref_d /= 2.0 ** 40
     ax = torch.empty_like(b_d)
@@ -329,8 +337,8 @@ def run_cuda(args, cfg):
     ref_res = float(torch.linalg.norm(b_d - ax) / torch.linalg.norm(b_d))
     nref = float(np.linalg.norm(x_ref))
     errors = {
-        "reference_solution": f"FP64 PCG to 1e-13 ({info_ref.iterations} iterations), true relative residual "
-                              f"{ref_res:.2e}",
+        "reference_solution": f"FP64 PCG to 1e-13 in three passes, each restarted from the last iterate "
+                              f"({ref_iters} iterations), true relative residual {ref_res:.2e}",
         "mixed": float(np.linalg.norm(x_mixed - x_ref) / nref),
         "fp64": float(np.linalg.norm(x_fp64 - x_ref) / nref),
         "metric": "relative L2 error ||x - x_ref|| / ||x_ref||",

@@ -148,16 +148,17 @@ __global__ void k_p2_metric_records(const int* __restrict__ cn, const double* __
 // P2 spaces whose rows have at most 255 slots). Lanes 10g .. 10g+9 own row g
 // of the warp's three consecutive rows, lane 10g+b local column b. At each
 // step every group takes its row's next contribution (cell c with the row's
-// dof at local index a, ascending cell order), forms the element entry
-// K_e[a][b] = sum_m S_c[m] R[m][a][b] from the cell's metric record, and adds
-// it to the row's accumulator of slot cmap[t][b] in shared memory. The ten
-// columns of one cell are ten distinct dofs, so the ten lanes of a group
-// update ten distinct slots: no atomics, and every slot sums its
-// contributions in ascending cell order, as the triplet assembly does. The
-// three rows' slots are contiguous in the pattern, so the warp writes them
-// with coalesced stores. One element entry costs one metric record read
-// (shared by the group), six reference-tensor reads from shared memory, six
-// FMAs and one shared-memory add; no per-entry summation lists are read.
+// dof at local index a; contributions ordered by (a, c)), forms the element
+// entry K_e[a][b] = sum_m S_c[m] R[m][a][b] from the cell's metric record,
+// and adds it to the row's accumulator of slot cmap[t][b] in shared memory.
+// The ten columns of one cell are ten distinct dofs, so the ten lanes of a
+// group update ten distinct slots: no atomics, and every slot sums its
+// contributions in one fixed order (the values repeat bit for bit; they agree
+// with the triplet assembly's ascending-cell sums to round-off). The three
+// rows' slots are contiguous in the pattern, so the warp writes them with
+// coalesced stores. One element entry costs one metric record read (shared by
+// the group), six FMAs and one shared-memory add; no per-entry summation
+// lists are read.
 constexpr int P2W = 8;  // warps per block
 
 __device__ __forceinline__ void p2_record(const double* __restrict__ p2geo, int cc, double2& s01, double2& s23,
@@ -168,12 +169,12 @@ __device__ __forceinline__ void p2_record(const double* __restrict__ p2geo, int 
   s45 = __ldg(rec + 2);
 }
 
-// PF: software pipeline over the steps (the next step's metric record and
-// slot, and the contribution two steps ahead, are loaded before the current
-// step's arithmetic), so a step does not wait for its own loads.
-template <bool PF>
+// Each row's contributions come ordered by (local index a of the row's dof,
+// cell), so a lane keeps its six reference-tensor entries R[m][a][b] in
+// registers and reloads them from shared memory only when a changes (at most
+// four times on a vertex row, six on an edge row) instead of at every step.
 __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
-    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib_a,
     const unsigned char* __restrict__ cmap, const double* __restrict__ p2geo, i64 nrows, int stride,
     double* __restrict__ v64, float* __restrict__ v32) {
   extern __shared__ double p2sh[];
@@ -195,63 +196,36 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     }
     for (int q = b; q < L; q += 10) my[q] = 0.0;
     const int steps = __reduce_max_sync(FULL, nct);
-    if (PF) {
-      // step t uses (cc0, s01.., sl0); cc1 is step t+1's contribution
-      int cc0 = nct > 0 ? contrib[cs] : 0;
-      int cc1 = nct > 1 ? contrib[cs + 1] : 0;
-      double2 s01 = make_double2(0.0, 0.0), s23 = s01, s45 = s01;
-      int sl0 = 0;
-      if (nct > 0) {
-        p2_record(p2geo, cc0, s01, s23, s45);
-        sl0 = cmap[(i64)cs * 10 + b];
+    __syncwarp();
+    int a_cur = -1;
+    double r0v = 0.0, r1v = 0.0, r2v = 0.0, r3v = 0.0, r4v = 0.0, r5v = 0.0;
+    for (int t = 0; t < steps; ++t) {
+      if (t < nct) {
+        const i64 ci = (i64)cs + t;
+        const int cc = contrib_a[ci];
+        double2 s01, s23, s45;
+        p2_record(p2geo, cc, s01, s23, s45);
+        const int sl = cmap[ci * 10 + b];
+        const int a = cc & 15;
+        if (a != a_cur) {
+          const double* Rab = R + a * 10 + b;
+          r0v = Rab[0];
+          r1v = Rab[100];
+          r2v = Rab[200];
+          r3v = Rab[300];
+          r4v = Rab[400];
+          r5v = Rab[500];
+          a_cur = a;
+        }
+        double v = s01.x * r0v;
+        v += s01.y * r1v;
+        v += s23.x * r2v;
+        v += s23.y * r3v;
+        v += s45.x * r4v;
+        v += s45.y * r5v;
+        my[sl] += v;
       }
       __syncwarp();
-      for (int t = 0; t < steps; ++t) {
-        double2 n01 = s01, n23 = s23, n45 = s45;
-        int nsl = 0, ncc = 0;
-        if (t + 1 < nct) {
-          p2_record(p2geo, cc1, n01, n23, n45);
-          nsl = cmap[((i64)cs + t + 1) * 10 + b];
-        }
-        if (t + 2 < nct) ncc = contrib[cs + t + 2];
-        if (t < nct) {
-          const double* Rab = R + (cc0 & 15) * 10 + b;
-          double v = s01.x * Rab[0];
-          v += s01.y * Rab[100];
-          v += s23.x * Rab[200];
-          v += s23.y * Rab[300];
-          v += s45.x * Rab[400];
-          v += s45.y * Rab[500];
-          my[sl0] += v;
-        }
-        cc0 = cc1;
-        cc1 = ncc;
-        s01 = n01;
-        s23 = n23;
-        s45 = n45;
-        sl0 = nsl;
-        __syncwarp();
-      }
-    } else {
-      __syncwarp();
-      for (int t = 0; t < steps; ++t) {
-        if (t < nct) {
-          const i64 ci = (i64)cs + t;
-          const int cc = contrib[ci];
-          double2 s01, s23, s45;
-          p2_record(p2geo, cc, s01, s23, s45);
-          const int sl = cmap[ci * 10 + b];
-          const double* Rab = R + (cc & 15) * 10 + b;
-          double v = s01.x * Rab[0];
-          v += s01.y * Rab[100];
-          v += s23.x * Rab[200];
-          v += s23.y * Rab[300];
-          v += s45.x * Rab[400];
-          v += s45.y * Rab[500];
-          my[sl] += v;
-        }
-        __syncwarp();
-      }
     }
     const i64 rend = r0 + 3 < nrows ? r0 + 3 : nrows;
     const int base = row_ptr[r0];
@@ -547,25 +521,43 @@ __global__ void __launch_bounds__(256) k_elast_records(const int* __restrict__ c
                                                        const unsigned char* __restrict__ valid,
                                                        const double* __restrict__ cellE, i64 nc,
                                                        double* __restrict__ rec) {
-  for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
-    const int4 q = reinterpret_cast<const int4*>(cn)[c];
-    const int v[4] = {q.x, q.y, q.z, q.w};
-    double2* o = reinterpret_cast<double2*>(rec + 16 * c);
-    if (!valid[c]) {
+  // Each warp computes 32 consecutive cells' records, stages them in shared
+  // memory (rows of 18 doubles, so 16-byte accesses by 8 lanes hit distinct
+  // banks) and writes the 4 KB with contiguous 16-byte stores.
+  constexpr int RS = 18;
+  __shared__ double2 st_all[8][32 * RS / 2];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double2* st = st_all[wib];
+  const i64 nwarps = (i64)gridDim.x * (blockDim.x >> 5);
+  for (i64 c0 = ((i64)blockIdx.x * (blockDim.x >> 5) + wib) * 32; c0 < nc; c0 += nwarps * 32) {
+    const i64 c = c0 + lane;
+    double2* o = st + lane * (RS / 2);
+    if (c < nc && valid[c]) {
+      const int4 q = reinterpret_cast<const int4*>(cn)[c];
+      const int v[4] = {q.x, q.y, q.z, q.w};
+      const Geo3 g = tet_geometry(X, v);
+      double sc = (1.0 / 6.0) * fabs(g.det);
+      if (cellE) sc *= cellE[c];
+      o[0] = make_double2(-g.G[0][0] - g.G[0][1] - g.G[0][2], -g.G[1][0] - g.G[1][1] - g.G[1][2]);
+      o[1] = make_double2(-g.G[2][0] - g.G[2][1] - g.G[2][2], sc);
+#pragma unroll
+      for (int b = 1; b < 4; ++b) {
+        o[2 * b] = make_double2(g.G[0][b - 1], g.G[1][b - 1]);
+        o[2 * b + 1] = make_double2(g.G[2][b - 1], sc);
+      }
+    } else {
 #pragma unroll
       for (int k = 0; k < 8; ++k) o[k] = make_double2(0.0, 0.0);
-      continue;
     }
-    const Geo3 g = tet_geometry(X, v);
-    double sc = (1.0 / 6.0) * fabs(g.det);
-    if (cellE) sc *= cellE[c];
-    o[0] = make_double2(-g.G[0][0] - g.G[0][1] - g.G[0][2], -g.G[1][0] - g.G[1][1] - g.G[1][2]);
-    o[1] = make_double2(-g.G[2][0] - g.G[2][1] - g.G[2][2], sc);
+    __syncwarp();
+    const i64 ncell = nc - c0 < 32 ? nc - c0 : 32;
+    double2* dst = reinterpret_cast<double2*>(rec + 16 * c0);
 #pragma unroll
-    for (int b = 1; b < 4; ++b) {
-      o[2 * b] = make_double2(g.G[0][b - 1], g.G[1][b - 1]);
-      o[2 * b + 1] = make_double2(g.G[2][b - 1], sc);
+    for (int k = 0; k < 8; ++k) {
+      const int f = lane + 32 * k;  // 16-byte word f of the warp's 32 records
+      if (f < 8 * ncell) dst[f] = st[(f >> 3) * (RS / 2) + (f & 7)];
     }
+    __syncwarp();
   }
 }
 
@@ -1086,15 +1078,6 @@ bool p2_row_gather() {
   return v;
 }
 
-// FCU_P2_PIPELINE=0 turns the P2 kernel's step pipeline off (comparison).
-bool p2_pipelined() {
-  static const bool v = [] {
-    const char* e = getenv("FCU_P2_PIPELINE");
-    return !e || atoi(e) != 0;
-  }();
-  return v;
-}
-
 // FCU_ELAST_KERNEL selects the elasticity kernel: 0 = row form over the
 // gradient records (default), 1 = block-parallel form, 2 = row-gather with
 // per-contribution geometry (kept as comparisons).
@@ -1124,27 +1107,19 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
     k_p2_metric_records<<<grid_for(me->nc, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
         s->cell_nodes.p, me->coords.p, coef_dev, me->nc, geo.p);
     LAUNCH_CHECK(ctx);
-    if (s->cmap.p && !p2_row_gather()) {
+    if (s->cmap.p && s->contrib_a.p && !p2_row_gather()) {
       const int stride = s->max_row | 1;  // odd, so the three rows' accumulators start in different banks
       const size_t smem = (600 + (size_t)P2W * 3 * stride) * sizeof(double);
       static bool attr_set[64] = {};
       if (smem > 48 * 1024 && !attr_set[ctx->device & 63]) {
-        CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        227 * 1024));
-        CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        227 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         attr_set[ctx->device & 63] = true;
       }
       const i64 groups = (s->nnodes + 3 * P2W - 1) / (3 * P2W);
       const int nbp = (int)std::max<i64>(1, std::min<i64>(groups, (i64)ctx->num_sms * 8));
-      if (p2_pipelined())
-        k_assemble_p2_rows<true><<<nbp, P2W * 32, smem, ctx->stream>>>(
-            s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->cmap.p, geo.p, s->nnodes, stride, m->val64.p,
-            m->val32.p);
-      else
-        k_assemble_p2_rows<false><<<nbp, P2W * 32, smem, ctx->stream>>>(
-            s->row_ptr.p, s->contrib_ptr.p, s->contrib.p, s->cmap.p, geo.p, s->nnodes, stride, m->val64.p,
-            m->val32.p);
+      k_assemble_p2_rows<<<nbp, P2W * 32, smem, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib_a.p,
+                                                                s->cmap.p, geo.p, s->nnodes, stride, m->val64.p,
+                                                                m->val32.p);
       LAUNCH_CHECK(ctx);
       return;
     }
@@ -1183,7 +1158,7 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
   fcu_mesh me = s->mesh;
   if (!s->cell_rec.p) s->cell_rec.alloc((size_t)me->nc * 16);
   if (me->nc) {
-    k_elast_records<<<grid_for(me->nc, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
+    k_elast_records<<<grid_for((me->nc + 31) / 32 * 32, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
         s->cell_nodes.p, me->coords.p, me->valid.p, cellE_dev, me->nc, s->cell_rec.p);
     LAUNCH_CHECK(ctx);
   }

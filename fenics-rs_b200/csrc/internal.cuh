@@ -167,11 +167,14 @@ struct fcu_space_s {
   // sl_ptr[p+1]) (diagonal slots have empty lists).
   DBuf<int> sl_ptr;
   DBuf<unsigned> sl_ent;
-  // P2 scalar: for contribution t of a row (position in `contrib`) and local
+  // P2 scalar: for contribution t of a row (position in `contrib_a`) and local
   // column b, the slot of dof cell_nodes[cell][b] within the row, as an
   // offset from the row's first slot (rows of at most 255 slots; empty when
   // a longer row exists).
   DBuf<unsigned char> cmap;
+  // P2 scalar: the row's contributions ordered by (local index, cell); cmap
+  // follows this order when contrib_a is present.
+  DBuf<int> contrib_a;
 };
 
 struct fcu_matrix_s {

@@ -294,6 +294,29 @@ __global__ void k_contrib_slot_map(const unsigned long long* __restrict__ keys, 
   }
 }
 
+// P2 contributions reordered by (row, local index of the row's dof, cell),
+// so that the assembly kernel can keep one reference-tensor row in
+// registers across the contributions that share it.
+__global__ void k_contrib_sort_keys(const int* __restrict__ contrib_ptr, const int* __restrict__ contrib, i64 nn,
+                                    unsigned long long* __restrict__ keys, int* __restrict__ idx) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < nn; i += (i64)gridDim.x * blockDim.x)
+    for (int t = contrib_ptr[i]; t < contrib_ptr[i + 1]; ++t) {
+      const unsigned cc = (unsigned)contrib[t];
+      keys[t] = ((unsigned long long)i << 32) | ((unsigned long long)(cc & 15u) << 28) | (cc >> 4);
+      idx[t] = t;
+    }
+}
+
+__global__ void k_contrib_permute(const int* __restrict__ order, const int* __restrict__ contrib,
+                                  const unsigned char* __restrict__ cmap, i64 nct, int k,
+                                  int* __restrict__ contrib_a, unsigned char* __restrict__ cmap_a) {
+  for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nct; t += (i64)gridDim.x * blockDim.x) {
+    const int src = order[t];
+    contrib_a[t] = contrib[src];
+    for (int b = 0; b < k; ++b) cmap_a[t * k + b] = cmap[(i64)src * k + b];
+  }
+}
+
 __global__ void k_u32_to_u16(const unsigned* __restrict__ a, i64 n, unsigned short* __restrict__ b,
                              int* __restrict__ overflow) {
   for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n; t += (i64)gridDim.x * blockDim.x) {
@@ -573,6 +596,28 @@ void build_space_pattern(fcu_space s) {
                                                                         sentinel, s->row_ptr.p, s->contrib_ptr.p,
                                                                         s->contrib.p, s->cmap.p);
     LAUNCH_CHECK(ctx);
+    if (nc < (1ll << 28)) {
+      // reorder each row's contributions by (local index, cell), map along
+      DBuf<unsigned long long> ck, cks;
+      DBuf<int> ci, cis;
+      ck.alloc(ncontrib); cks.alloc(ncontrib); ci.alloc(ncontrib); cis.alloc(ncontrib);
+      k_contrib_sort_keys<<<grid_for(nn, 256, cap), 256, 0, ctx->stream>>>(s->contrib_ptr.p, s->contrib.p, nn, ck.p,
+                                                                            ci.p);
+      LAUNCH_CHECK(ctx);
+      const int kb = 32 + bit_length((unsigned long long)nn);
+      size_t tb = 0;
+      CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tb, ck.p, cks.p, ci.p, cis.p, (int)ncontrib, 0, kb,
+                                                 ctx->stream));
+      CUDA_CHECK(cub::DeviceRadixSort::SortPairs(ctx->temp_bytes(tb), tb, ck.p, cks.p, ci.p, cis.p, (int)ncontrib, 0,
+                                                 kb, ctx->stream));
+      s->contrib_a.alloc(ncontrib);
+      DBuf<unsigned char> cm;
+      cm.alloc((i64)k * ncontrib);
+      k_contrib_permute<<<grid_for(ncontrib, 256, cap), 256, 0, ctx->stream>>>(cis.p, s->contrib.p, s->cmap.p,
+                                                                               ncontrib, k, s->contrib_a.p, cm.p);
+      LAUNCH_CHECK(ctx);
+      s->cmap = std::move(cm);
+    }
   }
 }
 
