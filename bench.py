@@ -362,8 +362,8 @@ def run_cuda(args, cfg):
     step(fcu.FCU_MIXED)
 
     # dominant kernel: the FP32 3x3-block SpMV of the mixed PCG, timed cold
-    # (L2 flushed before each launch, as inside a solve whose operator
-    # exceeds L2) and warm (back-to-back launches: the 85 MB operator then
+    # (L2 evicted by a read sweep before each launch, as inside a solve whose
+    # operator exceeds L2, and as an ncu capture starts) and warm (back-to-back launches: the 85 MB operator then
     # partly stays in the 126 MB L2, as it does inside the C2 solve)
     spmv_ms, spmv_bytes = M.time_spmv(fcu.FCU_MIXED, reps=20, cold=True)
     spmv_warm_ms, _ = M.time_spmv(fcu.FCU_MIXED, reps=50)
@@ -423,7 +423,7 @@ def run_cuda(args, cfg):
                                "tiles, p.Ap partials)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "bytes_per_launch": spmv_bytes,
-                     "timing": "mean of 20 single launches, each after a 256 MiB write that flushes L2",
+                     "timing": "mean of 20 single launches, each after a 256 MiB read sweep that evicts L2 (clean lines, as an ncu cache flush leaves it)",
                      "warm": {"ms": spmv_warm_ms, "frac": spmv_bytes / (spmv_warm_ms * 1e-3) / 1e9 / peak,
                               "timing": "mean of 50 back-to-back launches"}},
         "clocks": clk.summary(),

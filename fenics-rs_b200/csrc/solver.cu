@@ -2085,9 +2085,22 @@ void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* b
   *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
 }
 
-// The same with L2 flushed before each launch: a memset of `flush_bytes`
+// Reads `n` 16-byte words and keeps one word per thread in `sink` (so the
+// loads are not removed): a read-only sweep that evicts L2 without leaving
+// dirty lines behind, whose write-back would otherwise land in the timed
+// launch.
+__global__ void k_flush_read(const uint4* __restrict__ buf, i64 n, uint4* __restrict__ sink) {
+  uint4 acc = make_uint4(0u, 0u, 0u, 0u);
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const uint4 v = __ldcg(buf + i);
+    acc.x ^= v.x; acc.y ^= v.y; acc.z ^= v.z; acc.w ^= v.w;
+  }
+  sink[blockIdx.x * (i64)blockDim.x + threadIdx.x] = acc;
+}
+
+// The same with L2 flushed before each launch: a read of `flush_bytes`
 // evicts the matrix and p, then one SpMV is timed by events on either side.
-// The memset is queued before the first event, so the launch never waits on
+// The sweep is queued before the first event, so the launch never waits on
 // the host. Returns the mean single-launch time.
 void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_bytes, double* ms, double* bytes) {
   const bool mixed = precision == FCU_MIXED;
@@ -2097,14 +2110,21 @@ void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_byt
   spmv_timing_state(m, w, mixed);
   fcu_ctx ctx = m->ctx;
   if (!flush_bytes) flush_bytes = 256ull << 20;
+  flush_bytes = (flush_bytes + 15) / 16 * 16;
   DBuf<unsigned char> flush;
   flush.alloc(flush_bytes);
+  CUDA_CHECK(cudaMemsetAsync(flush.p, 0, flush_bytes, ctx->stream));
+  const int fgrid = ctx->num_sms * 8;
+  DBuf<uint4> sink;
+  sink.alloc((size_t)fgrid * 256);
   cudaEvent_t e0, e1;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
   double total = 0.0;
   for (int r = 0; r < reps; ++r) {
-    CUDA_CHECK(cudaMemsetAsync(flush.p, r & 0xff, flush_bytes, ctx->stream));
+    k_flush_read<<<fgrid, 256, 0, ctx->stream>>>(reinterpret_cast<const uint4*>(flush.p), (i64)(flush_bytes / 16),
+                                                 sink.p);
+    CUDA_CHECK(cudaGetLastError());
     CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
     enqueue_spmv(m, w, mixed);
     CUDA_CHECK(cudaEventRecord(e1, ctx->stream));

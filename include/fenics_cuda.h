@@ -402,8 +402,9 @@ int fcu_device_name(int device, char* name, size_t len);
 int fcu_time_spmv(fcu_ctx ctx, fcu_matrix m, int precision, int reps, double* ms_per_launch,
                   double* bytes_per_launch);
 /* As fcu_time_spmv, with the L2 cache flushed before every timed launch: a
- * write of `flush_bytes` (at least the L2 size; 0 picks 256 MiB) to a buffer
- * the call allocates, then one launch bracketed by CUDA events. Returns the
+ * read of `flush_bytes` (at least the L2 size; 0 picks 256 MiB) from a buffer
+ * the call allocates (a read, so no dirty lines are written back during the
+ * timed launch), then one launch bracketed by CUDA events. Returns the
  * mean of the `reps` single-launch times, so the matrix and the operand
  * vector come from HBM as they do inside a solve whose operator exceeds L2. */
 int fcu_time_spmv_cold(fcu_ctx ctx, fcu_matrix m, int precision, int reps, size_t flush_bytes,
