@@ -749,6 +749,121 @@ __global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_
   }
 }
 
+// Vector-P1 elasticity, row form with the records staged (the kernel
+// fcu_assemble_elasticity runs when every row has at most 16 blocks and 24
+// cells, as on the Kuhn box meshes). Each half-warp owns one block row: it
+// copies the 128-byte records of the row's cells into shared memory with
+// contiguous 16-byte loads (eight lanes per record), then every lane walks the
+// (cell, column) list of its block from shared memory, as k_elast_rows does
+// from global memory. Gathering the records per lane from global memory
+// costs one L1 sector request per gradient; staging them costs four per cell.
+constexpr int ES_W = 4;      // warps per block, two rows per warp
+constexpr int ES_MAXC = 24;  // staged cells per row
+constexpr int ES_RS = 18;    // record stride in shared memory, doubles (144 B: 16-byte aligned, spreads banks)
+
+__global__ void __launch_bounds__(ES_W * 32) k_elast_rows_staged(
+    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
+    const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
+    const int* __restrict__ diag_pos, const double* __restrict__ rec, i64 nrows, double lam, double mu,
+    double* __restrict__ v64, float* __restrict__ v32) {
+  __shared__ __align__(16) double recs_all[ES_W][2][ES_MAXC * ES_RS];
+  __shared__ unsigned short ents_all[ES_W][2][4 * ES_MAXC];
+  __shared__ unsigned char aof_all[ES_W][2][ES_MAXC];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int seg = lane >> 4, sub = lane & 15;
+  double* R = recs_all[wib][seg];
+  unsigned short* E = ents_all[wib][seg];
+  unsigned char* A = aof_all[wib][seg];
+  const i64 nwarps = (i64)gridDim.x * ES_W;
+  for (i64 r0 = ((i64)blockIdx.x * ES_W + wib) * 2; r0 < nrows; r0 += nwarps * 2) {
+    const i64 row = r0 + seg;
+    int rs = 0, L = 0, cs = 0, nct = 0, dl = -1;
+    if (row < nrows) {
+      rs = row_ptr[row];
+      L = row_ptr[row + 1] - rs;
+      cs = contrib_ptr[row];
+      nct = contrib_ptr[row + 1] - cs;
+      dl = diag_pos[row] - rs;
+    }
+    // stage the cells' records, their local indices and the row's entry lists
+    for (int w = sub; w < 8 * nct; w += 16) {
+      const int t = w >> 3, k = w & 7;
+      const int cc = contrib[cs + t];
+      const double2 v = __ldg(reinterpret_cast<const double2*>(rec + 16 * (i64)(cc >> 4)) + k);
+      *reinterpret_cast<double2*>(R + t * ES_RS + 2 * k) = v;
+    }
+    for (int t = sub; t < nct; t += 16) A[t] = (unsigned char)(contrib[cs + t] & 15);
+    for (int q = sub; q < 4 * nct; q += 16) E[q] = slot_ent[4 * (i64)cs + q];
+    // the block's entries: a segmented exclusive scan of the row's slot counts
+    const int cnt = sub < L ? (int)slot_cnt[rs + sub] : 0;
+    int x = cnt;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, x, o, 16);
+      if (sub >= o) x += y;
+    }
+    const int off = x - cnt;
+    __syncwarp();
+    double M[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) M[k] = 0.0;
+    const bool own = sub < L && sub != dl;
+    if (own) {
+      for (int e = off; e < off + cnt; ++e) {
+        const unsigned ent = E[e];
+        const int t = (int)(ent >> 4), b = (int)(ent & 15u);
+        const double* rt = R + t * ES_RS;
+        const double2 h01 = *reinterpret_cast<const double2*>(rt + 4 * A[t]);
+        const double2 h2s = *reinterpret_cast<const double2*>(rt + 4 * A[t] + 2);
+        const double2 g01 = *reinterpret_cast<const double2*>(rt + 4 * b);
+        const double2 g2s = *reinterpret_cast<const double2*>(rt + 4 * b + 2);
+        const double hx = h2s.y * h01.x, hy = h2s.y * h01.y, hz = h2s.y * h2s.x;
+        M[0] += hx * g01.x; M[1] += hx * g01.y; M[2] += hx * g2s.x;
+        M[3] += hy * g01.x; M[4] += hy * g01.y; M[5] += hy * g2s.x;
+        M[6] += hz * g01.x; M[7] += hz * g01.y; M[8] += hz * g2s.x;
+      }
+    }
+    __syncwarp();
+    // the records are no longer needed: their space holds the row's blocks
+    // (9 x 16 doubles) and the lanes' M for the row sum (9 x 16 doubles)
+    double* out = R;
+    double* ms = R + 9 * 16;
+    if (own) {
+      const double tr = mu * (M[0] + M[4] + M[8]);
+#pragma unroll
+      for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+        for (int b2 = 0; b2 < 3; ++b2)
+          out[9 * sub + 3 * a2 + b2] = lam * M[3 * a2 + b2] + mu * M[3 * b2 + a2] + (a2 == b2 ? tr : 0.0);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) ms[9 * sub + k] = M[k];
+    __syncwarp();
+    const i64 base = 9 * (i64)rs;
+    for (int idx = sub; idx < 9 * L; idx += 16) {
+      if (idx / 9 == dl) continue;
+      const double v = out[idx];
+      v64[base + idx] = v;
+      v32[base + idx] = (float)v;
+    }
+    double tsum = 0.0;
+    if (sub < 9)
+      for (int l = 0; l < 16; ++l) tsum += ms[9 * l + sub];
+    __syncwarp();
+    if (sub < 9) ms[sub] = tsum;
+    __syncwarp();
+    if (row < nrows && sub < 9 && dl >= 0) {
+      const int a2 = sub / 3, b2 = sub - 3 * (sub / 3);
+      const double d = -0.5 * (ms[3 * a2 + b2] + ms[3 * b2 + a2]);
+      const double tr = -(ms[0] + ms[4] + ms[8]);
+      const double v = (lam + mu) * d + (a2 == b2 ? mu * tr : 0.0);
+      v64[9 * ((i64)rs + dl) + sub] = v;
+      v32[9 * ((i64)rs + dl) + sub] = (float)v;
+    }
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Mass matrices (mass.rs:10-250). Entry (a, b) of cell c is s_c F[a][b]:
 // s_c = rho * measure (area |det|/2, volume |det|/6; the P2 products already
@@ -1079,8 +1194,10 @@ bool p2_row_gather() {
 }
 
 // FCU_ELAST_KERNEL selects the elasticity kernel: 0 = row form over the
-// gradient records (default), 1 = block-parallel form, 2 = row-gather with
-// per-contribution geometry (kept as comparisons).
+// gradient records (default; staged in shared memory when the rows are
+// short, else read from global memory), 3 = the unstaged row form always,
+// 1 = block-parallel form, 2 = row-gather with per-contribution geometry
+// (kept as comparisons).
 int elasticity_kernel() {
   static const int v = [] {
     const char* e = getenv("FCU_ELAST_KERNEL");
@@ -1162,7 +1279,17 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
         s->cell_nodes.p, me->coords.p, me->valid.p, cellE_dev, me->nc, s->cell_rec.p);
     LAUNCH_CHECK(ctx);
   }
-  if (mode == 0) {
+  if (mode == 0 && s->max_row <= 16 && s->max_contrib <= ES_MAXC) {
+    const i64 need = (s->nnodes + 2 * ES_W - 1) / (2 * ES_W);
+    const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
+    k_elast_rows_staged<<<nbr, ES_W * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
+                                                            s->slot_cnt.p, s->slot_ent.p, s->diag_pos.p,
+                                                            s->cell_rec.p, s->nnodes, lam, mu, m->val64.p,
+                                                            m->val32.p);
+    LAUNCH_CHECK(ctx);
+    return;
+  }
+  if (mode == 0 || mode == 3) {
     const i64 rows_per_block = 8 * (s->max_row <= 16 ? 2 : 1);
     const i64 need = (s->nnodes + rows_per_block - 1) / rows_per_block;
     const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
