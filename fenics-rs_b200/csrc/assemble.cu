@@ -173,6 +173,18 @@ __device__ __forceinline__ void p2_record(const double* __restrict__ p2geo, int 
 // cell), so a lane keeps its six reference-tensor entries R[m][a][b] in
 // registers and reloads them from shared memory only when a changes (at most
 // four times on a vertex row, six on an edge row) instead of at every step.
+// The per-contribution inputs of a row (metric records, local indices and
+// slot maps, up to P2_MAXC contributions at a time) are staged in shared
+// memory with contiguous loads before the steps, so a step reads only shared
+// memory: one broadcast record read per group, one slot byte, and the
+// accumulator update.
+constexpr int P2_MAXC = 32;
+
+__host__ __device__ constexpr size_t p2_smem_bytes(int stride) {
+  return (600 + (size_t)P2W * 3 * stride + (size_t)P2W * 3 * P2_MAXC * 6) * sizeof(double) +
+         (size_t)P2W * 3 * P2_MAXC * (10 + 1);
+}
+
 __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib_a,
     const unsigned char* __restrict__ cmap, const double* __restrict__ p2geo, i64 nrows, int stride,
@@ -183,8 +195,14 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
   for (int q = threadIdx.x; q < 600; q += blockDim.x) R[q] = (&c_p2_R[0][0][0])[q];
   __syncthreads();
   const int g = lane / 10, b = lane - 10 * g;  // g == 3 on lanes 30 and 31
+  const int gg0 = g < 3 ? g : 0;
   double* acc = p2sh + 600 + (i64)wib * 3 * stride;
-  double* my = acc + (g < 3 ? g : 0) * stride;
+  double* my = acc + gg0 * stride;
+  double* Sst = p2sh + 600 + (i64)P2W * 3 * stride + ((i64)wib * 3 + gg0) * P2_MAXC * 6;
+  unsigned char* bytes = reinterpret_cast<unsigned char*>(p2sh + 600 + (i64)P2W * 3 * stride +
+                                                           (i64)P2W * 3 * P2_MAXC * 6);
+  unsigned char* Ast = bytes + ((i64)wib * 3 + gg0) * P2_MAXC;
+  unsigned char* CMst = bytes + (i64)P2W * 3 * P2_MAXC + ((i64)wib * 3 + gg0) * P2_MAXC * 10;
   const i64 nwarps = (i64)gridDim.x * P2W;
   for (i64 r0 = ((i64)blockIdx.x * P2W + wib) * 3; r0 < nrows; r0 += nwarps * 3) {
     const i64 row = r0 + g;
@@ -195,37 +213,49 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
       nct = contrib_ptr[row + 1] - cs;
     }
     for (int q = b; q < L; q += 10) my[q] = 0.0;
-    const int steps = __reduce_max_sync(FULL, nct);
-    __syncwarp();
+    const int nch = __reduce_max_sync(FULL, (nct + P2_MAXC - 1) / P2_MAXC);
     int a_cur = -1;
     double r0v = 0.0, r1v = 0.0, r2v = 0.0, r3v = 0.0, r4v = 0.0, r5v = 0.0;
-    for (int t = 0; t < steps; ++t) {
-      if (t < nct) {
-        const i64 ci = (i64)cs + t;
-        const int cc = contrib_a[ci];
-        double2 s01, s23, s45;
-        p2_record(p2geo, cc, s01, s23, s45);
-        const int sl = cmap[ci * 10 + b];
-        const int a = cc & 15;
-        if (a != a_cur) {
-          const double* Rab = R + a * 10 + b;
-          r0v = Rab[0];
-          r1v = Rab[100];
-          r2v = Rab[200];
-          r3v = Rab[300];
-          r4v = Rab[400];
-          r5v = Rab[500];
-          a_cur = a;
-        }
-        double v = s01.x * r0v;
-        v += s01.y * r1v;
-        v += s23.x * r2v;
-        v += s23.y * r3v;
-        v += s45.x * r4v;
-        v += s45.y * r5v;
-        my[sl] += v;
-      }
+    for (int ch = 0; ch < nch; ++ch) {
+      const int c0 = ch * P2_MAXC;
+      const int n = nct - c0 < P2_MAXC ? (nct - c0 > 0 ? nct - c0 : 0) : P2_MAXC;
+      const i64 cb = (i64)cs + c0;
       __syncwarp();
+      for (int w = b; w < 3 * n; w += 10) {
+        const int t = w / 3, k = w - 3 * t;
+        const int cc = contrib_a[cb + t];
+        reinterpret_cast<double2*>(Sst)[3 * t + k] =
+            __ldg(reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO) + k);
+      }
+      for (int t = b; t < n; t += 10) Ast[t] = (unsigned char)(contrib_a[cb + t] & 15);
+      for (int q = b; q < 10 * n; q += 10) CMst[q] = cmap[cb * 10 + q];
+      const int steps = __reduce_max_sync(FULL, n);
+      __syncwarp();
+      for (int t = 0; t < steps; ++t) {
+        if (t < n) {
+          const int a = Ast[t];
+          if (a != a_cur) {
+            const double* Rab = R + a * 10 + b;
+            r0v = Rab[0];
+            r1v = Rab[100];
+            r2v = Rab[200];
+            r3v = Rab[300];
+            r4v = Rab[400];
+            r5v = Rab[500];
+            a_cur = a;
+          }
+          const double2* S = reinterpret_cast<const double2*>(Sst) + 3 * t;
+          const double2 s01 = S[0], s23 = S[1], s45 = S[2];
+          double v = s01.x * r0v;
+          v += s01.y * r1v;
+          v += s23.x * r2v;
+          v += s23.y * r3v;
+          v += s45.x * r4v;
+          v += s45.y * r5v;
+          my[CMst[10 * t + b]] += v;
+        }
+        __syncwarp();
+      }
     }
     const i64 rend = r0 + 3 < nrows ? r0 + 3 : nrows;
     const int base = row_ptr[r0];
@@ -233,8 +263,8 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     const int off1 = row_ptr[r0 + 1 < rend ? r0 + 1 : rend] - base;
     const int off2 = row_ptr[r0 + 2 < rend ? r0 + 2 : rend] - base;
     for (int q = lane; q < tot; q += 32) {
-      const int gg = q >= off2 ? 2 : (q >= off1 ? 1 : 0);
-      const double v = acc[gg * stride + q - (gg == 2 ? off2 : gg == 1 ? off1 : 0)];
+      const int gq = q >= off2 ? 2 : (q >= off1 ? 1 : 0);
+      const double v = acc[gq * stride + q - (gq == 2 ? off2 : gq == 1 ? off1 : 0)];
       v64[base + q] = v;
       v32[base + q] = (float)v;
     }
@@ -648,20 +678,34 @@ __global__ void __launch_bounds__(256) k_elast_blocks(i64 nup, const int* __rest
 // Vector-P1 elasticity, row form over the gradient records: LPR lanes per
 // block row (16 when every row has at most 16 blocks, as on the Kuhn box
 // meshes, else 32), one off-diagonal block per lane. A lane sums
-// M = sum_c s_c g_a g_b^T over the block's cell list (sl_ent, ascending cell
-// order) reading two 32-byte gradient records per cell, forms
+// M = sum_c s_c (g_a g_b^T) over the block's cell list (sl_ent, ascending
+// cell order) reading two 32-byte gradient records per cell, two cells per
+// round so that four record loads are in flight, forms
 // K = lam M + mu M^T + mu tr(M) I, and stages it in shared memory; each chunk
-// of LPR blocks is then written with contiguous stores. The diagonal block
-// comes from the row-sum identity: every cell's gradients sum to zero, so
+// of LPR blocks is then written with contiguous stores. Each product
+// g_a[i] g_b[j] is rounded before it is scaled by s_c, so block (j, i) comes
+// out as the exact transpose of block (i, j): the assembled matrix, and its
+// FP32 copy, are exactly symmetric. The diagonal block comes from the
+// row-sum identity: every cell's gradients sum to zero, so
 // sum_j M_ij = 0 and M_ii = -sum_{j != i} M_ij (symmetrised), summed over the
-// row's lanes through shared memory. Relative to the summed-per-cell diagonal
-// this moves the diagonal by a few ulps of the row's largest block.
+// row's lanes through shared memory; relative to the summed-per-cell
+// diagonal this moves it by a few ulps of the row's largest block.
+__device__ __forceinline__ void elast_accumulate(double (&M)[9], double s, double2 a01, double2 a2s, double2 b01,
+                                                 double2 b2s) {
+  const double ga[3] = {a01.x, a01.y, a2s.x}, gb[3] = {b01.x, b01.y, b2s.x};
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) M[3 * i + j] = fma(s, ga[i] * gb[j], M[3 * i + j]);
+}
+
 template <int LPR>
-__global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_ptr, const int* __restrict__ diag_pos,
-                                                    const int* __restrict__ sl_ptr,
-                                                    const unsigned* __restrict__ sl_ent,
-                                                    const double* __restrict__ rec, i64 nrows, double lam, double mu,
-                                                    double* __restrict__ v64, float* __restrict__ v32) {
+__global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ row_ptr,
+                                                       const int* __restrict__ diag_pos,
+                                                       const int* __restrict__ sl_ptr,
+                                                       const unsigned* __restrict__ sl_ent,
+                                                       const double* __restrict__ rec, i64 nrows, double lam,
+                                                       double mu, double* __restrict__ v64, float* __restrict__ v32) {
   constexpr int RPW = 32 / LPR;
   constexpr int W = 8;
   __shared__ double out_all[W][32 * 9];
@@ -670,6 +714,7 @@ __global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_
   const int sub = lane % LPR, seg = lane / LPR;
   double* out = out_all[wib];
   double* ms = ms_all[wib];
+  const double2* R2 = reinterpret_cast<const double2*>(rec);
   const i64 nwarps = (i64)gridDim.x * W;
   for (i64 r0 = ((i64)blockIdx.x * W + wib) * RPW; r0 < nrows; r0 += nwarps * RPW) {
     const i64 row = r0 + seg;
@@ -680,9 +725,8 @@ __global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_
       L = row_ptr[row + 1] - rs;
       dl = diag_pos[row] - rs;
     }
-    double S[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) S[k] = 0.0;
+    for (int k = 0; k < 9; ++k) ms[9 * lane + k] = 0.0;
     const int nch = __reduce_max_sync(FULL, (L + LPR - 1) / LPR);
     for (int ch = 0; ch < nch; ++ch) {
       const int q = ch * LPR + sub;
@@ -690,19 +734,25 @@ __global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_
         double M[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) M[k] = 0.0;
+        int e = sl_ptr[rs + q];
         const int e1 = sl_ptr[rs + q + 1];
-        for (int e = sl_ptr[rs + q]; e < e1; ++e) {
-          const unsigned ent = sl_ent[e];
-          const unsigned c = ent >> 4, a = (ent >> 2) & 3u, b = ent & 3u;
-          double hx, hy, hz, sc, gx, gy, gz, s2;
-          load_rec(rec, c, a, hx, hy, hz, sc);
-          load_rec(rec, c, b, gx, gy, gz, s2);
-          hx *= sc;
-          hy *= sc;
-          hz *= sc;
-          M[0] += hx * gx; M[1] += hx * gy; M[2] += hx * gz;
-          M[3] += hy * gx; M[4] += hy * gy; M[5] += hy * gz;
-          M[6] += hz * gx; M[7] += hz * gy; M[8] += hz * gz;
+        for (; e + 1 < e1; e += 2) {
+          const unsigned u0 = sl_ent[e], u1 = sl_ent[e + 1];
+          const double2* pa0 = R2 + 8 * (i64)(u0 >> 4) + 2 * ((u0 >> 2) & 3u);
+          const double2* pb0 = R2 + 8 * (i64)(u0 >> 4) + 2 * (u0 & 3u);
+          const double2* pa1 = R2 + 8 * (i64)(u1 >> 4) + 2 * ((u1 >> 2) & 3u);
+          const double2* pb1 = R2 + 8 * (i64)(u1 >> 4) + 2 * (u1 & 3u);
+          const double2 a01 = __ldg(pa0), a2s = __ldg(pa0 + 1), b01 = __ldg(pb0), b2s = __ldg(pb0 + 1);
+          const double2 c01 = __ldg(pa1), c2s = __ldg(pa1 + 1), d01 = __ldg(pb1), d2s = __ldg(pb1 + 1);
+          elast_accumulate(M, a2s.y, a01, a2s, b01, b2s);
+          elast_accumulate(M, c2s.y, c01, c2s, d01, d2s);
+        }
+        if (e < e1) {
+          const unsigned u0 = sl_ent[e];
+          const double2* pa0 = R2 + 8 * (i64)(u0 >> 4) + 2 * ((u0 >> 2) & 3u);
+          const double2* pb0 = R2 + 8 * (i64)(u0 >> 4) + 2 * (u0 & 3u);
+          const double2 a01 = __ldg(pa0), a2s = __ldg(pa0 + 1), b01 = __ldg(pb0), b2s = __ldg(pb0 + 1);
+          elast_accumulate(M, a2s.y, a01, a2s, b01, b2s);
         }
         const double tr = mu * (M[0] + M[4] + M[8]);
         double* o = out + 9 * lane;
@@ -711,7 +761,7 @@ __global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_
 #pragma unroll
           for (int b2 = 0; b2 < 3; ++b2) {
             o[3 * a2 + b2] = lam * M[3 * a2 + b2] + mu * M[3 * b2 + a2] + (a2 == b2 ? tr : 0.0);
-            S[3 * a2 + b2] += M[3 * a2 + b2];
+            ms[9 * lane + 3 * a2 + b2] += M[3 * a2 + b2];
           }
       }
       __syncwarp();
@@ -727,9 +777,6 @@ __global__ void __launch_bounds__(256) k_elast_rows(const int* __restrict__ row_
       __syncwarp();
     }
     // diagonal block: M_ii = -sum_j M_ij, symmetrised
-#pragma unroll
-    for (int k = 0; k < 9; ++k) ms[9 * lane + k] = S[k];
-    __syncwarp();
     double t = 0.0;
     if (sub < 9)
       for (int l = 0; l < LPR; ++l) t += ms[9 * (seg * LPR + l) + sub];
@@ -1194,10 +1241,9 @@ bool p2_row_gather() {
 }
 
 // FCU_ELAST_KERNEL selects the elasticity kernel: 0 = row form over the
-// gradient records (default; staged in shared memory when the rows are
-// short, else read from global memory), 3 = the unstaged row form always,
-// 1 = block-parallel form, 2 = row-gather with per-contribution geometry
-// (kept as comparisons).
+// gradient records (default), 4 = the same with the records staged in
+// shared memory per row, 1 = block-parallel form, 2 = row-gather with
+// per-contribution geometry (kept as comparisons).
 int elasticity_kernel() {
   static const int v = [] {
     const char* e = getenv("FCU_ELAST_KERNEL");
@@ -1226,7 +1272,7 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
     LAUNCH_CHECK(ctx);
     if (s->cmap.p && s->contrib_a.p && !p2_row_gather()) {
       const int stride = s->max_row | 1;  // odd, so the three rows' accumulators start in different banks
-      const size_t smem = (600 + (size_t)P2W * 3 * stride) * sizeof(double);
+      const size_t smem = p2_smem_bytes(stride);
       static bool attr_set[64] = {};
       if (smem > 48 * 1024 && !attr_set[ctx->device & 63]) {
         CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
@@ -1279,7 +1325,7 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
         s->cell_nodes.p, me->coords.p, me->valid.p, cellE_dev, me->nc, s->cell_rec.p);
     LAUNCH_CHECK(ctx);
   }
-  if (mode == 0 && s->max_row <= 16 && s->max_contrib <= ES_MAXC) {
+  if (mode == 4 && s->max_row <= 16 && s->max_contrib <= ES_MAXC) {
     const i64 need = (s->nnodes + 2 * ES_W - 1) / (2 * ES_W);
     const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
     k_elast_rows_staged<<<nbr, ES_W * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
@@ -1289,7 +1335,7 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
     LAUNCH_CHECK(ctx);
     return;
   }
-  if (mode == 0 || mode == 3) {
+  if (mode == 0 || mode == 4) {
     const i64 rows_per_block = 8 * (s->max_row <= 16 ? 2 : 1);
     const i64 need = (s->nnodes + rows_per_block - 1) / rows_per_block;
     const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
