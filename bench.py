@@ -848,7 +848,7 @@ def run_reference(args, cfg):
 
 
 PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5", "p2_cube40",
-                 "spmv_c2p", "spmv_c2")
+                 "spmv_c2p", "spmv_c2", "p2_c3")
 
 
 def profile_case(name):
@@ -869,7 +869,9 @@ def profile_case(name):
       spmv_c2p         the mixed PCG's FP32 block SpMV on the C2' system
                        (1,568,403 dofs, operator larger than L2), 3 launches
                        each after an L2 flush, shape tuning off
-      spmv_c2          the same on the C2 system (421,443 dofs)"""
+      spmv_c2          the same on the C2 system (421,443 dofs)
+      p2_c3            P2 stiffness of the C3 cube (64^3 x 6 tets, random
+                       kappa), assembled 3 times (for one-pass metrics only)"""
     import torch
     if name in ("spmv_c2p", "spmv_c2"):
         os.environ["FCU_TUNE"] = "0"   # no shape-tuning launches before the captured ones
@@ -907,8 +909,8 @@ def profile_case(name):
             M.pcg(b, tol=1e-30, max_iter=12, raise_on_error=False)
         ctx.synchronize()
         M.close(); V.close()
-    elif name == "p2_cube40":
-        mesh = fcu.unit_cube(40, 40, 40)
+    elif name in ("p2_cube40", "p2_c3"):
+        mesh = fcu.unit_cube(40, 40, 40) if name == "p2_cube40" else fcu.unit_cube(64, 64, 64)
         kap = np.exp(np.random.default_rng(3).standard_normal(mesh.nc))
         V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P2)
         M = fcu.Matrix(ctx, V)
