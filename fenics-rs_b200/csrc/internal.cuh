@@ -193,16 +193,6 @@ struct fcu_matrix_s {
   bool wrapped_general = false;  // wrapped CSC (export needs the stored layout)
   DBuf<double> val64;   // nnzb*bs*bs
   DBuf<float> val32;
-  // Symmetric FP32 operator of the mixed PCG (3x3 blocks of an assembled
-  // space): per block row its diagonal block (the FP64 row sum, rounded) and
-  // upper blocks as 40-byte records {9 FP32 values, column} at
-  // sym_rec[sym_ptr[i] .. sym_ptr[i+1]); its lower blocks as (row j, record
-  // of block (j, i)) pairs at low_ent[low_ptr[i] .. low_ptr[i+1]).
-  DBuf<int> sym_ptr, low_ptr;
-  DBuf<float> sym_rec;
-  DBuf<int2> low_ent;
-  int sym_max_up = 0, sym_max_low = 0;
-  i64 nsym = 0, nlow = 0;
   DBuf<unsigned char> dirichlet;  // n: 1 if eliminated (empty when no BC applied)
   i64 n_dirichlet = 0;
   DBuf<double> diag_count;        // n: diagonal value for eliminated dofs

@@ -731,250 +731,6 @@ __global__ void __launch_bounds__(SPMV_THREADS)
   store_pap_partial(em.dot, partials);
 }
 
-// ---------------------------------------------------------------------------
-// Symmetric FP32 block SpMV of the mixed PCG (3x3 blocks of an assembled,
-// exactly symmetric vector space). The operator is stored once per block
-// pair: block row i keeps its diagonal block (the FP64 row sum rounded to
-// FP32, as the difference form below uses) and its upper blocks (j > i) as
-// 40-byte records {9 values, column}; a lower block (i, j), j < i, is read as
-// the transpose of record (j, i), found through row i's list of (j, record)
-// pairs. Per block pair the kernel streams 40 bytes of record plus 8 bytes of
-// list instead of 2 x 40 bytes, and the transposed reads hit L2, because the
-// rows j < i that own them were streamed a moment before (a window of about
-// one mesh layer of block rows). The difference form
-//   y_i = S_i x_i + sum_{j != i} A_ij (x_j - x_i)
-// is the one of the full-storage FP32 operator. Tiles of SYM_TR block rows:
-// warp 0 streams each tile's record pointers, records, list pointers and
-// list entries into a shared-memory ring with bulk copies; 16 consumer warps
-// compute the tile's rows, 8 lanes per row, as k_spmv_tiled does. Each CTA
-// stores one p.Ap partial.
-// ---------------------------------------------------------------------------
-constexpr int SYM_TR = 64;
-constexpr int SYM_LPR = 32 * SPMV_CONSUMER_WARPS / SYM_TR;
-
-struct SymTileHeader {
-  int b0;       // first record of the tile
-  int rows;     // rows in the tile
-  int rec_off;  // byte offset of record b0 in the staged record region
-  int l0;       // first list entry of the tile
-  int low_off;  // byte offset of entry l0 in the staged list region
-};
-
-__host__ __device__ inline size_t sym_stage_bytes(int cap_rec, int cap_low) {
-  return align128(sizeof(SymTileHeader)) + align128((SYM_TR + 1) * 4 + 16) + align128((size_t)cap_rec * 40 + 32) +
-         align128((SYM_TR + 1) * 4 + 16) + align128((size_t)cap_low * 8 + 32);
-}
-
-__global__ void __launch_bounds__(SPMV_THREADS)
-    k_spmv_sym32(const int* __restrict__ sptr, const float* __restrict__ rec, const int* __restrict__ lptr,
-                 const int2* __restrict__ lent, i64 nrows, int cap_rec, int cap_low, int nstage,
-                 const float* __restrict__ p, float* __restrict__ ap, CgState* st, double* partials) {
-  extern __shared__ __align__(128) unsigned char tile_smem[];
-  __shared__ unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
-  const size_t stage_bytes = sym_stage_bytes(cap_rec, cap_low);
-  const i64 ntiles = (nrows + SYM_TR - 1) / SYM_TR;
-  const i64 G = gridDim.x;
-  const int mytiles = blockIdx.x < ntiles ? (int)((ntiles - blockIdx.x + G - 1) / G) : 0;
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
-  if (tid == 0) {
-    for (int s = 0; s < nstage; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], SPMV_CONSUMER_WARPS);
-    }
-    fence_mbar_init();
-  }
-  __syncthreads();
-  auto regions = [&](int s, unsigned char*& h, unsigned char*& rps, unsigned char*& rs, unsigned char*& lps,
-                     unsigned char*& ls) {
-    h = tile_smem + s * stage_bytes;
-    rps = h + align128(sizeof(SymTileHeader));
-    rs = rps + align128((SYM_TR + 1) * 4 + 16);
-    lps = rs + align128((size_t)cap_rec * 40 + 32);
-    ls = lps + align128((SYM_TR + 1) * 4 + 16);
-  };
-
-  // producer (warp 0): lane j holds the record and list bounds of tile k0 + j
-  int pb0 = 0, pb1 = 0, pl0 = 0, pl1 = 0;
-  auto load_desc = [&](int k0) {
-    const i64 t = blockIdx.x + (i64)(k0 + lane) * G;
-    if (t < ntiles) {
-      const i64 r0 = t * SYM_TR, r1 = min(r0 + SYM_TR, nrows);
-      pb0 = sptr[r0];
-      pb1 = sptr[r1];
-      pl0 = lptr[r0];
-      pl1 = lptr[r1];
-    }
-  };
-  auto issue = [&](int k) {
-    const int b0 = __shfl_sync(FULL, pb0, k & 31), b1 = __shfl_sync(FULL, pb1, k & 31);
-    const int l0 = __shfl_sync(FULL, pl0, k & 31), l1 = __shfl_sync(FULL, pl1, k & 31);
-    if (lane == 0) {
-      const int s = k % nstage;
-      unsigned char *hb, *rps, *rs, *lps, *ls;
-      regions(s, hb, rps, rs, lps, ls);
-      SymTileHeader* h = reinterpret_cast<SymTileHeader*>(hb);
-      const i64 r0 = (blockIdx.x + (i64)k * G) * SYM_TR;
-      const int rows = (int)min((i64)SYM_TR, nrows - r0);
-      const unsigned p_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);  // r0 is a multiple of 64
-      const uintptr_t r_lo = reinterpret_cast<uintptr_t>(rec + 10 * (i64)b0) & ~(uintptr_t)15;
-      const uintptr_t r_hi = (reinterpret_cast<uintptr_t>(rec + 10 * (i64)b1) + 15) & ~(uintptr_t)15;
-      const uintptr_t e_lo = reinterpret_cast<uintptr_t>(lent + l0) & ~(uintptr_t)15;
-      const uintptr_t e_hi = (reinterpret_cast<uintptr_t>(lent + l1) + 15) & ~(uintptr_t)15;
-      h->b0 = b0;
-      h->rows = rows;
-      h->rec_off = (int)(reinterpret_cast<uintptr_t>(rec + 10 * (i64)b0) - r_lo);
-      h->l0 = l0;
-      h->low_off = (int)(reinterpret_cast<uintptr_t>(lent + l0) - e_lo);
-      const unsigned rb = (unsigned)(r_hi - r_lo), eb = (unsigned)(e_hi - e_lo);
-      fence_proxy_async();
-      mbar_arrive_expect_tx(&full[s], 2 * p_bytes + rb + eb);
-      bulk_load(rps, sptr + r0, p_bytes, &full[s]);
-      bulk_load(lps, lptr + r0, p_bytes, &full[s]);
-      if (rb) bulk_load(rs, reinterpret_cast<const void*>(r_lo), rb, &full[s]);
-      if (eb) bulk_load(ls, reinterpret_cast<const void*>(e_lo), eb, &full[s]);
-    }
-  };
-
-  const int prologue = min(nstage, mytiles);
-  if (warp == 0) {
-    load_desc(0);
-    for (int k = 0; k < prologue; ++k) issue(k);
-  }
-  grid_dep_sync();
-  if (st->done || st->pause) {
-    if (warp == 0 && lane == 0)
-      for (int s = 0; s < prologue; ++s) mbar_wait(&full[s], 0);
-    return;
-  }
-  if (warp == 0) {
-    bool ok = true;
-    for (int k = prologue; k < mytiles; ++k) {
-      if ((k & 31) == 0) load_desc(k);
-      if (lane == 0) ok = mbar_wait(&empty[k % nstage], (unsigned)(((k / nstage) - 1) & 1));
-      if (!__shfl_sync(FULL, ok ? 1 : 0, 0)) {
-        if (lane == 0) {
-          atomicExch(&st->fault, 1);
-          for (int q = max(0, k - nstage); q < k; ++q) mbar_wait(&full[q % nstage], (unsigned)((q / nstage) & 1));
-        }
-        break;
-      }
-      issue(k);
-    }
-    store_pap_partial(0.0, partials);
-    return;
-  }
-
-  double dot = 0.0;
-  const int sub = lane % SYM_LPR;
-  const int row_in_tile = (warp - 1) * (32 / SYM_LPR) + lane / SYM_LPR;
-  for (int k = 0; k < mytiles; ++k) {
-    const int s = k % nstage;
-    if (!mbar_wait(&full[s], (unsigned)((k / nstage) & 1))) {
-      if (lane == 0) atomicExch(&st->fault, 1);
-      break;
-    }
-    unsigned char *hb, *rps, *rs, *lps, *ls;
-    regions(s, hb, rps, rs, lps, ls);
-    const SymTileHeader* h = reinterpret_cast<const SymTileHeader*>(hb);
-    const int* srp = reinterpret_cast<const int*>(rps);
-    const int* slp = reinterpret_cast<const int*>(lps);
-    const float* srec = reinterpret_cast<const float*>(rs + h->rec_off);
-    const int2* slow = reinterpret_cast<const int2*>(ls + h->low_off);
-    const int b0 = h->b0, l0 = h->l0;
-    const i64 row = (blockIdx.x + (i64)k * G) * SYM_TR + row_in_tile;
-    const bool valid = row_in_tile < h->rows;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, x0 = 0.f, x1 = 0.f, x2 = 0.f;
-    if (valid) {
-      x0 = p[3 * row];
-      x1 = p[3 * row + 1];
-      x2 = p[3 * row + 2];
-      const int kb1 = srp[row_in_tile + 1] - b0;
-#pragma unroll 2
-      for (int kb = srp[row_in_tile] - b0 + sub; kb < kb1; kb += SYM_LPR) {
-        const float* v = srec + 10 * kb;
-        const int c = __float_as_int(v[9]);
-        float y0, y1, y2;
-        if (c == (int)row) {
-          y0 = x0; y1 = x1; y2 = x2;
-        } else {
-          const i64 c3 = 3 * (i64)c;
-          y0 = p[c3] - x0; y1 = p[c3 + 1] - x1; y2 = p[c3 + 2] - x2;
-        }
-        a0 += v[0] * y0 + v[1] * y1 + v[2] * y2;
-        a1 += v[3] * y0 + v[4] * y1 + v[5] * y2;
-        a2 += v[6] * y0 + v[7] * y1 + v[8] * y2;
-      }
-      const int lk1 = slp[row_in_tile + 1] - l0;
-      for (int lk = slp[row_in_tile] - l0 + sub; lk < lk1; lk += SYM_LPR) {
-        const int2 e = slow[lk];
-        const float2* u = reinterpret_cast<const float2*>(rec + 10 * (i64)e.y);
-        const float2 u01 = __ldg(u), u23 = __ldg(u + 1), u45 = __ldg(u + 2), u67 = __ldg(u + 3), u89 = __ldg(u + 4);
-        const i64 j3 = 3 * (i64)e.x;
-        const float y0 = p[j3] - x0, y1 = p[j3 + 1] - x1, y2 = p[j3 + 2] - x2;
-        // block (i, j) is the transpose of the stored block (j, i)
-        a0 += u01.x * y0 + u23.y * y1 + u67.x * y2;
-        a1 += u01.y * y0 + u45.x * y1 + u67.y * y2;
-        a2 += u23.x * y0 + u45.y * y1 + u89.x * y2;
-      }
-    }
-    __syncwarp();
-    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
-#pragma unroll
-    for (int o = SYM_LPR / 2; o > 0; o >>= 1) {
-      a0 += __shfl_xor_sync(FULL, a0, o);
-      a1 += __shfl_xor_sync(FULL, a1, o);
-      a2 += __shfl_xor_sync(FULL, a2, o);
-    }
-    if (valid && sub < 3) {
-      const float yv = sub == 0 ? a0 : (sub == 1 ? a1 : a2);
-      const float xv = sub == 0 ? x0 : (sub == 1 ? x1 : x2);
-      ap[3 * row + sub] = yv;
-      dot += (double)xv * (double)yv;
-    }
-  }
-  store_pap_partial(dot, partials);
-}
-
-// Records of the symmetric operator from the FP32 values (whose diagonal
-// blocks hold the FP64 row sums, as build_rowsum32 leaves them): one thread
-// per record word.
-__global__ void k_sym32_fill(const int* __restrict__ row_ptr, const int* __restrict__ diag_pos,
-                             const int* __restrict__ col_idx, const int* __restrict__ sptr, i64 nn,
-                             const float* __restrict__ v32, float* __restrict__ rec) {
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < nn; i += (i64)gridDim.x * blockDim.x) {
-    const int d = diag_pos[i], e = row_ptr[i + 1];
-    float* o = rec + 10 * (i64)sptr[i];
-    for (int q = d; q < e; ++q, o += 10) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) o[k] = v32[9 * (i64)q + k];
-      o[9] = __int_as_float(col_idx[q]);
-    }
-  }
-}
-
-__global__ void k_sym32_counts(const int* __restrict__ row_ptr, const int* __restrict__ diag_pos, i64 nn,
-                               int* __restrict__ cnt_up, int* __restrict__ cnt_low) {
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < nn; i += (i64)gridDim.x * blockDim.x) {
-    cnt_up[i] = row_ptr[i + 1] - diag_pos[i];
-    cnt_low[i] = diag_pos[i] - row_ptr[i];
-  }
-}
-
-__global__ void k_sym32_low(const int* __restrict__ row_ptr, const int* __restrict__ diag_pos,
-                            const int* __restrict__ col_idx, const int* __restrict__ tpos,
-                            const int* __restrict__ sptr, const int* __restrict__ lptr, i64 nn,
-                            int2* __restrict__ lent, int* __restrict__ bad) {
-  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < nn; i += (i64)gridDim.x * blockDim.x) {
-    const int r = row_ptr[i], d = diag_pos[i];
-    for (int q = r; q < d; ++q) {
-      const int j = col_idx[q], tq = tpos[q];
-      if (tq < 0) { atomicExch(bad, 1); lent[lptr[i] + q - r] = make_int2(j, sptr[j]); continue; }
-      lent[lptr[i] + q - r] = make_int2(j, sptr[j] + (tq - diag_pos[j]));
-    }
-  }
-}
-
 // --- update -----------------------------------------------------------------
 __device__ __forceinline__ void decide_after_update(CgState* st, double rz_new, double rr) {
   st->iter += 1;
@@ -1470,10 +1226,6 @@ fcu_matrix_s::~fcu_matrix_s() {
   destroy_batch_ws(bws);
 }
 
-// defined below (outside the anonymous namespace)
-bool use_sym32(fcu_matrix m);
-double spmv_algorithmic_bytes(fcu_matrix m, bool mixed);
-
 namespace {
 
 // Blocks per SM for the solver kernels (grid-stride loops); FCU_SOLVER_BPSM
@@ -1752,33 +1504,6 @@ int launch_spmv_tiled_tr(fcu_matrix m, Workspace* w, const T* val, const T* p, T
   return grid;
 }
 
-// The symmetric FP32 block SpMV (k_spmv_sym32): ring depth as tuned for the
-// FP32 tiled kernel, TILED_CTAS_PER_SM CTAs per SM. Returns the grid.
-int launch_spmv_sym32(fcu_matrix m, Workspace* w, const float* p, float* ap) {
-  fcu_ctx ctx = m->ctx;
-  const int cap_rec = SYM_TR * std::max(1, m->sym_max_up);
-  const int cap_low = SYM_TR * std::max(1, m->sym_max_low);
-  const size_t stage = sym_stage_bytes(cap_rec, cap_low);
-  const int nstage = fitted_stages(ctx, w->stages[1], stage);
-  const size_t smem = nstage * stage;
-  static int configured_dev = -1;
-  static size_t configured_smem = 0;
-  if (configured_dev != ctx->device || configured_smem < smem) {
-    CUDA_CHECK(cudaFuncSetAttribute(k_spmv_sym32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured_dev = ctx->device;
-    configured_smem = smem;
-  }
-  int per_sm = 0;
-  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_sym32, SPMV_THREADS, smem));
-  if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "rows too long for the symmetric SpMV");
-  const i64 ntiles = (m->nnodes + SYM_TR - 1) / SYM_TR;
-  const int grid =
-      (int)std::max<i64>(1, std::min<i64>(ntiles, (i64)std::min(per_sm, TILED_CTAS_PER_SM) * ctx->num_sms));
-  launch_pdl_cfg(ctx, k_spmv_sym32, grid, SPMV_THREADS, smem, m->sym_ptr.p, m->sym_rec.p, m->low_ptr.p,
-                 m->low_ent.p, m->nnodes, cap_rec, cap_low, nstage, p, ap, w->st.p, w->partials.p);
-  return grid;
-}
-
 // Returns the grid (the number of p.Ap partials the update kernel adds).
 template <int DIFF, class T>
 int launch_spmv_tiled(fcu_matrix m, Workspace* w, const T* val, const T* p, T* ap) {
@@ -1866,9 +1591,7 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
     } else {
       launch_pdl(ctx, k_direction<float>, w->vgrid, n, w->pa32.p, w->z32.p, w->st.p);
       int npap = g;
-      if (use_sym32(m)) {
-        npap = launch_spmv_sym32(m, w, w->pa32.p, w->ap32.p);
-      } else if (m->bs == 3 && use_tiled_spmv()) {
+      if (m->bs == 3 && use_tiled_spmv()) {
         npap = launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
       } else if (w->tiled1[1]) {
         npap = launch_spmv_tiled_scalar<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
@@ -1964,76 +1687,6 @@ void ensure_inv_diag(fcu_matrix m, Workspace* w) {
   LAUNCH_CHECK(ctx);
 }
 
-// FCU_SYM32=0 keeps the full-storage FP32 operator for the mixed PCG of
-// assembled 3x3-block matrices (comparison).
-bool sym32_enabled() {
-  static int v = [] {
-    const char* e = getenv("FCU_SYM32");
-    return e ? atoi(e) : 1;
-  }();
-  return v != 0;
-}
-
-bool use_sym32(fcu_matrix m) { return m->bs == 3 && m->space && sym32_enabled(); }
-
-// Structure of the symmetric operator (once per matrix): record and list
-// pointers from the pattern, and each lower block's record through the
-// transpose positions.
-void ensure_sym32(fcu_matrix m) {
-  if (m->sym_ptr.p) return;
-  fcu_ctx ctx = m->ctx;
-  fcu_space s = m->space;
-  build_transpose_positions(s);
-  const i64 nn = m->nnodes;
-  std::vector<int> rp(nn + 1), dp(nn), sp(nn + 1), lp(nn + 1);
-  download(ctx, rp.data(), m->row_ptr, nn + 1);
-  download(ctx, dp.data(), m->diag_pos, nn);
-  i64 ns = 0, nl = 0;
-  int mu = 0, ml = 0;
-  for (i64 i = 0; i < nn; ++i) {
-    sp[i] = (int)ns;
-    lp[i] = (int)nl;
-    const int u = rp[i + 1] - dp[i], l = dp[i] - rp[i];
-    ns += u;
-    nl += l;
-    mu = std::max(mu, u);
-    ml = std::max(ml, l);
-  }
-  sp[nn] = (int)ns;
-  lp[nn] = (int)nl;
-  upload(ctx, m->sym_ptr, sp.data(), nn + 1);
-  upload(ctx, m->low_ptr, lp.data(), nn + 1);
-  m->nsym = ns;
-  m->nlow = nl;
-  m->sym_max_up = mu;
-  m->sym_max_low = ml;
-  m->sym_rec.alloc((size_t)ns * 10);
-  m->low_ent.alloc((size_t)std::max<i64>(nl, 1));
-  DBuf<int> bad;
-  bad.alloc(1);
-  CUDA_CHECK(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
-  k_sym32_low<<<grid_for(nn, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
-      m->row_ptr, m->diag_pos, m->col_idx, s->tpos.p, m->sym_ptr.p, m->low_ptr.p, nn, m->low_ent.p, bad.p);
-  LAUNCH_CHECK(ctx);
-  int hb = 0;
-  download(ctx, &hb, bad.p, 1);
-  if (hb) fail(FCU_ERR_UNSUPPORTED, "the symmetric FP32 operator needs a symmetric pattern");
-}
-
-void build_rowsum32(fcu_matrix m);
-
-// The FP32 operator of the mixed PCG: FP64 row sums on the diagonal, and the
-// symmetric records when they are used.
-void prepare_fp32_operator(fcu_matrix m) {
-  build_rowsum32(m);
-  if (!use_sym32(m)) return;
-  ensure_sym32(m);
-  fcu_ctx ctx = m->ctx;
-  k_sym32_fill<<<grid_for(m->nnodes, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
-      m->row_ptr, m->diag_pos, m->col_idx, m->sym_ptr.p, m->nnodes, m->val32.p, m->sym_rec.p);
-  LAUNCH_CHECK(ctx);
-}
-
 void build_rowsum32(fcu_matrix m) {
   fcu_ctx ctx = m->ctx;
   const i64 t = m->nnodes * m->bs * m->bs;
@@ -2109,7 +1762,7 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
   } else {
     ensure_inv_diag(m, w);
   }
-  if (mixed) prepare_fp32_operator(m);
+  if (mixed) build_rowsum32(m);
   tune_spmv(m, w, mixed);  // first solve in this precision only
 
   CgState init{};
@@ -2259,8 +1912,7 @@ void enqueue_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   fcu_ctx ctx = m->ctx;
   const int g = w->grid;
   if (mixed) {
-    if (use_sym32(m)) launch_spmv_sym32(m, w, w->pa32.p, w->ap32.p);
-    else if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
+    if (m->bs == 3 && use_tiled_spmv()) launch_spmv_tiled<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
     else if (w->tiled1[1]) launch_spmv_tiled_scalar<1, float>(m, w, m->val32.p, w->pa32.p, w->ap32.p);
     else if (w->stream[1])
       launch_pdl_cfg(ctx, k_spmv_stream<float>, stream_grid_for(ctx, m->nrowblk, k_spmv_stream<float>), STREAM_THREADS, 0, m->row_ptr,
@@ -2419,27 +2071,18 @@ void tune_spmv(fcu_matrix m, Workspace* w, bool mixed) {
   }
 }
 
-// Bytes one SpMV launch must move: the stored operator (values and column
-// indices, or for the symmetric FP32 operator its records and lower-block
-// lists), the row pointers, one read of p and one write of Ap.
-double spmv_algorithmic_bytes(fcu_matrix m, bool mixed) {
-  const double wv = mixed ? 4.0 : 8.0;
-  if (mixed && use_sym32(m) && m->sym_ptr.p)
-    return 40.0 * (double)m->nsym + 8.0 * (double)m->nlow + 8.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
-  const double bs2 = (double)m->bs * m->bs;
-  return (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
-}
-
 // Average time of the PCG SpMV kernel over `reps` launches (diagnostics),
 // with the shape the solver uses.
 void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes) {
   const bool mixed = precision == FCU_MIXED;
   Workspace* w = ensure_ws(m, mixed);
-  if (mixed) prepare_fp32_operator(m);
+  if (mixed) build_rowsum32(m);
   tune_spmv(m, w, mixed);
   spmv_timing_state(m, w, mixed);
   *ms = time_spmv_launches(m, w, mixed, reps);
-  *bytes = spmv_algorithmic_bytes(m, mixed);
+  const double bs2 = (double)m->bs * m->bs;
+  const double wv = mixed ? 4.0 : 8.0;
+  *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
 }
 
 // Reads `n` 16-byte words and keeps one word per thread in `sink` (so the
@@ -2462,7 +2105,7 @@ __global__ void k_flush_read(const uint4* __restrict__ buf, i64 n, uint4* __rest
 void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_bytes, double* ms, double* bytes) {
   const bool mixed = precision == FCU_MIXED;
   Workspace* w = ensure_ws(m, mixed);
-  if (mixed) prepare_fp32_operator(m);
+  if (mixed) build_rowsum32(m);
   tune_spmv(m, w, mixed);
   spmv_timing_state(m, w, mixed);
   fcu_ctx ctx = m->ctx;
@@ -2493,7 +2136,9 @@ void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_byt
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *ms = reps > 0 ? total / reps : 0.0;
-  *bytes = spmv_algorithmic_bytes(m, mixed);
+  const double bs2 = (double)m->bs * m->bs;
+  const double wv = mixed ? 4.0 : 8.0;
+  *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
 }
 
 // ---------------------------------------------------------------------------
