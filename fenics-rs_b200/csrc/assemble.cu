@@ -173,18 +173,6 @@ __device__ __forceinline__ void p2_record(const double* __restrict__ p2geo, int 
 // cell), so a lane keeps its six reference-tensor entries R[m][a][b] in
 // registers and reloads them from shared memory only when a changes (at most
 // four times on a vertex row, six on an edge row) instead of at every step.
-// The per-contribution inputs of a row (metric records, local indices and
-// slot maps, up to P2_MAXC contributions at a time) are staged in shared
-// memory with contiguous loads before the steps, so a step reads only shared
-// memory: one broadcast record read per group, one slot byte, and the
-// accumulator update.
-constexpr int P2_MAXC = 32;
-
-__host__ __device__ constexpr size_t p2_smem_bytes(int stride) {
-  return (600 + (size_t)P2W * 3 * stride + (size_t)P2W * 3 * P2_MAXC * 6) * sizeof(double) +
-         (size_t)P2W * 3 * P2_MAXC * (10 + 1);
-}
-
 __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib_a,
     const unsigned char* __restrict__ cmap, const double* __restrict__ p2geo, i64 nrows, int stride,
@@ -195,14 +183,8 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
   for (int q = threadIdx.x; q < 600; q += blockDim.x) R[q] = (&c_p2_R[0][0][0])[q];
   __syncthreads();
   const int g = lane / 10, b = lane - 10 * g;  // g == 3 on lanes 30 and 31
-  const int gg0 = g < 3 ? g : 0;
   double* acc = p2sh + 600 + (i64)wib * 3 * stride;
-  double* my = acc + gg0 * stride;
-  double* Sst = p2sh + 600 + (i64)P2W * 3 * stride + ((i64)wib * 3 + gg0) * P2_MAXC * 6;
-  unsigned char* bytes = reinterpret_cast<unsigned char*>(p2sh + 600 + (i64)P2W * 3 * stride +
-                                                           (i64)P2W * 3 * P2_MAXC * 6);
-  unsigned char* Ast = bytes + ((i64)wib * 3 + gg0) * P2_MAXC;
-  unsigned char* CMst = bytes + (i64)P2W * 3 * P2_MAXC + ((i64)wib * 3 + gg0) * P2_MAXC * 10;
+  double* my = acc + (g < 3 ? g : 0) * stride;
   const i64 nwarps = (i64)gridDim.x * P2W;
   for (i64 r0 = ((i64)blockIdx.x * P2W + wib) * 3; r0 < nrows; r0 += nwarps * 3) {
     const i64 row = r0 + g;
@@ -213,49 +195,37 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
       nct = contrib_ptr[row + 1] - cs;
     }
     for (int q = b; q < L; q += 10) my[q] = 0.0;
-    const int nch = __reduce_max_sync(FULL, (nct + P2_MAXC - 1) / P2_MAXC);
+    const int steps = __reduce_max_sync(FULL, nct);
+    __syncwarp();
     int a_cur = -1;
     double r0v = 0.0, r1v = 0.0, r2v = 0.0, r3v = 0.0, r4v = 0.0, r5v = 0.0;
-    for (int ch = 0; ch < nch; ++ch) {
-      const int c0 = ch * P2_MAXC;
-      const int n = nct - c0 < P2_MAXC ? (nct - c0 > 0 ? nct - c0 : 0) : P2_MAXC;
-      const i64 cb = (i64)cs + c0;
-      __syncwarp();
-      for (int w = b; w < 3 * n; w += 10) {
-        const int t = w / 3, k = w - 3 * t;
-        const int cc = contrib_a[cb + t];
-        reinterpret_cast<double2*>(Sst)[3 * t + k] =
-            __ldg(reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO) + k);
-      }
-      for (int t = b; t < n; t += 10) Ast[t] = (unsigned char)(contrib_a[cb + t] & 15);
-      for (int q = b; q < 10 * n; q += 10) CMst[q] = cmap[cb * 10 + q];
-      const int steps = __reduce_max_sync(FULL, n);
-      __syncwarp();
-      for (int t = 0; t < steps; ++t) {
-        if (t < n) {
-          const int a = Ast[t];
-          if (a != a_cur) {
-            const double* Rab = R + a * 10 + b;
-            r0v = Rab[0];
-            r1v = Rab[100];
-            r2v = Rab[200];
-            r3v = Rab[300];
-            r4v = Rab[400];
-            r5v = Rab[500];
-            a_cur = a;
-          }
-          const double2* S = reinterpret_cast<const double2*>(Sst) + 3 * t;
-          const double2 s01 = S[0], s23 = S[1], s45 = S[2];
-          double v = s01.x * r0v;
-          v += s01.y * r1v;
-          v += s23.x * r2v;
-          v += s23.y * r3v;
-          v += s45.x * r4v;
-          v += s45.y * r5v;
-          my[CMst[10 * t + b]] += v;
+    for (int t = 0; t < steps; ++t) {
+      if (t < nct) {
+        const i64 ci = (i64)cs + t;
+        const int cc = contrib_a[ci];
+        double2 s01, s23, s45;
+        p2_record(p2geo, cc, s01, s23, s45);
+        const int sl = cmap[ci * 10 + b];
+        const int a = cc & 15;
+        if (a != a_cur) {
+          const double* Rab = R + a * 10 + b;
+          r0v = Rab[0];
+          r1v = Rab[100];
+          r2v = Rab[200];
+          r3v = Rab[300];
+          r4v = Rab[400];
+          r5v = Rab[500];
+          a_cur = a;
         }
-        __syncwarp();
+        double v = s01.x * r0v;
+        v += s01.y * r1v;
+        v += s23.x * r2v;
+        v += s23.y * r3v;
+        v += s45.x * r4v;
+        v += s45.y * r5v;
+        my[sl] += v;
       }
+      __syncwarp();
     }
     const i64 rend = r0 + 3 < nrows ? r0 + 3 : nrows;
     const int base = row_ptr[r0];
@@ -263,8 +233,8 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     const int off1 = row_ptr[r0 + 1 < rend ? r0 + 1 : rend] - base;
     const int off2 = row_ptr[r0 + 2 < rend ? r0 + 2 : rend] - base;
     for (int q = lane; q < tot; q += 32) {
-      const int gq = q >= off2 ? 2 : (q >= off1 ? 1 : 0);
-      const double v = acc[gq * stride + q - (gq == 2 ? off2 : gq == 1 ? off1 : 0)];
+      const int gg = q >= off2 ? 2 : (q >= off1 ? 1 : 0);
+      const double v = acc[gg * stride + q - (gg == 2 ? off2 : gg == 1 ? off1 : 0)];
       v64[base + q] = v;
       v32[base + q] = (float)v;
     }
@@ -796,121 +766,6 @@ __global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ r
   }
 }
 
-// Vector-P1 elasticity, row form with the records staged (the kernel
-// fcu_assemble_elasticity runs when every row has at most 16 blocks and 24
-// cells, as on the Kuhn box meshes). Each half-warp owns one block row: it
-// copies the 128-byte records of the row's cells into shared memory with
-// contiguous 16-byte loads (eight lanes per record), then every lane walks the
-// (cell, column) list of its block from shared memory, as k_elast_rows does
-// from global memory. Gathering the records per lane from global memory
-// costs one L1 sector request per gradient; staging them costs four per cell.
-constexpr int ES_W = 4;      // warps per block, two rows per warp
-constexpr int ES_MAXC = 24;  // staged cells per row
-constexpr int ES_RS = 18;    // record stride in shared memory, doubles (144 B: 16-byte aligned, spreads banks)
-
-__global__ void __launch_bounds__(ES_W * 32) k_elast_rows_staged(
-    const int* __restrict__ row_ptr, const int* __restrict__ contrib_ptr, const int* __restrict__ contrib,
-    const unsigned short* __restrict__ slot_cnt, const unsigned short* __restrict__ slot_ent,
-    const int* __restrict__ diag_pos, const double* __restrict__ rec, i64 nrows, double lam, double mu,
-    double* __restrict__ v64, float* __restrict__ v32) {
-  __shared__ __align__(16) double recs_all[ES_W][2][ES_MAXC * ES_RS];
-  __shared__ unsigned short ents_all[ES_W][2][4 * ES_MAXC];
-  __shared__ unsigned char aof_all[ES_W][2][ES_MAXC];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int seg = lane >> 4, sub = lane & 15;
-  double* R = recs_all[wib][seg];
-  unsigned short* E = ents_all[wib][seg];
-  unsigned char* A = aof_all[wib][seg];
-  const i64 nwarps = (i64)gridDim.x * ES_W;
-  for (i64 r0 = ((i64)blockIdx.x * ES_W + wib) * 2; r0 < nrows; r0 += nwarps * 2) {
-    const i64 row = r0 + seg;
-    int rs = 0, L = 0, cs = 0, nct = 0, dl = -1;
-    if (row < nrows) {
-      rs = row_ptr[row];
-      L = row_ptr[row + 1] - rs;
-      cs = contrib_ptr[row];
-      nct = contrib_ptr[row + 1] - cs;
-      dl = diag_pos[row] - rs;
-    }
-    // stage the cells' records, their local indices and the row's entry lists
-    for (int w = sub; w < 8 * nct; w += 16) {
-      const int t = w >> 3, k = w & 7;
-      const int cc = contrib[cs + t];
-      const double2 v = __ldg(reinterpret_cast<const double2*>(rec + 16 * (i64)(cc >> 4)) + k);
-      *reinterpret_cast<double2*>(R + t * ES_RS + 2 * k) = v;
-    }
-    for (int t = sub; t < nct; t += 16) A[t] = (unsigned char)(contrib[cs + t] & 15);
-    for (int q = sub; q < 4 * nct; q += 16) E[q] = slot_ent[4 * (i64)cs + q];
-    // the block's entries: a segmented exclusive scan of the row's slot counts
-    const int cnt = sub < L ? (int)slot_cnt[rs + sub] : 0;
-    int x = cnt;
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-      const int y = __shfl_up_sync(FULL, x, o, 16);
-      if (sub >= o) x += y;
-    }
-    const int off = x - cnt;
-    __syncwarp();
-    double M[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) M[k] = 0.0;
-    const bool own = sub < L && sub != dl;
-    if (own) {
-      for (int e = off; e < off + cnt; ++e) {
-        const unsigned ent = E[e];
-        const int t = (int)(ent >> 4), b = (int)(ent & 15u);
-        const double* rt = R + t * ES_RS;
-        const double2 h01 = *reinterpret_cast<const double2*>(rt + 4 * A[t]);
-        const double2 h2s = *reinterpret_cast<const double2*>(rt + 4 * A[t] + 2);
-        const double2 g01 = *reinterpret_cast<const double2*>(rt + 4 * b);
-        const double2 g2s = *reinterpret_cast<const double2*>(rt + 4 * b + 2);
-        const double hx = h2s.y * h01.x, hy = h2s.y * h01.y, hz = h2s.y * h2s.x;
-        M[0] += hx * g01.x; M[1] += hx * g01.y; M[2] += hx * g2s.x;
-        M[3] += hy * g01.x; M[4] += hy * g01.y; M[5] += hy * g2s.x;
-        M[6] += hz * g01.x; M[7] += hz * g01.y; M[8] += hz * g2s.x;
-      }
-    }
-    __syncwarp();
-    // the records are no longer needed: their space holds the row's blocks
-    // (9 x 16 doubles) and the lanes' M for the row sum (9 x 16 doubles)
-    double* out = R;
-    double* ms = R + 9 * 16;
-    if (own) {
-      const double tr = mu * (M[0] + M[4] + M[8]);
-#pragma unroll
-      for (int a2 = 0; a2 < 3; ++a2)
-#pragma unroll
-        for (int b2 = 0; b2 < 3; ++b2)
-          out[9 * sub + 3 * a2 + b2] = lam * M[3 * a2 + b2] + mu * M[3 * b2 + a2] + (a2 == b2 ? tr : 0.0);
-    }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) ms[9 * sub + k] = M[k];
-    __syncwarp();
-    const i64 base = 9 * (i64)rs;
-    for (int idx = sub; idx < 9 * L; idx += 16) {
-      if (idx / 9 == dl) continue;
-      const double v = out[idx];
-      v64[base + idx] = v;
-      v32[base + idx] = (float)v;
-    }
-    double tsum = 0.0;
-    if (sub < 9)
-      for (int l = 0; l < 16; ++l) tsum += ms[9 * l + sub];
-    __syncwarp();
-    if (sub < 9) ms[sub] = tsum;
-    __syncwarp();
-    if (row < nrows && sub < 9 && dl >= 0) {
-      const int a2 = sub / 3, b2 = sub - 3 * (sub / 3);
-      const double d = -0.5 * (ms[3 * a2 + b2] + ms[3 * b2 + a2]);
-      const double tr = -(ms[0] + ms[4] + ms[8]);
-      const double v = (lam + mu) * d + (a2 == b2 ? mu * tr : 0.0);
-      v64[9 * ((i64)rs + dl) + sub] = v;
-      v32[9 * ((i64)rs + dl) + sub] = (float)v;
-    }
-    __syncwarp();
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Mass matrices (mass.rs:10-250). Entry (a, b) of cell c is s_c F[a][b]:
 // s_c = rho * measure (area |det|/2, volume |det|/6; the P2 products already
@@ -1241,8 +1096,7 @@ bool p2_row_gather() {
 }
 
 // FCU_ELAST_KERNEL selects the elasticity kernel: 0 = row form over the
-// gradient records (default), 4 = the same with the records staged in
-// shared memory per row, 1 = block-parallel form, 2 = row-gather with
+// gradient records (default), 1 = block-parallel form, 2 = row-gather with
 // per-contribution geometry (kept as comparisons).
 int elasticity_kernel() {
   static const int v = [] {
@@ -1272,7 +1126,7 @@ void assemble_stiffness_impl(fcu_matrix m, const double* coef_dev) {
     LAUNCH_CHECK(ctx);
     if (s->cmap.p && s->contrib_a.p && !p2_row_gather()) {
       const int stride = s->max_row | 1;  // odd, so the three rows' accumulators start in different banks
-      const size_t smem = p2_smem_bytes(stride);
+      const size_t smem = (600 + (size_t)P2W * 3 * stride) * sizeof(double);
       static bool attr_set[64] = {};
       if (smem > 48 * 1024 && !attr_set[ctx->device & 63]) {
         CUDA_CHECK(cudaFuncSetAttribute(k_assemble_p2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
@@ -1325,17 +1179,7 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
         s->cell_nodes.p, me->coords.p, me->valid.p, cellE_dev, me->nc, s->cell_rec.p);
     LAUNCH_CHECK(ctx);
   }
-  if (mode == 4 && s->max_row <= 16 && s->max_contrib <= ES_MAXC) {
-    const i64 need = (s->nnodes + 2 * ES_W - 1) / (2 * ES_W);
-    const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
-    k_elast_rows_staged<<<nbr, ES_W * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
-                                                            s->slot_cnt.p, s->slot_ent.p, s->diag_pos.p,
-                                                            s->cell_rec.p, s->nnodes, lam, mu, m->val64.p,
-                                                            m->val32.p);
-    LAUNCH_CHECK(ctx);
-    return;
-  }
-  if (mode == 0 || mode == 4) {
+  if (mode == 0) {
     const i64 rows_per_block = 8 * (s->max_row <= 16 ? 2 : 1);
     const i64 need = (s->nnodes + rows_per_block - 1) / rows_per_block;
     const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
