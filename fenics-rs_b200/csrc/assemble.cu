@@ -163,10 +163,11 @@ constexpr int P2W = 8;  // warps per block
 
 __device__ __forceinline__ void p2_record(const double* __restrict__ p2geo, int cc, double2& s01, double2& s23,
                                           double2& s45) {
-  const double2* rec = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
-  s01 = __ldg(rec);
-  s23 = __ldg(rec + 1);
-  s45 = __ldg(rec + 2);
+  // the 64-byte record as two 256-bit loads (its last two words are padding)
+  const double* r = p2geo + (i64)(cc >> 4) * P2_GEO;
+  double2 pad;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(s01.x), "=d"(s01.y), "=d"(s23.x), "=d"(s23.y) : "l"(r));
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(s45.x), "=d"(s45.y), "=d"(pad.x), "=d"(pad.y) : "l"(r + 4));
 }
 
 // Each row's contributions come ordered by (local index a of the row's dof,
@@ -199,10 +200,13 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     __syncwarp();
     int a_cur = -1;
     double r0v = 0.0, r1v = 0.0, r2v = 0.0, r3v = 0.0, r4v = 0.0, r5v = 0.0;
+    int cc_chunk = 0;  // lane b holds contribution t0 + b of its row's current chunk of ten
     for (int t = 0; t < steps; ++t) {
+      if (t % 10 == 0) cc_chunk = (t + b < nct) ? contrib_a[(i64)cs + t + b] : 0;
+      const int cc_t = __shfl_sync(FULL, cc_chunk, (g < 3 ? 10 * g : 0) + t % 10);
       if (t < nct) {
         const i64 ci = (i64)cs + t;
-        const int cc = contrib_a[ci];
+        const int cc = cc_t;
         double2 s01, s23, s45;
         p2_record(p2geo, cc, s01, s23, s45);
         const int sl = cmap[ci * 10 + b];
@@ -660,6 +664,12 @@ __global__ void __launch_bounds__(256) k_elast_blocks(i64 nup, const int* __rest
 // sum_j M_ij = 0 and M_ii = -sum_{j != i} M_ij (symmetrised), summed over the
 // row's lanes through shared memory; relative to the summed-per-cell
 // diagonal this moves it by a few ulps of the row's largest block.
+// One 32-byte gradient record {g.x, g.y, g.z, s} with a single 256-bit load
+// (read-only path): one L1 request per record instead of two 16-byte ones.
+__device__ __forceinline__ void ld_rec4(const double* p, double2& a, double2& b) {
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p));
+}
+
 __device__ __forceinline__ void elast_accumulate(double (&M)[9], double s, double2 a01, double2 a2s, double2 b01,
                                                  double2 b2s) {
   const double ga[3] = {a01.x, a01.y, a2s.x}, gb[3] = {b01.x, b01.y, b2s.x};
@@ -684,7 +694,6 @@ __global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ r
   const int sub = lane % LPR, seg = lane / LPR;
   double* out = out_all[wib];
   double* ms = ms_all[wib];
-  const double2* R2 = reinterpret_cast<const double2*>(rec);
   const i64 nwarps = (i64)gridDim.x * W;
   for (i64 r0 = ((i64)blockIdx.x * W + wib) * RPW; r0 < nrows; r0 += nwarps * RPW) {
     const i64 row = r0 + seg;
@@ -708,20 +717,19 @@ __global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ r
         const int e1 = sl_ptr[rs + q + 1];
         for (; e + 1 < e1; e += 2) {
           const unsigned u0 = sl_ent[e], u1 = sl_ent[e + 1];
-          const double2* pa0 = R2 + 8 * (i64)(u0 >> 4) + 2 * ((u0 >> 2) & 3u);
-          const double2* pb0 = R2 + 8 * (i64)(u0 >> 4) + 2 * (u0 & 3u);
-          const double2* pa1 = R2 + 8 * (i64)(u1 >> 4) + 2 * ((u1 >> 2) & 3u);
-          const double2* pb1 = R2 + 8 * (i64)(u1 >> 4) + 2 * (u1 & 3u);
-          const double2 a01 = __ldg(pa0), a2s = __ldg(pa0 + 1), b01 = __ldg(pb0), b2s = __ldg(pb0 + 1);
-          const double2 c01 = __ldg(pa1), c2s = __ldg(pa1 + 1), d01 = __ldg(pb1), d2s = __ldg(pb1 + 1);
+          double2 a01, a2s, b01, b2s, c01, c2s, d01, d2s;
+          ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * ((u0 >> 2) & 3u), a01, a2s);
+          ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * (u0 & 3u), b01, b2s);
+          ld_rec4(rec + 16 * (i64)(u1 >> 4) + 4 * ((u1 >> 2) & 3u), c01, c2s);
+          ld_rec4(rec + 16 * (i64)(u1 >> 4) + 4 * (u1 & 3u), d01, d2s);
           elast_accumulate(M, a2s.y, a01, a2s, b01, b2s);
           elast_accumulate(M, c2s.y, c01, c2s, d01, d2s);
         }
         if (e < e1) {
           const unsigned u0 = sl_ent[e];
-          const double2* pa0 = R2 + 8 * (i64)(u0 >> 4) + 2 * ((u0 >> 2) & 3u);
-          const double2* pb0 = R2 + 8 * (i64)(u0 >> 4) + 2 * (u0 & 3u);
-          const double2 a01 = __ldg(pa0), a2s = __ldg(pa0 + 1), b01 = __ldg(pb0), b2s = __ldg(pb0 + 1);
+          double2 a01, a2s, b01, b2s;
+          ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * ((u0 >> 2) & 3u), a01, a2s);
+          ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * (u0 & 3u), b01, b2s);
           elast_accumulate(M, a2s.y, a01, a2s, b01, b2s);
         }
         const double tr = mu * (M[0] + M[4] + M[8]);
