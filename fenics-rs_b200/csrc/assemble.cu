@@ -163,11 +163,10 @@ constexpr int P2W = 8;  // warps per block
 
 __device__ __forceinline__ void p2_record(const double* __restrict__ p2geo, int cc, double2& s01, double2& s23,
                                           double2& s45) {
-  // the 64-byte record as two 256-bit loads (its last two words are padding)
-  const double* r = p2geo + (i64)(cc >> 4) * P2_GEO;
-  double2 pad;
-  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(s01.x), "=d"(s01.y), "=d"(s23.x), "=d"(s23.y) : "l"(r));
-  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(s45.x), "=d"(s45.y), "=d"(pad.x), "=d"(pad.y) : "l"(r + 4));
+  const double2* rec = reinterpret_cast<const double2*>(p2geo + (i64)(cc >> 4) * P2_GEO);
+  s01 = __ldg(rec);
+  s23 = __ldg(rec + 1);
+  s45 = __ldg(rec + 2);
 }
 
 // Each row's contributions come ordered by (local index a of the row's dof,
@@ -200,13 +199,10 @@ __global__ void __launch_bounds__(P2W * 32) k_assemble_p2_rows(
     __syncwarp();
     int a_cur = -1;
     double r0v = 0.0, r1v = 0.0, r2v = 0.0, r3v = 0.0, r4v = 0.0, r5v = 0.0;
-    int cc_chunk = 0;  // lane b holds contribution t0 + b of its row's current chunk of ten
     for (int t = 0; t < steps; ++t) {
-      if (t % 10 == 0) cc_chunk = (t + b < nct) ? contrib_a[(i64)cs + t + b] : 0;
-      const int cc_t = __shfl_sync(FULL, cc_chunk, (g < 3 ? 10 * g : 0) + t % 10);
       if (t < nct) {
         const i64 ci = (i64)cs + t;
-        const int cc = cc_t;
+        const int cc = contrib_a[ci];
         double2 s01, s23, s45;
         p2_record(p2geo, cc, s01, s23, s45);
         const int sl = cmap[ci * 10 + b];
