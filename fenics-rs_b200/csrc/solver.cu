@@ -799,6 +799,9 @@ __global__ void __launch_bounds__(VBLOCK, 5) k_update(i64 n, double* __restrict_
       rr += ri * ri;
     }
   }
+  // the remaining elements (about six per thread at 1.5M rows): unrolled so
+  // that the loads of several elements are in flight together
+#pragma unroll 4
   for (i64 i = i0 + 2 * stride; i < n; i += stride) {
     x[i] += alpha * (double)p[i];
     const double ri = r[i] - alpha * (double)ap[i];
