@@ -370,9 +370,15 @@ def run_cuda(args, cfg):
     spmv64_ms, spmv64_bytes = M.time_spmv(fcu.FCU_FP64, reps=20, cold=True)
     spmv64_warm_ms, _ = M.time_spmv(fcu.FCU_FP64, reps=20)
     peak, peak_kind = _peaks()
-    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
     traffic = _profile_traffic("spmv_bsr3_fp32_elasticity_c2.txt")
     traffic64 = _profile_traffic("spmv_bsr3_fp64_elasticity_c2.txt")
+    # dominant kernel: the mixed solve's persistent loop (the whole iteration:
+    # FP32 SpMV, vector update, grid barriers), one launch of exactly 300
+    # iterations after an L2 read sweep, as the profiling case pcg_c2 runs it
+    pcg_iters = 300
+    pcg_ms, pcg_bytes = M.time_pcg(fcu.FCU_MIXED, iterations=pcg_iters, reps=5)
+    achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9
+    traffic_pcg = _profile_traffic("pcg_persistent_fp32_elasticity_c2.txt")
 
     # e2e through the public API from pinned host buffers, every timed step
     e2e_ms = []
@@ -419,13 +425,21 @@ def run_cuda(args, cfg):
                       "gbs_cold": spmv64_bytes / (spmv64_ms * 1e-3) / 1e9, "bytes": spmv64_bytes,
                       "frac_cold": spmv64_bytes / (spmv64_ms * 1e-3) / 1e9 / peak,
                       "frac_warm": spmv64_bytes / (spmv64_warm_ms * 1e-3) / 1e9 / peak, "traffic": traffic64},
-        "roofline": {"kernel": "k_spmv_tiled<1,float> (mixed operator: FP32 3x3-block SpMV, bulk-copy staged "
-                               "tiles, p.Ap partials)", "bound": "hbm",
-                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "bytes_per_launch": spmv_bytes,
-                     "timing": "mean of 20 single launches, each after a 256 MiB read sweep that evicts L2 (clean lines, as an ncu cache flush leaves it)",
-                     "warm": {"ms": spmv_warm_ms, "frac": spmv_bytes / (spmv_warm_ms * 1e-3) / 1e9 / peak,
-                              "timing": "mean of 50 back-to-back launches"}},
+        "roofline": {"kernel": "k_pcg_persistent<1,float,64> (the mixed PCG loop: FP32 3x3-block SpMV from "
+                               "bulk-copy staged tiles, vector update, grid barriers; one cooperative launch)",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic_pcg, "bytes_per_launch": pcg_bytes,
+                     "iterations_per_launch": pcg_iters, "ms_per_launch": pcg_ms,
+                     "us_per_iteration": pcg_ms * 1e3 / pcg_iters,
+                     "timing": f"mean of 5 launches of {pcg_iters} iterations, each after a 256 MiB read sweep "
+                               "that evicts L2",
+                     "spmv_fp32": {"kernel": "k_spmv_tiled<1,float> (the same product as a standalone launch)",
+                                   "bytes_per_launch": spmv_bytes, "traffic": traffic,
+                                   "ms_cold": spmv_ms, "frac_cold": spmv_bytes / (spmv_ms * 1e-3) / 1e9 / peak,
+                                   "ms_warm": spmv_warm_ms,
+                                   "frac_warm": spmv_bytes / (spmv_warm_ms * 1e-3) / 1e9 / peak,
+                                   "timing": "cold: mean of 20 single launches each after a 256 MiB read sweep; "
+                                             "warm: mean of 50 back-to-back launches"}},
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "e2e": {"value": n / (statistics.mean(e2e_ms) * 1e-3), "unit": "DOF/s", "h2d_bytes_per_step": h2d,
@@ -874,9 +888,15 @@ def profile_case(name):
                        each after an L2 flush, shape tuning off
       spmv_c2          the same on the C2 system (421,443 dofs)
       p2_c3            P2 stiffness of the C3 cube (64^3 x 6 tets, random
-                       kappa), assembled 3 times (for one-pass metrics only)"""
+                       kappa), assembled 3 times (for one-pass metrics only)
+      pcg_c2           the mixed PCG's persistent loop on the C2 system: one
+                       launch of exactly 300 iterations after an L2 flush
+                       (the launch the bench's roofline times; shape tuning
+                       off)
+      pcg_c2_small     the same loop on the 32x8x8 beam (24k dofs), 20
+                       iterations, for the full-section capture"""
     import torch
-    if name in ("spmv_c2p", "spmv_c2"):
+    if name in ("spmv_c2p", "spmv_c2", "pcg_c2", "pcg_c2_small"):
         os.environ["FCU_TUNE"] = "0"   # no shape-tuning launches before the captured ones
     import fenics_cuda as fcu
     ctx = fcu.Context(0)
@@ -890,6 +910,18 @@ def profile_case(name):
         b = V.body_force([0.0, 0.0, -7.8e4])
         M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
         M.time_spmv(fcu.FCU_MIXED, reps=3, cold=True)
+        ctx.synchronize()
+        M.close(); V.close()
+    elif name in ("pcg_c2", "pcg_c2_small"):
+        dims = (128, 32, 32) if name == "pcg_c2" else (32, 8, 8)
+        mesh = fcu.box_beam(4.0, 1.0, 1.0, *dims)
+        V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+        M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+        cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+        dofs = (3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64)
+        b = V.body_force([0.0, 0.0, -7.8e4])
+        M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
+        M.time_pcg(fcu.FCU_MIXED, iterations=300 if name == "pcg_c2" else 20, reps=1)
         ctx.synchronize()
         M.close(); V.close()
     elif name in ("elasticity_c2", "mass_c2", "block_update_c2"):

@@ -400,4 +400,14 @@ extern "C" {
         ms_per_launch: *mut f64,
         bytes_per_launch: *mut f64,
     ) -> c_int;
+    pub fn fcu_time_pcg(
+        ctx: fcu_ctx,
+        m: fcu_matrix,
+        precision: c_int,
+        iterations: i64,
+        reps: c_int,
+        flush_bytes: usize,
+        ms_per_launch: *mut f64,
+        bytes_per_launch: *mut f64,
+    ) -> c_int;
 }

@@ -29,6 +29,7 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
 void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev);
 void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes);
 void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_bytes, double* ms, double* bytes);
+void time_pcg_impl(fcu_matrix m, int precision, i64 iters, int reps, size_t flush_bytes, double* ms, double* bytes);
 int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
                    i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
                    fcu_solve_info* info, const int* fixed_shape = nullptr);
@@ -1500,6 +1501,16 @@ int fcu_time_spmv_cold(fcu_ctx ctx, fcu_matrix m, int precision, int reps, size_
     if (!m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
     if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
     time_spmv_cold_impl(m, precision, reps, flush_bytes, ms_per_launch, bytes_per_launch);
+  });
+}
+
+int fcu_time_pcg(fcu_ctx ctx, fcu_matrix m, int precision, int64_t iterations, int reps, size_t flush_bytes,
+                 double* ms_per_launch, double* bytes_per_launch) {
+  return guarded(ctx, [&] {
+    if (!m || !ms_per_launch || !bytes_per_launch || reps < 0 || iterations < 1) fail(FCU_ERR_BAD_ARG, "bad arguments");
+    if (!m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
+    time_pcg_impl(m, precision, iterations, reps, flush_bytes, ms_per_launch, bytes_per_launch);
   });
 }
 

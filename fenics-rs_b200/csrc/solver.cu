@@ -278,6 +278,30 @@ __device__ __forceinline__ void store_pap_partial(double dot, double* __restrict
   }
 }
 
+// alpha = r.z / p.Ap from the state record `st`, or the end of the solve:
+// cg.rs:102-107 make |p.Ap| < 1e-30 a breakdown (Err); the GPU solvers
+// (gpu.rs:1326-1329, 1034-1037) stop with Ok when p.Ap <= 1e-30, the
+// iteration counting as done; a fault flag ends it with FCU_ERR_CUDA. The
+// ending is written into `st` when `record` is set. Returns false when the
+// solve ends here.
+__device__ __forceinline__ bool alpha_decide(CgState* st, double pap, bool fault, bool record, double* alpha) {
+  const bool brk = !st->timing && (st->gpu_semantics ? !(pap > 1e-30) : fabs(pap) < 1e-30);
+  if (fault || brk) {
+    if (record) {
+      st->done = 1;
+      if (fault) {
+        st->status = FCU_ERR_CUDA;
+      } else {
+        st->status = st->gpu_semantics ? FCU_OK : FCU_ERR_BREAKDOWN;
+        st->iter += 1;
+      }
+    }
+    return false;
+  }
+  *alpha = st->rz / pap;
+  return true;
+}
+
 // The update kernel's alpha = r.z / p.Ap. Every block adds the SpMV's np
 // per-block partials in the same fixed order (so all blocks hold the same
 // alpha, and it is the same in every run), which takes the SpMV's grid-wide
@@ -303,23 +327,7 @@ __device__ __forceinline__ bool take_alpha(CgState* st, const double* __restrict
     pap_s = t;
   }
   __syncthreads();
-  const double pap = pap_s;
-  const bool fault = st->fault != 0;
-  const bool brk = !st->timing && (st->gpu_semantics ? !(pap > 1e-30) : fabs(pap) < 1e-30);
-  if (fault || brk) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      st->done = 1;
-      if (fault) {
-        st->status = FCU_ERR_CUDA;
-      } else {
-        st->status = st->gpu_semantics ? FCU_OK : FCU_ERR_BREAKDOWN;
-        st->iter += 1;
-      }
-    }
-    return false;
-  }
-  *alpha = st->rz / pap;
-  return true;
+  return alpha_decide(st, pap_s, st->fault != 0, blockIdx.x == 0 && threadIdx.x == 0, alpha);
 }
 
 // Reads the stop flags once per block (block 0 of the update kernel may set
@@ -519,6 +527,83 @@ struct EmitApOwn {
   }
 };
 
+// One tile of the tiled SpMV, computed by the consumer warps from the ring
+// stage at `base`. `tile_r0` is the first row of a fixed-size tile (BLK
+// tiles carry theirs in the header). Each warp releases the stage on
+// `empty_bar` as soon as it has read its operands from it.
+template <bool DIFF, class T, int TR, int BS, bool BLK, class GX, class Emit>
+__device__ __forceinline__ void consume_tile(const unsigned char* base, int cap_blocks, i64 tile_r0, int row_in_tile,
+                                             int sub, int lane, unsigned long long* empty_bar, const GX& gx,
+                                             Emit& emit) {
+  constexpr int LPR = 32 * SPMV_CONSUMER_WARPS / TR;
+  const TileHeader* h = reinterpret_cast<const TileHeader*>(base);
+  const int* rps = reinterpret_cast<const int*>(base + align128(sizeof(TileHeader))) + (BLK ? h->rp_off : 0);
+  const unsigned char* cs = base + align128(sizeof(TileHeader)) + align128((TR + 1) * 4 + 16);
+  const unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
+  const int* cis = reinterpret_cast<const int*>(cs + h->col_off);
+  const T* vls = reinterpret_cast<const T*>(vs + h->val_off);
+  const int b0 = h->b0;
+  const i64 row = BLK ? (i64)h->r0 + row_in_tile : tile_r0 + row_in_tile;
+  const bool valid = row_in_tile < h->rows;
+  if constexpr (BS == 1) {
+    // scalar row: lane `sub` sums entries sub, sub + LPR, ... (difference
+    // form for the mixed operator: the diagonal slot holds the row sum)
+    T a = T(0), xo = T(0);
+    if (valid) {
+      xo = gx(row);
+      const int kb1 = rps[row_in_tile + 1] - b0;
+#pragma unroll 2
+      for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += LPR) {
+        const int c = cis[kb];
+        const T v = vls[kb];
+        const T y = DIFF ? (c == (int)row ? xo : gx(c) - xo) : gx(c);
+        a += v * y;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(empty_bar)) : "memory");
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) a += __shfl_xor_sync(FULL, a, o);
+    if (valid && sub == 0) emit(row, 0, a, xo);
+    return;
+  }
+  T a0 = T(0), a1 = T(0), a2 = T(0);
+  T x0 = T(0), x1 = T(0), x2 = T(0);
+  if (valid) {
+    x0 = gx(3 * row);
+    x1 = gx(3 * row + 1);
+    x2 = gx(3 * row + 2);
+    const int kb1 = rps[row_in_tile + 1] - b0;
+#pragma unroll 2
+    for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += LPR) {
+      const int c = cis[kb];
+      const T* v = vls + 9 * kb;
+      const i64 c3 = 3 * (i64)c;
+      T y0, y1, y2;
+      if (DIFF && c == (int)row) {
+        y0 = x0; y1 = x1; y2 = x2;
+      } else if (DIFF) {
+        y0 = gx(c3) - x0; y1 = gx(c3 + 1) - x1; y2 = gx(c3 + 2) - x2;
+      } else {
+        y0 = gx(c3); y1 = gx(c3 + 1); y2 = gx(c3 + 2);
+      }
+      a0 += v[0] * y0 + v[1] * y1 + v[2] * y2;
+      a1 += v[3] * y0 + v[4] * y1 + v[5] * y2;
+      a2 += v[6] * y0 + v[7] * y1 + v[8] * y2;
+    }
+  }
+  __syncwarp();
+  if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(empty_bar)) : "memory");
+#pragma unroll
+  for (int o = LPR / 2; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(FULL, a0, o);
+    a1 += __shfl_xor_sync(FULL, a1, o);
+    a2 += __shfl_xor_sync(FULL, a2, o);
+  }
+  if (valid && sub < 3)
+    emit(row, sub, sub == 0 ? a0 : (sub == 1 ? a1 : a2), sub == 0 ? x0 : (sub == 1 ? x1 : x2));
+}
+
 // The matrix does not depend on the preceding kernel, so the ring's first
 // stages are issued before the programmatic dependency wait and overlap the
 // predecessor's tail; the producer warp's lanes fetch the row-pointer bounds
@@ -648,73 +733,8 @@ __device__ __forceinline__ bool tiled_rows(const int* __restrict__ rp, const int
       if (lane == 0) atomicExch(&st->fault, 1);
       break;
     }
-    unsigned char* base = tile_smem + s * stage_bytes;
-    const TileHeader* h = reinterpret_cast<const TileHeader*>(base);
-    const int* rps = reinterpret_cast<const int*>(base + align128(sizeof(TileHeader))) + (BLK ? h->rp_off : 0);
-    const unsigned char* cs = base + align128(sizeof(TileHeader)) + align128((TR + 1) * 4 + 16);
-    const unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
-    const int* cis = reinterpret_cast<const int*>(cs + h->col_off);
-    const T* vls = reinterpret_cast<const T*>(vs + h->val_off);
-    const int b0 = h->b0;
-    const i64 row = BLK ? (i64)h->r0 + row_in_tile : (blockIdx.x + (i64)k * G) * TR + row_in_tile;
-    const bool valid = row_in_tile < h->rows;
-    if constexpr (BS == 1) {
-      // scalar row: lane `sub` sums entries sub, sub + LPR, ... (difference
-      // form for the mixed operator: the diagonal slot holds the row sum)
-      T a = T(0), xo = T(0);
-      if (valid) {
-        xo = gx(row);
-        const int kb1 = rps[row_in_tile + 1] - b0;
-#pragma unroll 2
-        for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += LPR) {
-          const int c = cis[kb];
-          const T v = vls[kb];
-          const T y = DIFF ? (c == (int)row ? xo : gx(c) - xo) : gx(c);
-          a += v * y;
-        }
-      }
-      __syncwarp();
-      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
-#pragma unroll
-      for (int o = LPR / 2; o > 0; o >>= 1) a += __shfl_xor_sync(FULL, a, o);
-      if (valid && sub == 0) emit(row, 0, a, xo);
-      continue;
-    }
-    T a0 = T(0), a1 = T(0), a2 = T(0);
-    T x0 = T(0), x1 = T(0), x2 = T(0);
-    if (valid) {
-      x0 = gx(3 * row);
-      x1 = gx(3 * row + 1);
-      x2 = gx(3 * row + 2);
-      const int kb1 = rps[row_in_tile + 1] - b0;
-#pragma unroll 2
-      for (int kb = rps[row_in_tile] - b0 + sub; kb < kb1; kb += LPR) {
-        const int c = cis[kb];
-        const T* v = vls + 9 * kb;
-        const i64 c3 = 3 * (i64)c;
-        T y0, y1, y2;
-        if (DIFF && c == (int)row) {
-          y0 = x0; y1 = x1; y2 = x2;
-        } else if (DIFF) {
-          y0 = gx(c3) - x0; y1 = gx(c3 + 1) - x1; y2 = gx(c3 + 2) - x2;
-        } else {
-          y0 = gx(c3); y1 = gx(c3 + 1); y2 = gx(c3 + 2);
-        }
-        a0 += v[0] * y0 + v[1] * y1 + v[2] * y2;
-        a1 += v[3] * y0 + v[4] * y1 + v[5] * y2;
-        a2 += v[6] * y0 + v[7] * y1 + v[8] * y2;
-      }
-    }
-    __syncwarp();
-    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
-#pragma unroll
-    for (int o = LPR / 2; o > 0; o >>= 1) {
-      a0 += __shfl_xor_sync(FULL, a0, o);
-      a1 += __shfl_xor_sync(FULL, a1, o);
-      a2 += __shfl_xor_sync(FULL, a2, o);
-    }
-    if (valid && sub < 3)
-      emit(row, sub, sub == 0 ? a0 : (sub == 1 ? a1 : a2), sub == 0 ? x0 : (sub == 1 ? x1 : x2));
+    consume_tile<DIFF, T, TR, BS, BLK>(tile_smem + s * stage_bytes, cap_blocks, (blockIdx.x + (i64)k * G) * TR,
+                                       row_in_tile, sub, lane, &empty[s], gx, emit);
   }
   return true;
 }
@@ -746,6 +766,27 @@ __device__ __forceinline__ void decide_after_update(CgState* st, double rz_new, 
   const double den = st->gpu_semantics ? fmax(st->rz, 1e-30) : st->rz;
   st->beta = rz_new / den;
   st->rz = rz_new;
+}
+
+// Mixed precision: replace the residual when it has dropped by `delta` since
+// the last replacement or claims convergence (the host runs the replacement
+// next); otherwise continue.
+__device__ __forceinline__ void decide_after_update_mixed(CgState* st, double rz_new, double rr) {
+  st->iter += 1;
+  st->rr = rr;
+  const double res = sqrt(rr);
+  const double rel = st->bnorm > 0.0 ? res / st->bnorm : res;
+  st->do_update = (rel < st->tol || res < st->delta * st->maxr) ? 1 : 0;
+  st->pause = st->do_update;
+  if (!st->do_update) {
+    if (st->iter >= st->max_iter) {
+      st->done = 1;
+      st->status = FCU_ERR_NO_CONVERGENCE;
+      return;
+    }
+    st->beta = rz_new / st->rz;
+    st->rz = rz_new;
+  }
 }
 
 // x += alpha p ; r -= alpha Ap ; z = D^-1 r (stored as T) ; (r.z, r.r).
@@ -813,26 +854,374 @@ __global__ void __launch_bounds__(VBLOCK, 5) k_update(i64 n, double* __restrict_
   }
   double v[2] = {rz, rr}, tot[2];
   if (grid_reduce<2>(v, partials, st->ticket[1], tot) && threadIdx.x == 0) {
-    if (sizeof(T) == 8) {
-      decide_after_update(st, tot[0], tot[1]);
-    } else {
-      // mixed: replace the residual when it has dropped by `delta` since the
-      // last replacement or claims convergence; otherwise continue.
-      st->iter += 1;
-      st->rr = tot[1];
-      const double res = sqrt(tot[1]);
-      const double rel = st->bnorm > 0.0 ? res / st->bnorm : res;
-      st->do_update = (rel < st->tol || res < st->delta * st->maxr) ? 1 : 0;
-      st->pause = st->do_update;  // the host runs the replacement next
-      if (!st->do_update) {
-        if (st->iter >= st->max_iter) {
-          st->done = 1;
-          st->status = FCU_ERR_NO_CONVERGENCE;
-          return;
-        }
-        st->beta = tot[0] / st->rz;
-        st->rz = tot[0];
+    if (sizeof(T) == 8) decide_after_update(st, tot[0], tot[1]);
+    else decide_after_update_mixed(st, tot[0], tot[1]);
+  }
+}
+
+// --- persistent PCG (3x3-block tiled operator, point Jacobi) -----------------
+// The iteration loop in one cooperative launch. The CTAs of the tiled SpMV's
+// grid stay resident, and the two grid-wide steps of an iteration (p.Ap
+// before alpha; r.z and r.r before beta and the stopping test) are grid
+// barriers instead of kernel boundaries. Warp 0 keeps streaming the matrix's
+// tiles through the shared-memory ring across iterations (the matrix does not
+// change), so the first tiles of the next product are in flight while the
+// consumer warps update the vectors. No separate direction step: z and p are
+// kept interleaved as pairs zp[i] = (z_i, p_i), the product forms
+// p = z + beta p_old from one pair load per operand, and the update forms the
+// same value for its own elements (same operands, same fused multiply-add)
+// and stores the new pair. Every CTA adds the per-CTA partials in the same
+// fixed order and takes the same decisions on its own copy of the state
+// record; CTA 0 writes that copy back when the loop ends. The loop ends when
+// the solve is over or, in mixed precision, when a residual replacement is due
+// (the host runs it and launches the loop again). Every wait is bounded: a
+// wait that gives up sets the fault flag, and the CTA ends the loop.
+__device__ __forceinline__ float dir_fma(float beta, float pold, float z) { return __fmaf_rn(beta, pold, z); }
+__device__ __forceinline__ double dir_fma(double beta, double pold, double z) { return __fma_rn(beta, pold, z); }
+
+template <class T>
+struct Pair;
+template <>
+struct Pair<float> {
+  using type = float2;
+};
+template <>
+struct Pair<double> {
+  using type = double2;
+};
+
+// The direction operand of the persistent loop. The pairs are written by the
+// same kernel (other CTAs, before the last grid barrier), so they are read
+// with ordinary coherent loads, never through the read-only path.
+template <class T>
+struct XDirPair {
+  using T2 = typename Pair<T>::type;
+  const T2* zp;
+  T beta;
+  __device__ __forceinline__ T operator()(i64 i) const {
+    const T2 v = zp[i];
+    return dir_fma(beta, v.y, v.x);
+  }
+};
+
+// zp[i] = (z[i], p[i]), or with p == nullptr only the z half (after a
+// residual replacement, which recomputes z and keeps p).
+template <class T>
+__global__ void k_zp_pack(const T* __restrict__ z, const T* __restrict__ p, i64 n,
+                          typename Pair<T>::type* __restrict__ zp) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    if (p) zp[i] = {z[i], p[i]};
+    else zp[i].x = z[i];
+  }
+}
+
+constexpr unsigned BARRIER_LIMIT = 1u << 22;  // polls of a grid barrier (~1 us each) before giving up
+
+// Named barrier of the consumer warps (warp 0, the producer, does not join).
+__device__ __forceinline__ void consumer_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"(32 * SPMV_CONSUMER_WARPS) : "memory");
+}
+
+// Grid barrier, entered by all consumer threads right after a consumer_sync
+// that follows their writes: the first consumer thread of each CTA arrives
+// with a release add (covering its CTA's writes, ordered before it by that
+// CTA barrier), polls the arrival count with relaxed loads until `target`,
+// then an acquire fence; the CTA's consumer warps pass together. False when
+// the poll gave up.
+__device__ __forceinline__ bool grid_barrier(unsigned long long* bar, unsigned long long target, int ctid) {
+  __shared__ int ok_s;
+  if (ctid == 0) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(bar) : "memory");
+    int ok = 0;
+    for (unsigned i = 0; i < BARRIER_LIMIT; ++i) {
+      unsigned long long v;
+      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+      if (v >= target) {
+        ok = 1;
+        break;
       }
+      __nanosleep(32);
+    }
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    ok_s = ok;
+  }
+  consumer_sync();
+  return ok_s != 0;
+}
+
+// Sums of the G per-CTA partials src[j * MAXG + 0 .. G) in one fixed order, the same
+// in every CTA: consumer thread t loads partials t, t + NCT, ... (one each
+// while G <= NCT, so the loads are one round trip), each warp adds its lanes
+// in a fixed shuffle tree, and the warps' sums are added in warp order. Called
+// by all consumer threads; the sums are valid in the first consumer thread.
+template <int NV>
+__device__ __forceinline__ void sum_partials(const double* src, int G, int ctid, double (&tot)[NV]) {
+  constexpr int NCT = 32 * SPMV_CONSUMER_WARPS;
+  __shared__ double ws[NV][SPMV_CONSUMER_WARPS];
+  double v[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    v[j] = 0.0;
+    for (int b = ctid; b < G; b += NCT) v[j] += __ldcg(src + j * MAXG + b);
+    v[j] = warp_sum(v[j]);
+    if ((ctid & 31) == 0) ws[j][ctid >> 5] = v[j];
+  }
+  consumer_sync();
+  if (ctid == 0)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double t = 0.0;
+      for (int w = 0; w < SPMV_CONSUMER_WARPS; ++w) t += ws[j][w];
+      tot[j] = t;
+    }
+}
+
+template <bool DIFF, class T, int TR>
+__global__ void __launch_bounds__(SPMV_THREADS, TILED_CTAS_PER_SM) k_pcg_persistent(
+    const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ val, i64 nrows, int cap_blocks,
+    int nstage, i64 n, double* x, double* r, const double* __restrict__ invd, typename Pair<T>::type* zp, T* ap,
+    CgState* st, double* partials, unsigned long long* bar) {
+  using T2 = typename Pair<T>::type;
+  constexpr int BS = 3;
+  constexpr int LPR = 32 * SPMV_CONSUMER_WARPS / TR;
+  constexpr int NCT = 32 * SPMV_CONSUMER_WARPS;  // consumer threads
+  extern __shared__ __align__(128) unsigned char tile_smem[];
+  __shared__ unsigned long long full[MAX_STAGES], empty[MAX_STAGES];
+  __shared__ CgState ls;  // this CTA's copy of the state record
+  __shared__ double red[2][SPMV_CONSUMER_WARPS];
+  __shared__ double alpha_s;
+  __shared__ int stop_s;             // consumers: the loop has ended
+  __shared__ volatile int ended_s;   // consumers -> producer: no more tiles are needed
+  __shared__ volatile int pfault_s;  // producer -> consumers: a ring wait gave up
+  const size_t stage_bytes = tile_stage_bytes<T, TR, BS>(cap_blocks);
+  const i64 ntiles = (nrows + TR - 1) / TR;
+  const i64 G = gridDim.x;
+  const int mytiles = blockIdx.x < ntiles ? (int)((ntiles - blockIdx.x + G - 1) / G) : 0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < nstage; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], SPMV_CONSUMER_WARPS);
+    }
+    fence_mbar_init();
+    ended_s = 0;
+    pfault_s = 0;
+  }
+  static_assert(sizeof(CgState) % 4 == 0, "state record copied by words");
+  for (int i = tid; i < (int)(sizeof(CgState) / 4); i += blockDim.x)
+    reinterpret_cast<int*>(&ls)[i] = reinterpret_cast<const int*>(st)[i];
+  __syncthreads();
+
+  if (warp == 0) {
+    // producer: tile q of the stream is tile q % mytiles of the CTA's share
+    if (mytiles == 0 || ls.done || ls.pause) return;
+    int pb0 = 0, pb1 = 0, desc0 = -1;
+    int k = 0;            // tile of the CTA's share
+    int s = 0;            // ring stage
+    unsigned ph = 0;      // phase parity of the stage's current use
+    int issued = 0;       // copies issued, counted up to nstage
+    for (;;) {
+      if ((k & 31) == 0 && desc0 != k) {
+        const i64 t = blockIdx.x + (i64)(k + lane) * G;
+        if (t < ntiles) {
+          pb0 = rp[t * TR];
+          pb1 = rp[min(t * TR + TR, nrows)];
+        }
+        desc0 = k;
+      }
+      int state = 1;  // 1: stage free, 2: loop ended, 3: wait gave up
+      if (lane == 0) {
+        if (issued >= nstage) {
+          state = 3;
+          for (unsigned i = 0; i < WAIT_LIMIT; ++i) {
+            if (mbar_try_wait(&empty[s], ph ^ 1u)) {
+              state = 1;
+              break;
+            }
+            if (ended_s) {
+              state = 2;
+              break;
+            }
+          }
+        } else if (ended_s) {
+          state = 2;
+        }
+      }
+      state = __shfl_sync(FULL, state, 0);
+      if (state != 1) {
+        if (state == 3 && lane == 0) {
+          atomicExch(&st->fault, 1);
+          pfault_s = 1;
+        }
+        break;
+      }
+      const int b0 = __shfl_sync(FULL, pb0, k & 31), b1 = __shfl_sync(FULL, pb1, k & 31);
+      if (lane == 0) {
+        unsigned char* base = tile_smem + s * stage_bytes;
+        TileHeader* h = reinterpret_cast<TileHeader*>(base);
+        unsigned char* rps = base + align128(sizeof(TileHeader));
+        unsigned char* cs = rps + align128((TR + 1) * 4 + 16);
+        unsigned char* vs = cs + align128((size_t)cap_blocks * 4 + 32);
+        const i64 r0 = (blockIdx.x + (i64)k * G) * TR;
+        const int rows = (int)min((i64)TR, nrows - r0);
+        const unsigned rp_bytes = (unsigned)(((rows + 1) * 4 + 15) & ~15);
+        const uintptr_t c_lo = reinterpret_cast<uintptr_t>(ci + b0) & ~(uintptr_t)15;
+        const uintptr_t c_hi = (reinterpret_cast<uintptr_t>(ci + b1) + 15) & ~(uintptr_t)15;
+        const uintptr_t v_lo = reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) & ~(uintptr_t)15;
+        const uintptr_t v_hi = (reinterpret_cast<uintptr_t>(val + 9 * (i64)b1) + 15) & ~(uintptr_t)15;
+        h->b0 = b0;
+        h->rows = rows;
+        h->col_off = (int)(reinterpret_cast<uintptr_t>(ci + b0) - c_lo);
+        h->val_off = (int)(reinterpret_cast<uintptr_t>(val + 9 * (i64)b0) - v_lo);
+        const unsigned cb = (unsigned)(c_hi - c_lo), vb = (unsigned)(v_hi - v_lo);
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&full[s], rp_bytes + cb + vb);
+        bulk_load(rps, rp + r0, rp_bytes, &full[s]);
+        if (cb) bulk_load(cs, reinterpret_cast<const void*>(c_lo), cb, &full[s]);
+        if (vb) bulk_load(vs, reinterpret_cast<const void*>(v_lo), vb, &full[s]);
+      }
+      if (issued < nstage) ++issued;
+      if (++k == mytiles) k = 0;
+      if (++s == nstage) {
+        s = 0;
+        ph ^= 1u;
+      }
+    }
+    // copies still in flight (at most one per stage) land before the CTA exits
+    if (lane == 0)
+      for (int i = 1; i <= issued; ++i) {
+        int s2 = s - i;
+        unsigned p2 = ph;
+        if (s2 < 0) {
+          s2 += nstage;
+          p2 ^= 1u;
+        }
+        mbar_wait(&full[s2], p2);
+      }
+    return;
+  }
+
+  // consumer warps
+  const int ctid = tid - 32;
+  const int sub = lane % LPR;
+  const int row_in_tile = (warp - 1) * (32 / LPR) + lane / LPR;
+  int cs = 0;                  // ring stage of the next tile
+  unsigned cph = 0;            // its phase parity
+  unsigned long long gen = 0;  // grid barriers passed
+  const i64 step = G * NCT;
+  const i64 i0 = (i64)blockIdx.x * NCT + ctid;  // the thread's first vector element
+  bool run = !(ls.done || ls.pause);
+  while (run) {
+    const T beta = (T)ls.beta;
+    // Ap = A p with p = z + beta p_old formed per operand
+    XDirPair<T> gx{zp, beta};
+    EmitApOwn<T, BS> em{ap};
+    bool tiles_ok = true;
+    for (int k = 0; k < mytiles; ++k) {
+      bool got = false;
+      for (unsigned i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_try_wait(&full[cs], cph)) {
+          got = true;
+          break;
+        }
+        if (pfault_s) break;
+      }
+      if (!got) {
+        tiles_ok = false;
+        break;
+      }
+      consume_tile<DIFF, T, TR, BS, false>(tile_smem + cs * stage_bytes, cap_blocks, (blockIdx.x + (i64)k * G) * TR,
+                                           row_in_tile, sub, lane, &empty[cs], gx, em);
+      if (++cs == nstage) {
+        cs = 0;
+        cph ^= 1u;
+      }
+    }
+    if (!tiles_ok && lane == 0) atomicExch(&st->fault, 1);
+    double d = warp_sum(em.dot);
+    if (lane == 0) red[0][warp - 1] = d;
+    consumer_sync();
+    if (ctid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < SPMV_CONSUMER_WARPS; ++w) t += red[0][w];
+      partials[PAP_REGION * MAXG + blockIdx.x] = t;
+    }
+    bool ok = grid_barrier(bar, ++gen * (unsigned long long)G, ctid);
+    // alpha from the G partials, added in the same order in every CTA
+    double pap[1] = {0.0};
+    sum_partials<1>(partials + PAP_REGION * MAXG, ok ? (int)G : 0, ctid, pap);
+    if (ctid == 0) {
+      const bool fault = !ok || *reinterpret_cast<volatile int*>(&st->fault) != 0;
+      if (!ok) atomicExch(&st->fault, 1);
+      double a = 0.0;
+      stop_s = alpha_decide(&ls, pap[0], fault, true, &a) ? 0 : 1;
+      alpha_s = a;
+    }
+    consumer_sync();
+    if (stop_s) break;
+    const double alpha = alpha_s;
+    // x += alpha p ; r -= alpha Ap ; z = D^-1 r ; (z, p) stored ; (r.z, r.r)
+    double rz = 0.0, rr = 0.0;
+    // (all loads of an element before its stores: the vectors are not
+    // declared unaliased, so the compiler keeps loads behind earlier stores)
+    for (i64 i = i0; i < n; i += step) {
+      const T2 v = zp[i];
+      const T av = __ldcg(ap + i);
+      const double xv = x[i], rv = r[i], dv = invd[i];
+      const T pi = dir_fma(beta, v.y, v.x);
+      const double ri = rv - alpha * (double)av;
+      const double zi = ri * dv;
+      zp[i] = {(T)zi, pi};
+      x[i] = xv + alpha * (double)pi;
+      r[i] = ri;
+      rz += ri * zi;
+      rr += ri * ri;
+    }
+    rz = warp_sum(rz);
+    rr = warp_sum(rr);
+    if (lane == 0) {
+      red[0][warp - 1] = rz;
+      red[1][warp - 1] = rr;
+    }
+    consumer_sync();
+    if (ctid == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < SPMV_CONSUMER_WARPS; ++w) {
+        a += red[0][w];
+        b += red[1][w];
+      }
+      partials[blockIdx.x] = a;
+      partials[MAXG + blockIdx.x] = b;
+    }
+    ok = grid_barrier(bar, ++gen * (unsigned long long)G, ctid);
+    double sums[2] = {0.0, 0.0};
+    sum_partials<2>(partials, ok ? (int)G : 0, ctid, sums);
+    if (ctid == 0) {
+      if (!ok || *reinterpret_cast<volatile int*>(&st->fault) != 0) {
+        if (!ok) atomicExch(&st->fault, 1);
+        ls.done = 1;
+        ls.status = FCU_ERR_CUDA;
+      } else if (sizeof(T) == 8) {
+        decide_after_update(&ls, sums[0], sums[1]);
+      } else {
+        decide_after_update_mixed(&ls, sums[0], sums[1]);
+      }
+      stop_s = (ls.done || ls.pause) ? 1 : 0;
+    }
+    consumer_sync();
+    run = stop_s == 0;
+  }
+  if (ctid == 0) {
+    ended_s = 1;
+    if (blockIdx.x == 0) {
+      st->rz = ls.rz;
+      st->beta = ls.beta;
+      st->rr = ls.rr;
+      st->iter = ls.iter;
+      st->done = ls.done;
+      st->status = ls.status;
+      st->do_update = ls.do_update;
+      st->pause = ls.pause;
     }
   }
 }
@@ -1201,6 +1590,9 @@ struct Workspace {
   DBuf<double> z64, pa64, pb64, ap64;  // FP64 path: z, p (two buffers), Ap
   DBuf<float> z32, pa32, pb32, ap32;   // mixed path
   DBuf<CgState> st;
+  DBuf<unsigned long long> bar;  // arrival count of the persistent loop's grid barriers
+  DBuf<float2> zp32;             // persistent loop: (z, p) pairs, mixed
+  DBuf<double2> zp64;            // persistent loop: (z, p) pairs, FP64
   CgState* host_st = nullptr;  // two pinned records: [0] set-up and final state, [0]/[1] alternate between replays
   cudaEvent_t ev[2] = {nullptr, nullptr};  // a replay's state record has arrived on the host
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -1630,6 +2022,119 @@ void enqueue_iteration(fcu_matrix m, Workspace* w, bool mixed, int parity) {
 
 int launches_per_iteration() { return fuse_direction() ? 2 : 3; }
 
+// The persistent loop (k_pcg_persistent) runs on 3x3-block matrices on the
+// tiled SpMV with point-Jacobi preconditioning.
+bool persistent_capable(fcu_matrix m) {
+  return m->bs == 3 && use_tiled_spmv() && !m->bdinv.p && !fuse_direction();
+}
+
+// Which solves take the persistent loop: mixed precision by default (on B200
+// at 421k and 1.57M elasticity dofs it beats the per-iteration graph by
+// 3-6% per iteration); FP64 keeps the graph, whose tiled SpMV gathers one
+// 8-byte operand per component instead of the loop's 16-byte (z, p) pair
+// (equal at 421k dofs, 12% faster at 1.57M). FCU_PERSISTENT=0 keeps the graph
+// for both, FCU_PERSISTENT=2 takes the loop for both.
+bool use_persistent(fcu_matrix m, bool mixed) {
+  static int v = [] {
+    const char* e = getenv("FCU_PERSISTENT");
+    return e ? atoi(e) : 1;
+  }();
+  return persistent_capable(m) && (v == 2 || (v == 1 && mixed));
+}
+
+// One cooperative launch of the persistent loop: the tiled SpMV's ring and
+// CTAs (up to TILED_CTAS_PER_SM per SM, all resident); the launch fails
+// rather than run when they cannot all be resident. The caller zeroes the
+// barrier count (w->bar) on the stream first.
+template <bool DIFF, class T, int TR>
+void launch_persistent_tr(fcu_matrix m, Workspace* w, const T* val, typename Pair<T>::type* zp, T* ap) {
+  fcu_ctx ctx = m->ctx;
+  const int cap = TR * max_block_row(m);
+  const size_t stage = tile_stage_bytes<T, TR, 3>(cap);
+  const int nstage = fitted_stages(ctx, w->stages[sizeof(T) == 4 ? 1 : 0], stage);
+  const size_t smem = nstage * stage;
+  auto kern = k_pcg_persistent<DIFF, T, TR>;
+  static int configured_dev = -1;
+  static size_t configured_smem = 0;
+  if (configured_dev != ctx->device || configured_smem < smem) {
+    CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured_dev = ctx->device;
+    configured_smem = smem;
+  }
+  int per_sm = 0;
+  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SPMV_THREADS, smem));
+  if (per_sm < 1) fail(FCU_ERR_UNSUPPORTED, "rows too long for the tiled SpMV");
+  const int grid = std::min(MAXG, std::min(per_sm, TILED_CTAS_PER_SM) * ctx->num_sms);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(SPMV_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m->row_ptr, m->col_idx, val, m->nnodes, cap, nstage, m->n, w->x.p,
+                                w->r.p, (const double*)w->invd.p, zp, ap, w->st.p, w->partials.p, w->bar.p));
+  ctx->launches++;
+}
+
+// The (z, p) pairs of the persistent loop from the solver's z and p vectors;
+// with_p false refreshes only the z half (after a residual replacement).
+void pack_zp(fcu_matrix m, Workspace* w, bool mixed, bool with_p) {
+  fcu_ctx ctx = m->ctx;
+  const i64 n = m->n;
+  const int g = grid_for(n, 256, ctx->num_sms * 8);
+  if (mixed) {
+    if (!w->zp32.p) w->zp32.alloc(n);
+    k_zp_pack<float><<<g, 256, 0, ctx->stream>>>(w->z32.p, with_p ? w->pa32.p : nullptr, n, w->zp32.p);
+  } else {
+    if (!w->zp64.p) w->zp64.alloc(n);
+    k_zp_pack<double><<<g, 256, 0, ctx->stream>>>(w->z64.p, with_p ? w->pa64.p : nullptr, n, w->zp64.p);
+  }
+  LAUNCH_CHECK(ctx);
+}
+
+// One launch of the persistent loop in the solve's precision, after zeroing
+// its barrier count.
+void launch_persistent(fcu_matrix m, Workspace* w, bool mixed) {
+  fcu_ctx ctx = m->ctx;
+  if (!w->bar.p) w->bar.alloc(1);
+  CUDA_CHECK(cudaMemsetAsync(w->bar.p, 0, sizeof(unsigned long long), ctx->stream));
+  if (mixed) {
+    if (tile_rows(4) == 64) launch_persistent_tr<true, float, 64>(m, w, m->val32.p, w->zp32.p, w->ap32.p);
+    else launch_persistent_tr<true, float, 32>(m, w, m->val32.p, w->zp32.p, w->ap32.p);
+  } else {
+    launch_persistent_tr<false, double, 32>(m, w, m->val64.p, w->zp64.p, w->ap64.p);
+  }
+}
+
+// Runs the solve to its end through the persistent loop: one launch in FP64;
+// in mixed precision one per stretch between residual replacements, each
+// replacement run by k_mx_replace between them.
+void run_persistent(fcu_matrix m, Workspace* w, bool mixed, i64 max_iter) {
+  fcu_ctx ctx = m->ctx;
+  CgState* hs = w->host_st;
+  pack_zp(m, w, mixed, true);
+  for (i64 round = 0; round <= max_iter + 1; ++round) {
+    launch_persistent(m, w, mixed);
+    CUDA_CHECK(cudaMemcpyAsync(hs, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    if (hs->done || hs->fault || !(mixed && hs->pause)) break;
+    // r = b - A64 x, z = D^-1 r, and the state's replacement step
+    DISPATCH_ROWS(m->bs, w->vpr, w->grid, K_REPLACE, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->x.p, w->b.p,
+                  w->invd.p, w->r.p, w->z32.p, w->st.p, w->partials.p);
+    pack_zp(m, w, mixed, false);
+  }
+  if (hs->fault && !hs->done) {
+    hs->done = 1;
+    hs->status = FCU_ERR_CUDA;
+  } else if (hs->fault) {
+    hs->status = FCU_ERR_CUDA;
+  }
+}
+
 // Kernels in one replay of the iteration graph.
 int launches_per_replay(bool mixed) { return CHUNK * launches_per_iteration() + (mixed ? 1 : 0); }
 
@@ -1796,6 +2301,8 @@ int run_pcg(fcu_matrix m, const double* b_dev, const double* x0_dev, double* x_d
     w->host_st->done = 1;
     w->host_st->status = FCU_OK;
     w->host_st->iter = 0;
+  } else if (!w->host_st->done && max_iter > 0 && use_persistent(m, mixed)) {
+    run_persistent(m, w, mixed, max_iter);
   } else if (!w->host_st->done && max_iter > 0) {
     // Replays of CHUNK iterations, each followed by a copy of the state
     // record to the host. The host keeps one replay queued beyond the one
@@ -2101,6 +2608,10 @@ __global__ void k_flush_read(const uint4* __restrict__ buf, i64 n, uint4* __rest
   sink[blockIdx.x * (i64)blockDim.x + threadIdx.x] = acc;
 }
 
+__global__ void k_fill_value(double* __restrict__ v, i64 n, double a) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) v[i] = a;
+}
+
 // The same with L2 flushed before each launch: a read of `flush_bytes`
 // evicts the matrix and p, then one SpMV is timed by events on either side.
 // The sweep is queued before the first event, so the launch never waits on
@@ -2142,6 +2653,90 @@ void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_byt
   const double bs2 = (double)m->bs * m->bs;
   const double wv = mixed ? 4.0 : 8.0;
   *bytes = (double)m->nnzb * (bs2 * wv + 4.0) + 4.0 * (double)(m->nnodes + 1) + 2.0 * (double)m->n * wv;
+}
+
+// Algorithmic bytes of one iteration of the persistent loop: the matrix
+// (values, columns, row pointers) once; the product reads z and p_old and
+// writes Ap; the update reads x, r, D^-1 (8-byte) and p_old, z, Ap, and
+// writes x, r (8-byte) and p, z.
+double persistent_bytes_per_iter(fcu_matrix m, bool mixed) {
+  const double w = mixed ? 4.0 : 8.0;
+  const double n = (double)m->n;
+  const double mat = (double)m->nnzb * (9.0 * w + 4.0) + 4.0 * (double)(m->nnodes + 1);
+  return mat + n * 3.0 * w + n * (24.0 + 3.0 * w) + n * (16.0 + 2.0 * w);
+}
+
+// Device time of one launch of the persistent loop running exactly `iters`
+// iterations (no stopping test, no residual replacement, no breakdown exit)
+// from x = 0 on b = 1, after a read sweep of `flush_bytes` that evicts L2;
+// the mean over `reps` launches, each from a fresh start.
+void time_pcg_impl(fcu_matrix m, int precision, i64 iters, int reps, size_t flush_bytes, double* ms,
+                   double* bytes) {
+  if (!persistent_capable(m)) fail(FCU_ERR_UNSUPPORTED, "the persistent loop runs on 3x3-block point-Jacobi systems");
+  const bool mixed = precision == FCU_MIXED;
+  if (mixed && !m->val32.p) fail(FCU_ERR_BAD_ARG, "matrix has no FP32 copy");
+  if (mixed && m->missing_diag) fail(FCU_ERR_UNSUPPORTED, "the mixed operator needs every diagonal block");
+  fcu_ctx ctx = m->ctx;
+  Workspace* w = ensure_ws(m, mixed);
+  if (!w->bar.p) w->bar.alloc(1);
+  ensure_inv_diag(m, w);
+  if (mixed) build_rowsum32(m);
+  tune_spmv(m, w, mixed);
+  const i64 n = m->n;
+  k_fill_value<<<grid_for(n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(w->b.p, n, 1.0);
+  LAUNCH_CHECK(ctx);
+  if (!flush_bytes) flush_bytes = 256ull << 20;
+  flush_bytes = (flush_bytes + 15) / 16 * 16;
+  DBuf<unsigned char> flush;
+  flush.alloc(flush_bytes);
+  CUDA_CHECK(cudaMemsetAsync(flush.p, 0, flush_bytes, ctx->stream));
+  const int fgrid = ctx->num_sms * 8;
+  DBuf<uint4> sink;
+  sink.alloc((size_t)fgrid * 256);
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  double total = 0.0;
+  for (int rep = 0; rep < reps; ++rep) {
+    CgState init{};
+    init.tol = 0.0;
+    init.max_iter = iters;
+    init.delta = 0.0;
+    init.timing = 1;
+    *w->host_st = init;
+    CUDA_CHECK(cudaMemcpyAsync(w->st.p, w->host_st, sizeof(CgState), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_CHECK(cudaMemsetAsync(w->x.p, 0, n * sizeof(double), ctx->stream));
+    if (mixed)
+      DISPATCH_ROWS(m->bs, w->vpr, w->grid, K_INIT32, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->x.p, w->b.p,
+                    w->invd.p, w->r.p, w->z32.p, w->pa32.p, n, w->st.p, w->partials.p);
+    else
+      DISPATCH_ROWS(m->bs, w->vpr, w->grid, K_INIT64, m->row_ptr, m->col_idx, m->val64.p, m->nnodes, w->x.p, w->b.p,
+                    w->invd.p, w->r.p, w->z64.p, w->pa64.p, n, w->st.p, w->partials.p);
+    pack_zp(m, w, mixed, true);
+    k_flush_read<<<fgrid, 256, 0, ctx->stream>>>(reinterpret_cast<const uint4*>(flush.p), (i64)(flush_bytes / 16),
+                                                 sink.p);
+    CUDA_CHECK(cudaGetLastError());
+    CUDA_CHECK(cudaMemsetAsync(w->bar.p, 0, sizeof(unsigned long long), ctx->stream));
+    CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+    if (mixed) {
+      if (tile_rows(4) == 64) launch_persistent_tr<true, float, 64>(m, w, m->val32.p, w->zp32.p, w->ap32.p);
+      else launch_persistent_tr<true, float, 32>(m, w, m->val32.p, w->zp32.p, w->ap32.p);
+    } else {
+      launch_persistent_tr<false, double, 32>(m, w, m->val64.p, w->zp64.p, w->ap64.p);
+    }
+    CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+    CUDA_CHECK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CUDA_CHECK(cudaEventElapsedTime(&t, e0, e1));
+    total += t;
+    CUDA_CHECK(cudaMemcpy(w->host_st, w->st.p, sizeof(CgState), cudaMemcpyDeviceToHost));
+    if (w->host_st->fault) fail(FCU_ERR_CUDA, "a bounded wait of the persistent loop gave up");
+    if (w->host_st->iter != iters) fail(FCU_ERR_CUDA, "the persistent loop stopped before its iteration count");
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = reps > 0 ? total / reps : 0.0;
+  *bytes = persistent_bytes_per_iter(m, mixed) * (double)iters;
 }
 
 // ---------------------------------------------------------------------------

@@ -627,6 +627,17 @@ class Matrix:
         _check(self.ctx, rc)
         return ms.value, by.value
 
+    def time_pcg(self, precision=FCU_MIXED, iterations=200, reps=3, flush_bytes=0):
+        """(ms per launch, algorithmic bytes per launch) of the persistent PCG
+        loop running exactly `iterations` iterations from x = 0 on b = 1, the
+        mean of `reps` launches each after an L2 flush. Overwrites the solver's
+        work vectors."""
+        ms, by = C.c_double(), C.c_double()
+        rc = _L().fcu_time_pcg(self.ctx.h, self.h, precision, int(iterations), reps, flush_bytes, C.byref(ms),
+                               C.byref(by))
+        _check(self.ctx, rc)
+        return ms.value, by.value
+
     def pcg(self, b, x=None, x0=None, tol=1e-8, max_iter=10000, precision=FCU_FP64, raise_on_error=True):
         """Jacobi-PCG (cg.rs:40-149). Returns (x, SolveInfo)."""
         x = np.empty(self.n) if x is None else x

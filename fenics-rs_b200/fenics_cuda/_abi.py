@@ -116,6 +116,7 @@ SIGNATURES = {
     "fcu_adjoint_gradient": (cint, [vp, vp, dbl, dbl, vp, vp, vp, vp]),
     "fcu_time_spmv": (cint, [vp, vp, cint, cint, C.POINTER(dbl), C.POINTER(dbl)]),
     "fcu_time_spmv_cold": (cint, [vp, vp, cint, cint, C.c_size_t, C.POINTER(dbl), C.POINTER(dbl)]),
+    "fcu_time_pcg": (cint, [vp, vp, cint, C.c_int64, cint, C.c_size_t, C.POINTER(dbl), C.POINTER(dbl)]),
     "fcu_buffer_alloc": (cint, [vp, C.c_size_t, C.POINTER(vp)]),
     "fcu_buffer_free": (cint, [vp, vp]),
     "fcu_buffer_copy": (cint, [vp, vp, vp, C.c_size_t]),

@@ -409,6 +409,18 @@ int fcu_time_spmv(fcu_ctx ctx, fcu_matrix m, int precision, int reps, double* ms
  * vector come from HBM as they do inside a solve whose operator exceeds L2. */
 int fcu_time_spmv_cold(fcu_ctx ctx, fcu_matrix m, int precision, int reps, size_t flush_bytes,
                        double* ms_per_launch, double* bytes_per_launch);
+/* Device time of one launch of the persistent PCG loop (the kernel fcu_pcg
+ * runs for mixed-precision solves of 3x3-block matrices with point-Jacobi
+ * preconditioning; FP64 solves take it when FCU_PERSISTENT=2) doing
+ * exactly `iterations` iterations from x = 0 on b = 1 (no stopping test, no
+ * residual replacement, no breakdown exit), after an L2 flush as in
+ * fcu_time_spmv_cold; the mean over `reps` launches, each from a fresh start,
+ * and the algorithmic bytes of one launch (per iteration: the matrix once;
+ * z, p_old read and Ap written by the product; x, r, D^-1, p_old, z, Ap read
+ * and x, r, p, z written by the update). FCU_ERR_UNSUPPORTED for other
+ * matrices. Overwrites the solver's work vectors. */
+int fcu_time_pcg(fcu_ctx ctx, fcu_matrix m, int precision, int64_t iterations, int reps, size_t flush_bytes,
+                 double* ms_per_launch, double* bytes_per_launch);
 
 #ifdef __cplusplus
 }
