@@ -865,7 +865,7 @@ def run_reference(args, cfg):
 
 
 PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5", "p2_cube40",
-                 "spmv_c2p", "spmv_c2", "p2_c3")
+                 "spmv_c2p", "spmv_c2", "p2_c3", "pcg_c2", "pcg_c2_small")
 
 
 def profile_case(name):
