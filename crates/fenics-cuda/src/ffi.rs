@@ -147,6 +147,13 @@ extern "C" {
     pub fn fcu_matrix_clone(ctx: fcu_ctx, src: fcu_matrix, out: *mut fcu_matrix) -> c_int;
     pub fn fcu_matrix_add_scaled(ctx: fcu_ctx, out: fcu_matrix, a: fcu_matrix, b: fcu_matrix, alpha: f64)
         -> c_int;
+    pub fn fcu_matrix_add_scaled_union(
+        ctx: fcu_ctx,
+        a: fcu_matrix,
+        b: fcu_matrix,
+        alpha: f64,
+        out: *mut fcu_matrix,
+    ) -> c_int;
     pub fn fcu_matrix_scale(ctx: fcu_ctx, m: fcu_matrix, s: f64) -> c_int;
     pub fn fcu_matrix_fold_dirichlet(
         ctx: fcu_ctx,

@@ -326,9 +326,66 @@ pub fn compute_element_stresses(mesh: &TetrahedronMesh, u: &[f64], mat: &Elastic
         .collect()
 }
 
+/// mass.rs:10 — same signature, GPU assembly (density 1).
+pub fn assemble_mass_2d(mesh: &TriangleMesh) -> SparseColMat<usize, f64> {
+    let _g = SESSION_LOCK.lock().unwrap();
+    let dm = device_mesh(&mesh.vertices, &mesh.cells);
+    let m = matrix(&space(&dm, ffi::FCU_SPACE_P1));
+    check(unsafe { ffi::fcu_assemble_mass(ctx().0, m.0, 1.0, std::ptr::null()) }).unwrap();
+    export(&m)
+}
+
+/// mass.rs:47 — same signature, GPU assembly (density 1).
+pub fn assemble_mass_3d(mesh: &TetrahedronMesh) -> SparseColMat<usize, f64> {
+    let _g = SESSION_LOCK.lock().unwrap();
+    let dm = device_mesh(&mesh.vertices, &mesh.cells);
+    let m = matrix(&space(&dm, ffi::FCU_SPACE_P1));
+    check(unsafe { ffi::fcu_assemble_mass(ctx().0, m.0, 1.0, std::ptr::null()) }).unwrap();
+    export(&m)
+}
+
+/// mass.rs:86 — same signature: the same-component entries of the vector
+/// P1 mass, exported as the reference builds them.
+pub fn assemble_elasticity_mass_3d(mesh: &TetrahedronMesh, density: f64) -> SparseColMat<usize, f64> {
+    let _g = SESSION_LOCK.lock().unwrap();
+    let dm = device_mesh(&mesh.vertices, &mesh.cells);
+    let m = matrix(&space(&dm, ffi::FCU_SPACE_P1_VEC3));
+    check(unsafe { ffi::fcu_assemble_mass(ctx().0, m.0, density, std::ptr::null()) }).unwrap();
+    export(&m)
+}
+
 // ---------------------------------------------------------------------------
 // Solvers (crates/fenics-solver)
 // ---------------------------------------------------------------------------
+
+/// transient.rs:72 — same signature: a + alpha * b on the union of the two
+/// patterns, built on the device.
+pub fn add_scaled_matrices(
+    a: &SparseColMat<usize, f64>,
+    b: &SparseColMat<usize, f64>,
+    alpha: f64,
+) -> SparseColMat<usize, f64> {
+    let _g = SESSION_LOCK.lock().unwrap();
+    let (ma, mb) = (wrap_csc(a), wrap_csc(b));
+    let mut h = std::ptr::null_mut();
+    check(unsafe { ffi::fcu_matrix_add_scaled_union(ctx().0, ma.0, mb.0, alpha, &mut h) })
+        .expect("Failed to build combined sparse matrix");
+    export(&Matrix(h))
+}
+
+/// eigen.rs:51 — same signature: constrained rows and columns folded on the
+/// device, a unit (or zero) diagonal on them, zero entries dropped.
+pub fn fold_dirichlet(mat: &SparseColMat<usize, f64>, fixed_dofs: &[usize], unit_diag: bool) -> SparseColMat<usize, f64> {
+    let _g = SESSION_LOCK.lock().unwrap();
+    let m = wrap_csc(mat);
+    let fixed: Vec<i64> = fixed_dofs.iter().map(|&d| d as i64).collect();
+    check(unsafe {
+        ffi::fcu_matrix_fold_dirichlet(ctx().0, m.0, fixed.len() as i64, fixed.as_ptr(), unit_diag as c_int)
+    })
+    .unwrap();
+    export(&m)
+}
+
 
 /// cg.rs:40 — same signature and Result semantics: Err carries the
 /// reference's strings ("CG failed to converge ...", "Breakdown in CG ...").

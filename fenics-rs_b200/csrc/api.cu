@@ -2,6 +2,8 @@
 // staging, handle lifetime, CSC import/export. Compute lives in the other .cu
 // files; every entry point converts FcuError into a status code.
 
+#include <climits>
+
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -896,33 +898,39 @@ int fcu_matrix_info(fcu_matrix m, int64_t* n, int64_t* nnz) {
   });
 }
 
+// Row indices and values of the exported CSC, on the device, for the column
+// pointers export_counts produced (either output may be null).
+static void export_fill(fcu_matrix m, const DBuf<i64>& cp, i64* rowidx_dev, double* vals_dev) {
+  fcu_ctx ctx = m->ctx;
+  const i64 n = m->n;
+  const unsigned char* dir = m->bc_applied ? m->dirichlet.p : nullptr;
+  if (m->wrapped_general) {
+    k_wexport_fill<<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
+        m->csc_colptr.p, m->csc_rowidx.p, m->csr_of.p, m->drop_zeros, dir, m->diag_count.p, m->val64.p, n, cp.p,
+        rowidx_dev, vals_dev);
+  } else {
+    build_transpose_positions(m->space);
+    if (m->bs == 3)
+      k_export_fill<3><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
+          m->row_ptr, m->col_idx, m->space->tpos.p, m->drop_zeros, m->comp_diag, m->diag_struct.p, dir,
+          m->diag_count.p, m->val64.p, m->nnodes, cp.p, rowidx_dev, vals_dev);
+    else
+      k_export_fill<1><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
+          m->row_ptr, m->col_idx, m->space->tpos.p, m->drop_zeros, false, m->diag_struct.p, dir, m->diag_count.p,
+          m->val64.p, m->nnodes, cp.p, rowidx_dev, vals_dev);
+  }
+  LAUNCH_CHECK(ctx);
+}
+
 int fcu_matrix_export_csc(fcu_ctx ctx, fcu_matrix m, int64_t* colptr, int64_t* rowidx, double* vals) {
   return guarded(ctx, [&] {
     if (!m) fail(FCU_ERR_BAD_ARG, "null matrix");
     const i64 n = m->n;
     DBuf<i64> cp;
     const i64 nnz = export_counts(m, cp);
-      DevOut<i64> R(rowidx, nnz);
+    DevOut<i64> R(rowidx, nnz);
     DevOut<double> V(vals, nnz);
-    const unsigned char* dir = m->bc_applied ? m->dirichlet.p : nullptr;
-    if (rowidx || vals) {
-      if (m->wrapped_general) {
-        k_wexport_fill<<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
-            m->csc_colptr.p, m->csc_rowidx.p, m->csr_of.p, m->drop_zeros, dir, m->diag_count.p, m->val64.p, n, cp.p,
-            R.p, V.p);
-      } else {
-        build_transpose_positions(m->space);
-        if (m->bs == 3)
-          k_export_fill<3><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
-              m->row_ptr, m->col_idx, m->space->tpos.p, m->drop_zeros, m->comp_diag, m->diag_struct.p, dir,
-              m->diag_count.p, m->val64.p, m->nnodes, cp.p, R.p, V.p);
-        else
-          k_export_fill<1><<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(
-              m->row_ptr, m->col_idx, m->space->tpos.p, m->drop_zeros, false, m->diag_struct.p, dir,
-              m->diag_count.p, m->val64.p, m->nnodes, cp.p, R.p, V.p);
-      }
-      LAUNCH_CHECK(ctx);
-    }
+    if (rowidx || vals) export_fill(m, cp, R.p, V.p);
     if (colptr) download(ctx, colptr, cp.p, (size_t)(n + 1));
     R.finish(ctx);
     V.finish(ctx);
@@ -993,6 +1001,88 @@ int fcu_matrix_add_scaled(fcu_ctx ctx, fcu_matrix out, fcu_matrix a, fcu_matrix 
     add_scaled_impl(out, a, b, alpha);
     out->has_values = true;
     sync(ctx);
+  });
+}
+
+// add_scaled_matrices on two CSC layouts (transient.rs:72-97): per column,
+// the union of the two sorted row lists. The triplet build sums a duplicate
+// in push order, so an entry held by both is a + (alpha * b), one held by b
+// alone is alpha * b, and explicit zeros stay. One thread per column.
+__global__ void k_union_count(const i64* __restrict__ acp, const i64* __restrict__ ari,
+                              const i64* __restrict__ bcp, const i64* __restrict__ bri, i64 n,
+                              i64* __restrict__ cnt) {
+  for (i64 j = blockIdx.x * (i64)blockDim.x + threadIdx.x; j < n; j += (i64)gridDim.x * blockDim.x) {
+    i64 p = acp[j], q = bcp[j], c = 0;
+    const i64 pe = acp[j + 1], qe = bcp[j + 1];
+    while (p < pe && q < qe) {
+      const i64 ra = ari[p], rb = bri[q];
+      p += ra <= rb;
+      q += rb <= ra;
+      ++c;
+    }
+    cnt[j] = c + (pe - p) + (qe - q);
+  }
+}
+
+__global__ void k_union_fill(const i64* __restrict__ acp, const i64* __restrict__ ari, const double* __restrict__ av,
+                             const i64* __restrict__ bcp, const i64* __restrict__ bri, const double* __restrict__ bv,
+                             double alpha, i64 n, const i64* __restrict__ ccp, i64* __restrict__ cri,
+                             double* __restrict__ cv) {
+  for (i64 j = blockIdx.x * (i64)blockDim.x + threadIdx.x; j < n; j += (i64)gridDim.x * blockDim.x) {
+    i64 p = acp[j], q = bcp[j], o = ccp[j];
+    const i64 pe = acp[j + 1], qe = bcp[j + 1];
+    while (p < pe || q < qe) {
+      const i64 ra = p < pe ? ari[p] : LLONG_MAX, rb = q < qe ? bri[q] : LLONG_MAX;
+      if (ra < rb) {
+        cri[o] = ra;
+        cv[o] = av[p++];
+      } else if (rb < ra) {
+        cri[o] = rb;
+        cv[o] = __dmul_rn(alpha, bv[q++]);
+      } else {
+        cri[o] = ra;
+        cv[o] = __dadd_rn(av[p++], __dmul_rn(alpha, bv[q++]));
+      }
+      ++o;
+    }
+  }
+}
+
+int fcu_matrix_add_scaled_union(fcu_ctx ctx, fcu_matrix a, fcu_matrix b, double alpha, fcu_matrix* out) {
+  if (!out) return FCU_ERR_BAD_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    if (!a || !b) fail(FCU_ERR_BAD_ARG, "null matrix");
+    if (!a->has_values || !b->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
+    if (a->n != b->n) fail(FCU_ERR_BAD_ARG, "add_scaled_matrices: operands of different order");
+    const i64 n = a->n;
+    DBuf<i64> acp, bcp, ari, bri, ccp, cri, cnt;
+    DBuf<double> av, bv, cv;
+    const i64 annz = export_counts(a, acp), bnnz = export_counts(b, bcp);
+    ari.alloc(std::max<i64>(annz, 1));
+    av.alloc(std::max<i64>(annz, 1));
+    bri.alloc(std::max<i64>(bnnz, 1));
+    bv.alloc(std::max<i64>(bnnz, 1));
+    export_fill(a, acp, ari.p, av.p);
+    export_fill(b, bcp, bri.p, bv.p);
+    cnt.alloc(n + 1);
+    CUDA_CHECK(cudaMemsetAsync(cnt.p + n, 0, sizeof(i64), ctx->stream));
+    k_union_count<<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(acp.p, ari.p, bcp.p, bri.p, n, cnt.p);
+    LAUNCH_CHECK(ctx);
+    ccp.alloc(n + 1);
+    size_t tb = 0;
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, ccp.p, (int)(n + 1), ctx->stream));
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(ctx->temp_bytes(tb), tb, cnt.p, ccp.p, (int)(n + 1), ctx->stream));
+    const i64 cnnz = read1(ctx, ccp.p + n);
+    cri.alloc(std::max<i64>(cnnz, 1));
+    cv.alloc(std::max<i64>(cnnz, 1));
+    k_union_fill<<<grid_for(n, 128, cap_blocks(ctx)), 128, 0, ctx->stream>>>(acp.p, ari.p, av.p, bcp.p, bri.p, bv.p,
+                                                                            alpha, n, ccp.p, cri.p, cv.p);
+    LAUNCH_CHECK(ctx);
+    fcu_matrix m = nullptr;
+    const int rc = fcu_matrix_from_csc(ctx, n, ccp.p, cri.p, cv.p, &m);
+    if (rc != FCU_OK) fail(rc, ctx->err);
+    *out = m;
   });
 }
 

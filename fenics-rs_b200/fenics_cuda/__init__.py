@@ -550,6 +550,14 @@ class Matrix:
         _check(self.ctx, _L().fcu_matrix_add_scaled(self.ctx.h, self.h, a.h, b.h, float(alpha)))
         return self
 
+    @classmethod
+    def add_scaled_union(cls, a: "Matrix", b: "Matrix", alpha) -> "Matrix":
+        """A new wrapped CSC matrix a + alpha * b on the union of the two
+        exported patterns (add_scaled_matrices, transient.rs:72-97)."""
+        h = C.c_void_p()
+        _check(a.ctx, _L().fcu_matrix_add_scaled_union(a.ctx.h, a.h, b.h, float(alpha), C.byref(h)))
+        return cls(a.ctx, None, h)
+
     def scale(self, s):
         _check(self.ctx, _L().fcu_matrix_scale(self.ctx.h, self.h, float(s)))
         return self
@@ -1232,14 +1240,25 @@ def _as_matrix(ctx, mat):
 
 
 def add_scaled_matrices(a, b, alpha, ctx: Context | None = None) -> CscMatrix:
-    """add_scaled_matrices (transient.rs:72-97): a + alpha * b. Both operands
-    must have the same pattern (FcuError FCU_ERR_UNSUPPORTED otherwise)."""
+    """add_scaled_matrices (transient.rs:72-97): a + alpha * b, on the union
+    of the operands' patterns. Two matrices of one space combine value by
+    value on the device; any other pair goes through the union build."""
     ctx = ctx or default_context()
     A, oa = _as_matrix(ctx, a)
     B, ob = _as_matrix(ctx, b)
     try:
-        out = A.clone()
-        out.set_add_scaled(A, B, alpha)
+        out = None
+        if A.space is not None and A.space is B.space:
+            out = A.clone()
+            try:
+                out.set_add_scaled(A, B, alpha)
+            except FcuError as e:
+                if e.code != _abi.FCU_ERR_UNSUPPORTED:
+                    raise
+                out.close()
+                out = None   # Dirichlet or folded state: the exported operands combine below
+        if out is None:
+            out = Matrix.add_scaled_union(A, B, alpha)
         res = out.export_csc()
         out.close()
     finally:

@@ -86,6 +86,7 @@ SIGNATURES = {
     "fcu_assemble_mass": (cint, [vp, vp, dbl, vp]),
     "fcu_matrix_clone": (cint, [vp, vp, C.POINTER(vp)]),
     "fcu_matrix_add_scaled": (cint, [vp, vp, vp, vp, dbl]),
+    "fcu_matrix_add_scaled_union": (cint, [vp, vp, vp, dbl, C.POINTER(vp)]),
     "fcu_matrix_scale": (cint, [vp, vp, dbl]),
     "fcu_matrix_fold_dirichlet": (cint, [vp, vp, i64, vp, cint]),
     "fcu_apply_dirichlet": (cint, [vp, vp, vp, i64, vp, vp]),

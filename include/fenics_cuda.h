@@ -167,6 +167,14 @@ int fcu_matrix_clone(fcu_ctx ctx, fcu_matrix src, fcu_matrix* out);
  * carry no eliminated Dirichlet dofs, else FCU_ERR_UNSUPPORTED; out may be
  * a or b. */
 int fcu_matrix_add_scaled(fcu_ctx ctx, fcu_matrix out, fcu_matrix a, fcu_matrix b, double alpha);
+/* add_scaled_matrices (transient.rs:72-97) on operands of any patterns: a new
+ * matrix *out holding a + alpha * b on the union of the two exported CSC
+ * patterns (an entry held by both is a + (alpha * b), one held by b alone
+ * alpha * b, explicit zeros kept), as the reference's triplet build gives.
+ * a and b must have the same order; either may carry Dirichlet or folded
+ * state (its exported matrix is the operand). *out is a wrapped CSC matrix:
+ * destroy it with fcu_matrix_destroy. */
+int fcu_matrix_add_scaled_union(fcu_ctx ctx, fcu_matrix a, fcu_matrix b, double alpha, fcu_matrix* out);
 /* Every value times s (the diffusivity scaling of heat_solver.rs:48-57). */
 int fcu_matrix_scale(fcu_ctx ctx, fcu_matrix m, double s);
 /* fold_dirichlet (eigen.rs:55-79), in place: entries on a fixed row or column

@@ -135,14 +135,85 @@ def test_add_scaled_scale_and_fold(fcu, ctx):
     B = fcu.CscMatrix(Mo.n, Mo.colptr, Mo.rowidx, 3.0 * Mo.vals)
     _same(fcu.add_scaled_matrices(A, B, -0.5, ctx), O.add_scaled_matrices(Mo, O.Csc(Mo.n, Mo.colptr, Mo.rowidx,
                                                                                    3.0 * Mo.vals), -0.5))
-    with pytest.raises(fcu.FcuError) as e:
-        fcu.add_scaled_matrices(A, fcu.CscMatrix(Ko.n, Ko.colptr, Ko.rowidx, Ko.vals), 1.0, ctx)
-    assert e.value.code == fcu._abi.FCU_ERR_UNSUPPORTED
+    # different layouts: the union pattern, as the triplet build gives it
+    _exact(fcu.add_scaled_matrices(A, fcu.CscMatrix(Ko.n, Ko.colptr, Ko.rowidx, Ko.vals), 1.0, ctx),
+           O.add_scaled_matrices(Mo, Ko, 1.0))
     with pytest.raises(fcu.FcuError):
         K.clone().fold_dirichlet(np.array([-1], np.int64), True)
     for x in (S, Ks, Kf, Mf, K, Mm):
         x.close()
     V.close()
+
+
+def _exact(A, B):
+    """Same pattern and identical values (a zero's sign aside)."""
+    assert A.n == B.n
+    assert np.array_equal(np.asarray(A.colptr), np.asarray(B.colptr))
+    assert np.array_equal(np.asarray(A.rowidx), np.asarray(B.rowidx))
+    assert np.array_equal(np.asarray(A.vals), np.asarray(B.vals))
+
+
+def _random_csc(n, density, seed, zeros=True):
+    """A faer-layout CSC with sorted rows, a full diagonal and, optionally,
+    explicit zeros among its entries."""
+    rng = np.random.default_rng(seed)
+    mask = rng.random((n, n)) < density
+    np.fill_diagonal(mask, True)
+    vals = rng.standard_normal((n, n))
+    if zeros:
+        vals[rng.random((n, n)) < 0.1] = 0.0
+    colptr = np.zeros(n + 1, np.int64)
+    rows, vs = [], []
+    for j in range(n):
+        r = np.nonzero(mask[:, j])[0]
+        rows.append(r)
+        vs.append(vals[r, j])
+        colptr[j + 1] = colptr[j] + len(r)
+    return O.Csc(n, colptr, np.concatenate(rows).astype(np.int64), np.concatenate(vs))
+
+
+def test_add_scaled_union_matches_oracle(fcu, ctx):
+    """add_scaled_matrices (transient.rs:72-97) on operands whose patterns
+    differ: the union build against the oracle's faer-style triplet build,
+    pattern and values bit for bit."""
+    # wrapped CSC operands with explicit zeros, empty columns on one side
+    n = 57
+    Ao, Bo = _random_csc(n, 0.08, 1), _random_csc(n, 0.05, 2)
+    A = fcu.CscMatrix(n, Ao.colptr, Ao.rowidx, Ao.vals)
+    B = fcu.CscMatrix(n, Bo.colptr, Bo.rowidx, Bo.vals)
+    for alpha in (1.0, -0.37, 0.0):
+        _exact(fcu.add_scaled_matrices(A, B, alpha, ctx), O.add_scaled_matrices(Ao, Bo, alpha))
+    # two spaces of one order: P1 stiffness on a mesh, P1 mass on the same
+    # vertices renumbered (another pattern)
+    m = O.unit_square(9, 7)
+    perm = np.random.default_rng(3).permutation(m.nv)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(m.nv)
+    m2 = O.Mesh(np.ascontiguousarray(m.coords[perm]), np.ascontiguousarray(inv[m.cells]).astype(m.cells.dtype))
+    V1 = fcu.FunctionSpace(ctx, fcu.Mesh(m.coords, m.cells), fcu.FCU_SPACE_P1)
+    V2 = fcu.FunctionSpace(ctx, fcu.Mesh(m2.coords, m2.cells), fcu.FCU_SPACE_P1)
+    K = fcu.Matrix(ctx, V1).assemble_stiffness(None)
+    Mm = fcu.Matrix(ctx, V2).assemble_mass(2.5)
+    Ko, Mo = K.export_csc(), Mm.export_csc()
+    _exact(fcu.add_scaled_matrices(K, Mm, 0.01, ctx), O.add_scaled_matrices(Ko, Mo, 0.01))
+    # one space, one operand with Dirichlet rows eliminated: its exported
+    # matrix is the operand
+    K2 = fcu.Matrix(ctx, V1).assemble_stiffness(None)
+    bd = V1.boundary_dofs().astype(np.int64)
+    rhs = np.ones(V1.ndofs)
+    K2.apply_dirichlet(rhs, bd, np.zeros(len(bd)))
+    K2o = K2.export_csc()
+    _exact(fcu.add_scaled_matrices(K, K2, -2.0, ctx), O.add_scaled_matrices(Ko, K2o, -2.0))
+    # the handle-level entry point; order mismatch refused
+    U = fcu.Matrix.add_scaled_union(K, Mm, 0.5)
+    _exact(U.export_csc(), O.add_scaled_matrices(Ko, Mo, 0.5))
+    with pytest.raises(fcu.FcuError) as e:
+        fcu.add_scaled_matrices(A, fcu.CscMatrix(1, np.array([0, 1]), np.array([0]), np.array([1.0])), 1.0, ctx)
+    assert e.value.code == fcu._abi.FCU_ERR_BAD_ARG
+    for x in (U, K, K2, Mm):
+        x.close()
+    V1.close()
+    V2.close()
 
 
 def test_transient_exponential_decay(fcu, ctx):
