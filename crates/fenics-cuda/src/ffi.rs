@@ -417,4 +417,5 @@ extern "C" {
         ms_per_launch: *mut f64,
         bytes_per_launch: *mut f64,
     ) -> c_int;
+    pub fn fcu_check_wait_limits(ctx: fcu_ctx, polls: u32, results: *mut c_int) -> c_int;
 }

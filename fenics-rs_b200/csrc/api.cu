@@ -32,6 +32,7 @@ void spmv_impl(fcu_matrix m, const double* x_dev, double* y_dev);
 void time_spmv_impl(fcu_matrix m, int precision, int reps, double* ms, double* bytes);
 void time_spmv_cold_impl(fcu_matrix m, int precision, int reps, size_t flush_bytes, double* ms, double* bytes);
 void time_pcg_impl(fcu_matrix m, int precision, i64 iters, int reps, size_t flush_bytes, double* ms, double* bytes);
+void check_wait_limits_impl(fcu_ctx ctx, unsigned limit, int* results_host);
 int batch_pcg_impl(fcu_matrix m, i64 nb, const i64* offsets_host, const double* b_dev, double* x_dev, double tol,
                    i64 max_iter, int precision, i64* iters_host, double* relres_host, int* status_host,
                    fcu_solve_info* info, const int* fixed_shape = nullptr);
@@ -1601,6 +1602,14 @@ int fcu_time_pcg(fcu_ctx ctx, fcu_matrix m, int precision, int64_t iterations, i
     if (!m->has_values) fail(FCU_ERR_BAD_ARG, "matrix has no values");
     if (precision != FCU_FP64 && precision != FCU_MIXED) fail(FCU_ERR_BAD_ARG, "unknown precision");
     time_pcg_impl(m, precision, iterations, reps, flush_bytes, ms_per_launch, bytes_per_launch);
+  });
+}
+
+int fcu_check_wait_limits(fcu_ctx ctx, uint32_t polls, int* results) {
+  return guarded(ctx, [&] {
+    check_ctx(ctx);
+    if (!results || polls < 1 || polls > (1u << 20)) fail(FCU_ERR_BAD_ARG, "bad arguments");
+    check_wait_limits_impl(ctx, polls, results);
   });
 }
 

@@ -476,8 +476,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
   return ok != 0;
 }
 // Bounded wait; false when the limit expired.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  for (unsigned i = 0; i < WAIT_LIMIT; ++i)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned limit = WAIT_LIMIT) {
+  for (unsigned i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -940,12 +940,13 @@ __device__ __forceinline__ void consumer_sync() {
 // CTA barrier), polls the arrival count with relaxed loads until `target`,
 // then an acquire fence; the CTA's consumer warps pass together. False when
 // the poll gave up.
-__device__ __forceinline__ bool grid_barrier(unsigned long long* bar, unsigned long long target, int ctid) {
+__device__ __forceinline__ bool grid_barrier(unsigned long long* bar, unsigned long long target, int ctid,
+                                             unsigned limit = BARRIER_LIMIT) {
   __shared__ int ok_s;
   if (ctid == 0) {
     asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(bar) : "memory");
     int ok = 0;
-    for (unsigned i = 0; i < BARRIER_LIMIT; ++i) {
+    for (unsigned i = 0; i < limit; ++i) {
       unsigned long long v;
       asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
       if (v >= target) {
@@ -2682,6 +2683,53 @@ double persistent_bytes_per_iter(fcu_matrix m, bool mixed) {
 // iterations (no stopping test, no residual replacement, no breakdown exit)
 // from x = 0 on b = 1, after a read sweep of `flush_bytes` that evicts L2;
 // the mean over `reps` launches, each from a fresh start.
+// Self-check of the bounded waits the persistent loop and the tiled SpMV
+// rely on, with `limit` polls each. One CTA of the tiled kernels' shape:
+// its consumer threads wait at a grid barrier whose count can never be
+// reached (target 2 with one CTA arriving) and then at the same target,
+// which their second arrival reaches; warp 0 waits on an mbarrier nothing arrives at and then
+// on one whose single arrival it makes. out = {first grid wait passed,
+// second grid wait passed, first mbarrier wait passed, second mbarrier wait
+// passed}; a correct build gives {0, 1, 0, 1}.
+__global__ void __launch_bounds__(SPMV_THREADS) k_wait_limits(unsigned long long* bar, unsigned limit,
+                                                              int* __restrict__ out) {
+  __shared__ unsigned long long mb[2];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&mb[0], 1);
+    mbar_init(&mb[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid >= 32) {
+    const int ctid = tid - 32;
+    const bool a = grid_barrier(bar, 2, ctid, limit);
+    const bool b = grid_barrier(bar, 2, ctid, limit);  // the count is now 2
+    if (ctid == 0) {
+      out[0] = a ? 1 : 0;
+      out[1] = b ? 1 : 0;
+    }
+  } else if (tid == 0) {
+    out[2] = mbar_wait(&mb[0], 0, limit) ? 1 : 0;
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&mb[1])) : "memory");
+    out[3] = mbar_wait(&mb[1], 0, limit) ? 1 : 0;
+  }
+}
+
+void check_wait_limits_impl(fcu_ctx ctx, unsigned limit, int* results_host) {
+  DBuf<unsigned long long> bar;
+  DBuf<int> out;
+  bar.alloc(1);
+  out.alloc(4);
+  CUDA_CHECK(cudaMemsetAsync(bar.p, 0, sizeof(unsigned long long), ctx->stream));
+  CUDA_CHECK(cudaMemsetAsync(out.p, 0xff, 4 * sizeof(int), ctx->stream));
+  k_wait_limits<<<1, SPMV_THREADS, 0, ctx->stream>>>(bar.p, limit, out.p);
+  LAUNCH_CHECK(ctx);
+  CUDA_CHECK(cudaMemcpyAsync(results_host, out.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  ctx->launches++;
+}
+
 void time_pcg_impl(fcu_matrix m, int precision, i64 iters, int reps, size_t flush_bytes, double* ms,
                    double* bytes) {
   if (!persistent_capable(m)) fail(FCU_ERR_UNSUPPORTED, "the persistent loop runs on 3x3-block point-Jacobi systems");

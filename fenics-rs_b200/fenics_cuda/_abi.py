@@ -118,6 +118,7 @@ SIGNATURES = {
     "fcu_time_spmv": (cint, [vp, vp, cint, cint, C.POINTER(dbl), C.POINTER(dbl)]),
     "fcu_time_spmv_cold": (cint, [vp, vp, cint, cint, C.c_size_t, C.POINTER(dbl), C.POINTER(dbl)]),
     "fcu_time_pcg": (cint, [vp, vp, cint, C.c_int64, cint, C.c_size_t, C.POINTER(dbl), C.POINTER(dbl)]),
+    "fcu_check_wait_limits": (cint, [vp, C.c_uint32, C.POINTER(cint)]),
     "fcu_buffer_alloc": (cint, [vp, C.c_size_t, C.POINTER(vp)]),
     "fcu_buffer_free": (cint, [vp, vp]),
     "fcu_buffer_copy": (cint, [vp, vp, vp, C.c_size_t]),

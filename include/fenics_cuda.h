@@ -429,6 +429,15 @@ int fcu_time_spmv_cold(fcu_ctx ctx, fcu_matrix m, int precision, int reps, size_
  * matrices. Overwrites the solver's work vectors. */
 int fcu_time_pcg(fcu_ctx ctx, fcu_matrix m, int precision, int64_t iterations, int reps, size_t flush_bytes,
                  double* ms_per_launch, double* bytes_per_launch);
+/* Self-check of the bounded waits (no reference counterpart): one CTA waits,
+ * `polls` polls each (1 .. 2^20), at a grid barrier of the persistent PCG
+ * loop whose arrival count can never be reached, then at one it reaches, and
+ * on a shared-memory mbarrier of the tiled SpMV ring that nothing arrives at,
+ * then on one it arrives at itself. results[4] = {1 if the unreachable grid
+ * wait passed, 1 if the reachable one passed, the same for the two mbarrier
+ * waits}: a correct build gives {0, 1, 0, 1}. A wait that gives up returns;
+ * nothing traps, and the context stays usable. */
+int fcu_check_wait_limits(fcu_ctx ctx, uint32_t polls, int* results);
 
 #ifdef __cplusplus
 }

@@ -149,3 +149,29 @@ def test_persistent_large_share_matches_graph(fcu, ctx, tmp_path):
         assert p_info[name][2] == 0
         assert _rel(p_x[name], g_x[name]) <= 1e-6
         assert abs(it - it_g) <= max(3, (0.01 if name == "fp64" else 0.15) * it_g)
+
+
+def test_bounded_waits_give_up_and_report(fcu, ctx):
+    """The waits the loop and the tiled SpMV rely on are bounded: a grid
+    barrier whose arrival count is never reached and an mbarrier nothing
+    arrives at each give up after their polls and say so, while the same
+    waits with their condition met pass; the context stays usable (a solve
+    follows). No wait is left unbounded and nothing traps."""
+    import ctypes as C
+    lib = fcu._abi.lib()
+    res = (C.c_int * 4)()
+    for polls in (64, 4096):
+        assert lib.fcu_check_wait_limits(ctx.h, polls, res) == 0, lib.fcu_last_error(ctx.h)
+        assert list(res) == [0, 1, 0, 1], (polls, list(res))
+    assert lib.fcu_check_wait_limits(ctx.h, 0, res) == fcu._abi.FCU_ERR_BAD_ARG
+    assert lib.fcu_check_wait_limits(ctx.h, (1 << 20) + 1, res) == fcu._abi.FCU_ERR_BAD_ARG
+    om = O.box_beam(4.0, 1.0, 1.0, 8, 2, 2)
+    V = fcu.FunctionSpace(ctx, fcu.Mesh(om.coords, om.cells), fcu.FCU_SPACE_P1_VEC3)
+    M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+    dofs = O.clamp_dofs(om)
+    b = V.body_force([0.0, 0.0, -7.8e4])
+    M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
+    x, info = M.pcg(b, tol=1e-8, max_iter=10000, precision=fcu.FCU_MIXED)
+    assert info.status == 0
+    M.close()
+    V.close()

@@ -34,6 +34,7 @@ C_TO_RUST = {
     "int64_t*": "*mut i64",
     "const uint32_t*": "*const u32",
     "uint32_t*": "*mut u32",
+    "uint32_t": "u32",
     "int*": "*mut c_int",
     "fcu_ctx": "fcu_ctx",
     "fcu_mesh": "fcu_mesh",
