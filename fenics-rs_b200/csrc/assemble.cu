@@ -657,8 +657,9 @@ __global__ void __launch_bounds__(256) k_elast_blocks(i64 nup, const int* __rest
 // out as the exact transpose of block (i, j): the assembled matrix, and its
 // FP32 copy, are exactly symmetric. The diagonal block comes from the
 // row-sum identity: every cell's gradients sum to zero, so
-// sum_j M_ij = 0 and M_ii = -sum_{j != i} M_ij (symmetrised), summed over the
-// row's lanes through shared memory; relative to the summed-per-cell
+// sum_j M_ij = 0 and M_ii = -sum_{j != i} M_ij; K is linear in M, so
+// K_ii = -sum_{j != i} K_ij (symmetrised), summed by nine lanes over the
+// blocks staged for the row's stores; relative to the summed-per-cell
 // diagonal this moves it by a few ulps of the row's largest block.
 // One 32-byte gradient record {g.x, g.y, g.z, s} with a single 256-bit load
 // (read-only path): one L1 request per record instead of two 16-byte ones.
@@ -685,11 +686,9 @@ __global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ r
   constexpr int RPW = 32 / LPR;
   constexpr int W = 8;
   __shared__ double out_all[W][32 * 9];
-  __shared__ double ms_all[W][32 * 9];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int sub = lane % LPR, seg = lane / LPR;
   double* out = out_all[wib];
-  double* ms = ms_all[wib];
   const i64 nwarps = (i64)gridDim.x * W;
   for (i64 r0 = ((i64)blockIdx.x * W + wib) * RPW; r0 < nrows; r0 += nwarps * RPW) {
     const i64 row = r0 + seg;
@@ -700,8 +699,7 @@ __global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ r
       L = row_ptr[row + 1] - rs;
       dl = diag_pos[row] - rs;
     }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) ms[9 * lane + k] = 0.0;
+    double t = 0.0;  // lanes sub < 9: entry sub of the row's sum of off-diagonal K blocks
     const int nch = __reduce_max_sync(FULL, (L + LPR - 1) / LPR);
     for (int ch = 0; ch < nch; ++ch) {
       const int q = ch * LPR + sub;
@@ -733,13 +731,14 @@ __global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ r
 #pragma unroll
         for (int a2 = 0; a2 < 3; ++a2)
 #pragma unroll
-          for (int b2 = 0; b2 < 3; ++b2) {
+          for (int b2 = 0; b2 < 3; ++b2)
             o[3 * a2 + b2] = lam * M[3 * a2 + b2] + mu * M[3 * b2 + a2] + (a2 == b2 ? tr : 0.0);
-            ms[9 * lane + 3 * a2 + b2] += M[3 * a2 + b2];
-          }
       }
       __syncwarp();
       const int n = L - ch * LPR < LPR ? L - ch * LPR : LPR;
+      if (sub < 9)
+        for (int l = 0; l < n; ++l)
+          if (ch * LPR + l != dl) t += out[9 * (seg * LPR + l) + sub];
       const i64 base = 9 * ((i64)rs + ch * LPR);
       for (int idx = sub; idx < 9 * n; idx += LPR) {
         const int blk = idx / 9;
@@ -750,19 +749,15 @@ __global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ r
       }
       __syncwarp();
     }
-    // diagonal block: M_ii = -sum_j M_ij, symmetrised
-    double t = 0.0;
-    if (sub < 9)
-      for (int l = 0; l < LPR; ++l) t += ms[9 * (seg * LPR + l) + sub];
+    // diagonal block: K_ii = -sum_{j != i} K_ij (K is linear in M and
+    // M_ii = -sum_{j != i} M_ij), symmetrised
     __syncwarp();
     if (sub < 9) out[9 * seg * LPR + sub] = t;
     __syncwarp();
     if (valid && sub < 9 && dl >= 0) {
-      const double* T = out + 9 * seg * LPR;
+      const double* S = out + 9 * seg * LPR;
       const int a2 = sub / 3, b2 = sub - 3 * (sub / 3);
-      const double d = -0.5 * (T[3 * a2 + b2] + T[3 * b2 + a2]);
-      const double tr = -(T[0] + T[4] + T[8]);
-      const double v = (lam + mu) * d + (a2 == b2 ? mu * tr : 0.0);
+      const double v = -0.5 * (S[3 * a2 + b2] + S[3 * b2 + a2]);
       v64[9 * ((i64)rs + dl) + sub] = v;
       v32[9 * ((i64)rs + dl) + sub] = (float)v;
     }
