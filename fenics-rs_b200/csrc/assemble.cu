@@ -677,7 +677,7 @@ __device__ __forceinline__ void elast_accumulate(double (&M)[9], double s, doubl
 }
 
 template <int LPR>
-__global__ void __launch_bounds__(256, 3) k_elast_rows(const int* __restrict__ row_ptr,
+__global__ void __launch_bounds__(256, 4) k_elast_rows(const int* __restrict__ row_ptr,
                                                        const int* __restrict__ diag_pos,
                                                        const int* __restrict__ sl_ptr,
                                                        const unsigned* __restrict__ sl_ent,
