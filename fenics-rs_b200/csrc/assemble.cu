@@ -901,6 +901,96 @@ void p2_mass_products(double out[100]) {
     }
 }
 
+// Vector-P1 mass, row form over the per-block cell lists of the elasticity
+// pattern (sl_ptr / sl_ent, ascending cell order). k_mass_scales computes
+// each cell's s_c = rho * |det J| / 6 (* coefficient) once, with the
+// arithmetic of k_assemble_mass; k_mass_rows_vec gives each off-diagonal
+// block one lane, which adds s_c F[a][b] (each product rounded) over the
+// block's cells in ascending order, exactly as k_assemble_mass sums that
+// entry, and the diagonal block's entry is summed over the row's
+// contributions by the row's lanes (a fixed butterfly). A block is m I_3;
+// the row's blocks are written with contiguous stores, the lane that holds
+// a block's m handing it to the lanes that store it. One 8-byte load per
+// (block, cell) instead of one geometry per contribution.
+__global__ void __launch_bounds__(256) k_mass_scales(const int* __restrict__ cn, const double* __restrict__ X,
+                                                     const double* __restrict__ coef, double rho, i64 nc,
+                                                     double* __restrict__ sc) {
+  for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
+    const int4 q = reinterpret_cast<const int4*>(cn)[c];
+    const int v[4] = {q.x, q.y, q.z, q.w};
+    const double meas = (1.0 / 6.0) * fabs(tet_geometry(X, v).det);
+    double s = __dmul_rn(rho, meas);
+    if (coef) s = __dmul_rn(s, coef[c]);
+    sc[c] = s;
+  }
+}
+
+template <int LPR>
+__global__ void __launch_bounds__(256) k_mass_rows_vec(const int* __restrict__ row_ptr,
+                                                       const int* __restrict__ diag_pos,
+                                                       const int* __restrict__ sl_ptr,
+                                                       const unsigned* __restrict__ sl_ent,
+                                                       const int* __restrict__ contrib_ptr,
+                                                       const int* __restrict__ contrib,
+                                                       const double* __restrict__ sc, const MassTable tab,
+                                                       i64 nrows, double* __restrict__ v64, float* __restrict__ v32) {
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % LPR, seg = lane / LPR;
+  const i64 nwarps = (i64)gridDim.x * (blockDim.x >> 5);
+  for (i64 r0 = ((i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * RPW; r0 < nrows; r0 += nwarps * RPW) {
+    const i64 row = r0 + seg;
+    const bool valid = row < nrows;
+    int rs = 0, L = 0, dl = -1, c0 = 0, c1 = 0;
+    if (valid) {
+      rs = row_ptr[row];
+      L = row_ptr[row + 1] - rs;
+      dl = diag_pos[row] - rs;
+      c0 = contrib_ptr[row];
+      c1 = contrib_ptr[row + 1];
+    }
+    // diagonal: sum of s_c F[a][a] over the row's contributions
+    double dsum = 0.0;
+    for (int k = c0 + sub; k < c1; k += LPR) {
+      const int cc = contrib[k];
+      dsum = __dadd_rn(dsum, __dmul_rn(sc[cc >> 4], tab.F[(cc & 15) * 5]));
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) dsum = __dadd_rn(dsum, __shfl_xor_sync(FULL, dsum, o));
+    const int nch = __reduce_max_sync(FULL, (L + LPR - 1) / LPR);
+    for (int ch = 0; ch < nch; ++ch) {
+      const int q = ch * LPR + sub;
+      double m = 0.0;
+      if (q < L) {
+        if (q == dl) {
+          m = dsum;
+        } else {
+          const int e1 = sl_ptr[rs + q + 1];
+          for (int e = sl_ptr[rs + q]; e < e1; ++e) {
+            const unsigned u = sl_ent[e];
+            m = __dadd_rn(m, __dmul_rn(sc[u >> 4], tab.F[((u >> 2) & 3u) * 4 + (u & 3u)]));
+          }
+        }
+      }
+      // the chunk's 9 * n values: value idx of the chunk is entry idx % 9 of block idx / 9
+      const int left = L - ch * LPR;
+      const int n = left < LPR ? left : LPR;
+      const i64 base = 9 * ((i64)rs + ch * LPR);
+#pragma unroll
+      for (int it = 0; it < 9; ++it) {
+        const int idx = sub + it * LPR;
+        const int blk = idx / 9;
+        const double mb = __shfl_sync(FULL, m, seg * LPR + (blk < LPR ? blk : LPR - 1));
+        if (idx < 9 * n) {
+          const double v = (idx - 9 * blk) % 4 == 0 ? mb : 0.0;
+          v64[base + idx] = v;
+          v32[base + idx] = (float)v;
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Dirichlet elimination (poisson.rs:222-263, elasticity.rs:188-227)
 // ---------------------------------------------------------------------------
@@ -1200,6 +1290,16 @@ void assemble_elasticity_impl(fcu_matrix m, double E, double nu, const double* c
   }
 }
 
+// FCU_MASS_ROWGATHER=1 keeps the row-gather mass kernel on vector P1 spaces
+// (for comparison).
+bool mass_row_gather() {
+  static const bool v = [] {
+    const char* e = getenv("FCU_MASS_ROWGATHER");
+    return e && atoi(e) != 0;
+  }();
+  return v;
+}
+
 void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev) {
   fcu_space s = m->space;
   fcu_ctx ctx = m->ctx;
@@ -1225,6 +1325,25 @@ void assemble_mass_impl(fcu_matrix m, double rho, const double* coef_dev) {
     k_assemble_mass<10, 3, 1><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                    s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
                                                                    tab, s->diag_pos.p, s->nnodes, m->val64.p, m->val32.p);
+  } else if (s->kind == FCU_SPACE_P1_VEC3 && s->sl_ptr.p && !mass_row_gather()) {
+    DBuf<double> scales;
+    scales.alloc(std::max<i64>(me->nc, 1));
+    if (me->nc) {
+      k_mass_scales<<<grid_for(me->nc, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(cn, X, coef_dev, rho, me->nc,
+                                                                                     scales.p);
+      LAUNCH_CHECK(ctx);
+    }
+    const int lpr = s->max_row <= 16 ? 16 : 32;
+    const i64 need = (s->nnodes + 8 * (32 / lpr) - 1) / (8 * (32 / lpr));
+    const int nbr = (int)std::max<i64>(1, std::min<i64>(need, (i64)ctx->num_sms * 8));
+    if (lpr == 16)
+      k_mass_rows_vec<16><<<nbr, 256, 0, ctx->stream>>>(s->row_ptr.p, s->diag_pos.p, s->sl_ptr.p, s->sl_ent.p,
+                                                         s->contrib_ptr.p, s->contrib.p, scales.p, tab, s->nnodes,
+                                                         m->val64.p, m->val32.p);
+    else
+      k_mass_rows_vec<32><<<nbr, 256, 0, ctx->stream>>>(s->row_ptr.p, s->diag_pos.p, s->sl_ptr.p, s->sl_ent.p,
+                                                         s->contrib_ptr.p, s->contrib.p, scales.p, tab, s->nnodes,
+                                                         m->val64.p, m->val32.p);
   } else if (s->kind == FCU_SPACE_P1_VEC3) {
     k_assemble_mass<4, 3, 3><<<nb, WARPS * 32, 0, ctx->stream>>>(s->row_ptr.p, s->contrib_ptr.p, s->contrib.p,
                                                                   s->slot_cnt.p, s->slot_ent.p, cn, X, coef_dev, rho,
