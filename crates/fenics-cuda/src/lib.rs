@@ -18,7 +18,7 @@ use faer::sparse::{SparseColMat, SymbolicSparseColMat};
 use fenics_assembly::{DirichletBC, ElasticMaterial, StressState, VectorDirichletBC};
 use fenics_mesh::{TetrahedronMesh, TriangleMesh};
 use std::ffi::CStr;
-use std::os::raw::c_int;
+use std::os::raw::{c_int, c_void};
 use std::sync::OnceLock;
 
 // ---------------------------------------------------------------------------
@@ -488,6 +488,335 @@ fn device_name(device: c_int) -> String {
         return format!("cuda:{device}");
     }
     unsafe { CStr::from_ptr(buf.as_ptr()).to_string_lossy().into_owned() }
+}
+
+// ---------------------------------------------------------------------------
+// Transient heat, vibration modes, 3x3 block CSR (crates/fenics-solver)
+// ---------------------------------------------------------------------------
+
+/// transient.rs:13 — the two schemes.
+#[derive(Clone, Copy, Debug, PartialEq)]
+pub enum TimeSteppingScheme {
+    BackwardEuler,
+    CrankNicolson,
+}
+
+/// transient.rs:21 — same fields; `step` runs on the device.
+pub struct TransientHeatSolver {
+    pub scheme: TimeSteppingScheme,
+    pub dt: f64,
+}
+
+fn same_layout(a: &SparseColMat<usize, f64>, b: &SparseColMat<usize, f64>) -> bool {
+    a.ncols() == b.ncols()
+        && a.symbolic().col_ptrs() == b.symbolic().col_ptrs()
+        && a.symbolic().row_indices() == b.symbolic().row_indices()
+}
+
+impl TransientHeatSolver {
+    pub fn new(scheme: TimeSteppingScheme, dt: f64) -> Self {
+        Self { scheme, dt }
+    }
+
+    /// transient.rs:32 — same signature. The left-hand system is solved by
+    /// FP64 Jacobi-PCG to 1e-12 from u_n, where the reference factorises it
+    /// densely. Operands of different patterns are first placed on their
+    /// union (each plus 0 times the other, which keeps its values).
+    pub fn step(
+        &self,
+        mass_mat: &SparseColMat<usize, f64>,
+        stiff_mat: &SparseColMat<usize, f64>,
+        u_n: &[f64],
+        f_n: &[f64],
+        f_next: &[f64],
+    ) -> Result<Vec<f64>, String> {
+        let _g = SESSION_LOCK.lock().unwrap();
+        let (mut m, mut k) = (wrap_csc(mass_mat), wrap_csc(stiff_mat));
+        if !same_layout(mass_mat, stiff_mat) {
+            let (mut mu, mut ku) = (std::ptr::null_mut(), std::ptr::null_mut());
+            check(unsafe { ffi::fcu_matrix_add_scaled_union(ctx().0, m.0, k.0, 0.0, &mut mu) })?;
+            check(unsafe { ffi::fcu_matrix_add_scaled_union(ctx().0, k.0, m.0, 0.0, &mut ku) })?;
+            m = Matrix(mu);
+            k = Matrix(ku);
+        }
+        let scheme = match self.scheme {
+            TimeSteppingScheme::BackwardEuler => ffi::FCU_BACKWARD_EULER,
+            TimeSteppingScheme::CrankNicolson => ffi::FCU_CRANK_NICOLSON,
+        };
+        let mut ts = std::ptr::null_mut();
+        check(unsafe { ffi::fcu_transient_create(ctx().0, m.0, k.0, scheme, self.dt, &mut ts) })?;
+        let mut u = vec![0.0; u_n.len()];
+        let mut info = ffi::fcu_solve_info::default();
+        let rc = unsafe {
+            ffi::fcu_transient_step(
+                ctx().0,
+                ts,
+                u_n.as_ptr(),
+                f_n.as_ptr(),
+                f_next.as_ptr(),
+                u.as_mut_ptr(),
+                1e-12,
+                (10 * u_n.len()).max(1000) as i64,
+                ffi::FCU_FP64,
+                &mut info,
+            )
+        };
+        unsafe { ffi::fcu_transient_destroy(ts) };
+        check(rc)?;
+        Ok(u)
+    }
+}
+
+/// eigen.rs:10 — same fields.
+#[derive(Clone, Debug)]
+pub struct VibrationMode {
+    pub frequency_hz: f64,
+    pub omega_rad_s: f64,
+    pub eigenvalue: f64,
+    pub mode_shape: Vec<f64>,
+}
+
+type InnerFn<'a> = &'a dyn Fn(&[f64], &[f64]) -> Result<Vec<f64>, String>;
+
+struct InnerCall<'a> {
+    f: InnerFn<'a>,
+    err: Option<String>,
+}
+
+/// The C callback behind `inner`: b and x0 arrive in device memory; they are
+/// copied to the host, the closure runs, and its solution is copied back.
+unsafe extern "C" fn inner_trampoline(user: *mut c_void, n: i64, b: *const f64, x0: *const f64, x: *mut f64) -> c_int {
+    let call = &mut *(user as *mut InnerCall);
+    let n = n as usize;
+    let (mut hb, mut hx0) = (vec![0.0f64; n], vec![0.0f64; n]);
+    let bytes = 8 * n;
+    if ffi::fcu_buffer_copy(ctx().0, hb.as_mut_ptr() as *mut c_void, b as *const c_void, bytes) != ffi::FCU_OK
+        || ffi::fcu_buffer_copy(ctx().0, hx0.as_mut_ptr() as *mut c_void, x0 as *const c_void, bytes) != ffi::FCU_OK
+    {
+        call.err = Some("inner solve: device copy failed".to_string());
+        return ffi::FCU_ERR_CUDA;
+    }
+    match (call.f)(&hb, &hx0) {
+        Ok(v) if v.len() == n => {
+            ffi::fcu_buffer_copy(ctx().0, x as *mut c_void, v.as_ptr() as *const c_void, bytes)
+        }
+        Ok(_) => {
+            call.err = Some("inner solve returned a vector of the wrong length".to_string());
+            ffi::FCU_ERR_BAD_ARG
+        }
+        Err(e) => {
+            call.err = Some(e);
+            ffi::FCU_ERR_NO_CONVERGENCE
+        }
+    }
+}
+
+fn vibration_modes(
+    k: &SparseColMat<usize, f64>,
+    m: &SparseColMat<usize, f64>,
+    fixed_dofs: &[usize],
+    num_modes: usize,
+    max_power_iters: usize,
+    tol: f64,
+    inner: Option<InnerFn>,
+) -> Result<Vec<VibrationMode>, String> {
+    let _g = SESSION_LOCK.lock().unwrap();
+    let (mk, mm) = (wrap_csc(k), wrap_csc(m));
+    let n = k.nrows();
+    let fixed: Vec<i64> = fixed_dofs.iter().map(|&d| d as i64).collect();
+    let mut eig = vec![0.0; num_modes];
+    let mut shapes = vec![0.0; num_modes * n];
+    let mut info = ffi::fcu_solve_info::default();
+    let mut call = inner.map(|f| InnerCall { f, err: None });
+    let (cb, user): (ffi::fcu_inner_solve, *mut c_void) = match call.as_mut() {
+        Some(c) => (Some(inner_trampoline), c as *mut InnerCall as *mut c_void),
+        None => (None, std::ptr::null_mut()),
+    };
+    let rc = unsafe {
+        ffi::fcu_vibration_modes(
+            ctx().0,
+            mk.0,
+            mm.0,
+            fixed.len() as i64,
+            fixed.as_ptr(),
+            num_modes as i64,
+            max_power_iters as i64,
+            tol,
+            1e-9,
+            1000,
+            ffi::FCU_FP64,
+            cb,
+            user,
+            eig.as_mut_ptr(),
+            shapes.as_mut_ptr(),
+            std::ptr::null_mut(),
+            &mut info,
+        )
+    };
+    if rc != ffi::FCU_OK {
+        if let Some(e) = call.and_then(|c| c.err) {
+            return Err(e);
+        }
+        check(rc)?;
+    }
+    Ok((0..num_modes)
+        .map(|i| {
+            let omega = eig[i].sqrt();
+            VibrationMode {
+                frequency_hz: omega / (2.0 * std::f64::consts::PI),
+                omega_rad_s: omega,
+                eigenvalue: eig[i],
+                mode_shape: shapes[i * n..(i + 1) * n].to_vec(),
+            }
+        })
+        .collect())
+}
+
+/// eigen.rs:282 — same signature: inverse power iteration on the device,
+/// inner solve FP64 Jacobi-PCG at 1e-9 (the reference's default).
+pub fn solve_vibration_modes(
+    k: &SparseColMat<usize, f64>,
+    m: &SparseColMat<usize, f64>,
+    fixed_dofs: &[usize],
+    num_modes: usize,
+    max_power_iters: usize,
+    tol: f64,
+) -> Result<Vec<VibrationMode>, String> {
+    vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, None)
+}
+
+/// eigen.rs:94 — same signature: the caller's inner solve (K x = b from x0)
+/// is called for every power iteration, on host vectors.
+pub fn solve_vibration_modes_with_inner(
+    k: &SparseColMat<usize, f64>,
+    m: &SparseColMat<usize, f64>,
+    fixed_dofs: &[usize],
+    num_modes: usize,
+    max_power_iters: usize,
+    tol: f64,
+    inner: &dyn Fn(&[f64], &[f64]) -> Result<Vec<f64>, String>,
+) -> Result<Vec<VibrationMode>, String> {
+    vibration_modes(k, m, fixed_dofs, num_modes, max_power_iters, tol, Some(inner))
+}
+
+/// gpu.rs:434 — a resident 3x3 block CSR matrix (its inverse diagonal blocks
+/// optional).
+pub struct GpuBsr3Context {
+    m: Matrix,
+    nnz_blocks: usize,
+    device_name: String,
+}
+
+unsafe impl Send for GpuBsr3Context {}
+
+impl GpuBsr3Context {
+    /// gpu.rs:453 — same signature (an empty dinv_flat: none).
+    pub fn new(
+        n_nodes: usize,
+        row_ptr: &[u32],
+        cols: &[u32],
+        vals_flat: &[f64],
+        dinv_flat: &[f64],
+        _device_index: Option<usize>,
+    ) -> Result<Self, String> {
+        let _g = SESSION_LOCK.lock().unwrap();
+        let mut h = std::ptr::null_mut();
+        check(unsafe {
+            ffi::fcu_bsr3_create(
+                ctx().0,
+                n_nodes as i64,
+                row_ptr.as_ptr(),
+                cols.as_ptr(),
+                vals_flat.as_ptr(),
+                if dinv_flat.is_empty() { std::ptr::null() } else { dinv_flat.as_ptr() },
+                &mut h,
+            )
+        })?;
+        Ok(Self { m: Matrix(h), nnz_blocks: cols.len(), device_name: device_name(0) })
+    }
+
+    pub fn device_name(&self) -> &str {
+        &self.device_name
+    }
+
+    pub fn nnz_blocks(&self) -> usize {
+        self.nnz_blocks
+    }
+
+    /// gpu.rs:505 — y = A x.
+    pub fn spmv(&self, x: &[f64], y: &mut [f64]) -> Result<(), String> {
+        let _g = SESSION_LOCK.lock().unwrap();
+        check(unsafe { ffi::fcu_spmv(ctx().0, self.m.0, x.as_ptr(), y.as_mut_ptr()) })
+    }
+
+    /// gpu.rs:547 — damped block-Jacobi sweeps.
+    pub fn jacobi_smooth(
+        &self,
+        r: &[f64],
+        z: &mut [f64],
+        sweeps: usize,
+        omega: f64,
+        zero_initial_z: bool,
+    ) -> Result<(), String> {
+        let _g = SESSION_LOCK.lock().unwrap();
+        check(unsafe {
+            ffi::fcu_bsr3_jacobi_smooth(
+                ctx().0,
+                self.m.0,
+                r.as_ptr(),
+                z.as_mut_ptr(),
+                sweeps as i64,
+                omega,
+                zero_initial_z as c_int,
+            )
+        })
+    }
+}
+
+/// gpu.rs:775 — same signature: block-Jacobi PCG in FP64.
+#[allow(clippy::too_many_arguments)]
+pub fn solve_bsr3_pcg_gpu(
+    n_nodes: usize,
+    row_ptr: &[u32],
+    cols: &[u32],
+    vals_flat: &[f64],
+    dinv_flat: &[f64],
+    b: &[f64],
+    x0: Option<&[f64]>,
+    rtol: f64,
+    max_iter: usize,
+    _device_index: Option<usize>,
+) -> Result<GpuSolveResult, String> {
+    let _g = SESSION_LOCK.lock().unwrap();
+    let mut x = vec![0.0; b.len()];
+    let mut info = ffi::fcu_solve_info::default();
+    let t0 = std::time::Instant::now();
+    check(unsafe {
+        ffi::fcu_solve_bsr3_pcg(
+            ctx().0,
+            n_nodes as i64,
+            row_ptr.as_ptr(),
+            cols.as_ptr(),
+            vals_flat.as_ptr(),
+            if dinv_flat.is_empty() { std::ptr::null() } else { dinv_flat.as_ptr() },
+            b.as_ptr(),
+            x0.map_or(std::ptr::null(), |v| v.as_ptr()),
+            rtol,
+            max_iter as i64,
+            x.as_mut_ptr(),
+            &mut info,
+        )
+    })?;
+    Ok(GpuSolveResult {
+        solution: x,
+        iterations: info.iterations as usize,
+        final_residual: info.rel_residual,
+        wall_ms: t0.elapsed().as_secs_f64() * 1e3,
+        kernel_ms: info.kernel_ms,
+        gflops: 0.0,
+        effective_bw_gbps: info.effective_bw_gbps,
+        devices_used: vec![device_name(0)],
+    })
 }
 
 // ---------------------------------------------------------------------------
