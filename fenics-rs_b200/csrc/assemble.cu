@@ -1090,9 +1090,8 @@ __global__ void k_adjoint_grad(const double* __restrict__ X, const int* __restri
                                const double* __restrict__ la, double* __restrict__ grad) {
   for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c < nc; c += (i64)gridDim.x * blockDim.x) {
     if (!valid[c]) { grad[c] = 0.0; continue; }
-    int v[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) v[i] = cells[4 * c + i];
+    const int4 q = __ldg(reinterpret_cast<const int4*>(cells) + c);
+    const int v[4] = {q.x, q.y, q.z, q.w};
     Geo3 g = tet_geometry(X, v);
     double gr[4][3];
 #pragma unroll
