@@ -477,9 +477,8 @@ __global__ void k_element_stresses(const double* __restrict__ X, const int* __re
     double s[3][3] = {{0.0}}, e[3][3] = {{0.0}};
     double v = 0.0, t = 0.0;
     if (valid[c]) {
-      int vv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) vv[i] = cells[4 * c + i];
+      const int4 q = __ldg(reinterpret_cast<const int4*>(cells) + c);
+      const int vv[4] = {q.x, q.y, q.z, q.w};
       const Geo3 g3 = tet_geometry(X, vv);
       // P1 gradients: g_0 = J^-T (-1,-1,-1), g_k = J^-T e_{k-1}
       double gr[4][3];
