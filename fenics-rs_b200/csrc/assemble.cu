@@ -951,9 +951,12 @@ __global__ void __launch_bounds__(256) k_mass_rows_vec(const int* __restrict__ r
     }
     // diagonal: sum of s_c F[a][a] over the row's contributions
     double dsum = 0.0;
-    for (int k = c0 + sub; k < c1; k += LPR) {
-      const int cc = contrib[k];
-      dsum = __dadd_rn(dsum, __dmul_rn(sc[cc >> 4], tab.F[(cc & 15) * 5]));
+    for (int k0 = c0 + sub; k0 < c1; k0 += 2 * LPR) {
+      const int k1 = k0 + LPR;
+      const int cc0 = contrib[k0], cc1 = k1 < c1 ? contrib[k1] : 0;
+      const double f0 = sc[cc0 >> 4], f1 = k1 < c1 ? sc[cc1 >> 4] : 0.0;
+      dsum = __dadd_rn(dsum, __dmul_rn(f0, tab.F[(cc0 & 15) * 5]));
+      if (k1 < c1) dsum = __dadd_rn(dsum, __dmul_rn(f1, tab.F[(cc1 & 15) * 5]));
     }
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) dsum = __dadd_rn(dsum, __shfl_xor_sync(FULL, dsum, o));
@@ -965,10 +968,18 @@ __global__ void __launch_bounds__(256) k_mass_rows_vec(const int* __restrict__ r
         if (q == dl) {
           m = dsum;
         } else {
+          // four list entries and their scales in flight at a time, added in list order
           const int e1 = sl_ptr[rs + q + 1];
-          for (int e = sl_ptr[rs + q]; e < e1; ++e) {
-            const unsigned u = sl_ent[e];
-            m = __dadd_rn(m, __dmul_rn(sc[u >> 4], tab.F[((u >> 2) & 3u) * 4 + (u & 3u)]));
+          for (int e0 = sl_ptr[rs + q]; e0 < e1; e0 += 4) {
+            unsigned u[4];
+            double f[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) u[j] = e0 + j < e1 ? sl_ent[e0 + j] : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) f[j] = e0 + j < e1 ? sc[u[j] >> 4] : 0.0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (e0 + j < e1) m = __dadd_rn(m, __dmul_rn(f[j], tab.F[((u[j] >> 2) & 3u) * 4 + (u[j] & 3u)]));
           }
         }
       }
