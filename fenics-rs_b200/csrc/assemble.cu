@@ -709,8 +709,12 @@ __global__ void __launch_bounds__(256, 4) k_elast_rows(const int* __restrict__ r
         for (int k = 0; k < 9; ++k) M[k] = 0.0;
         int e = sl_ptr[rs + q];
         const int e1 = sl_ptr[rs + q + 1];
+        // the next pair's list entries are fetched while this pair is summed
+        unsigned n0 = e < e1 ? sl_ent[e] : 0u, n1 = e + 1 < e1 ? sl_ent[e + 1] : 0u;
         for (; e + 1 < e1; e += 2) {
-          const unsigned u0 = sl_ent[e], u1 = sl_ent[e + 1];
+          const unsigned u0 = n0, u1 = n1;
+          n0 = e + 2 < e1 ? sl_ent[e + 2] : 0u;
+          n1 = e + 3 < e1 ? sl_ent[e + 3] : 0u;
           double2 a01, a2s, b01, b2s, c01, c2s, d01, d2s;
           ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * ((u0 >> 2) & 3u), a01, a2s);
           ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * (u0 & 3u), b01, b2s);
@@ -720,7 +724,7 @@ __global__ void __launch_bounds__(256, 4) k_elast_rows(const int* __restrict__ r
           elast_accumulate(M, c2s.y, c01, c2s, d01, d2s);
         }
         if (e < e1) {
-          const unsigned u0 = sl_ent[e];
+          const unsigned u0 = n0;
           double2 a01, a2s, b01, b2s;
           ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * ((u0 >> 2) & 3u), a01, a2s);
           ld_rec4(rec + 16 * (i64)(u0 >> 4) + 4 * (u0 & 3u), b01, b2s);
