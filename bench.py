@@ -865,7 +865,7 @@ def run_reference(args, cfg):
 
 
 PROFILE_CASES = ("elasticity_c2", "mass_c2", "block_update_c2", "transient_1024", "batch_c5", "p2_cube40",
-                 "spmv_c2p", "spmv_c2", "p2_c3", "pcg_c2", "pcg_c2_small")
+                 "spmv_c2p", "spmv_c2", "p2_c3", "pcg_c2", "pcg_c2_small", "solve_c2_mixed", "solve_c2_fp64")
 
 
 def profile_case(name):
@@ -894,9 +894,13 @@ def profile_case(name):
                        (the launch the bench's roofline times; shape tuning
                        off)
       pcg_c2_small     the same loop on the 32x8x8 beam (24k dofs), 20
-                       iterations, for the full-section capture"""
+                       iterations, for the full-section capture
+      solve_c2_mixed   one complete mixed PCG solve of the C2 system to 1e-8
+                       (assembly, load and Dirichlet before it; shape tuning
+                       off), for the launch list of a solve
+      solve_c2_fp64    the FP64 PCG of the C2 system, 100 iterations"""
     import torch
-    if name in ("spmv_c2p", "spmv_c2", "pcg_c2", "pcg_c2_small"):
+    if name in ("spmv_c2p", "spmv_c2", "pcg_c2", "pcg_c2_small", "solve_c2_mixed", "solve_c2_fp64"):
         os.environ["FCU_TUNE"] = "0"   # no shape-tuning launches before the captured ones
     import fenics_cuda as fcu
     ctx = fcu.Context(0)
@@ -910,6 +914,20 @@ def profile_case(name):
         b = V.body_force([0.0, 0.0, -7.8e4])
         M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
         M.time_spmv(fcu.FCU_MIXED, reps=3, cold=True)
+        ctx.synchronize()
+        M.close(); V.close()
+    elif name in ("solve_c2_mixed", "solve_c2_fp64"):
+        mesh = fcu.box_beam(4.0, 1.0, 1.0, 128, 32, 32)
+        V = fcu.FunctionSpace(ctx, mesh, fcu.FCU_SPACE_P1_VEC3)
+        M = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+        cv = np.nonzero(mesh.coords[:, 0] < 1e-6)[0]
+        dofs = (3 * cv[:, None] + np.arange(3)).ravel().astype(np.int64)
+        b = V.body_force([0.0, 0.0, -7.8e4])
+        M.apply_dirichlet(b, dofs, np.zeros(len(dofs)))
+        if name == "solve_c2_mixed":
+            M.pcg(b, tol=1e-8, max_iter=100000, precision=fcu.FCU_MIXED)
+        else:
+            M.pcg(b, tol=1e-30, max_iter=100, precision=fcu.FCU_FP64, raise_on_error=False)
         ctx.synchronize()
         M.close(); V.close()
     elif name in ("pcg_c2", "pcg_c2_small"):
