@@ -164,8 +164,8 @@ int fcu_matrix_clone(fcu_ctx ctx, fcu_matrix src, fcu_matrix* out);
 /* add_scaled_matrices (transient.rs:72-97): out = a + alpha * b entry by
  * entry (each entry a + (alpha * b), as the triplet sum rounds it). a, b and
  * out share one pattern (one space, or identical wrapped CSC layouts) and
- * carry no eliminated Dirichlet dofs, else FCU_ERR_UNSUPPORTED; out may be
- * a or b. */
+ * carry no eliminated Dirichlet dofs, else FCU_ERR_UNSUPPORTED
+ * (fcu_matrix_add_scaled_union combines any two); out may be a or b. */
 int fcu_matrix_add_scaled(fcu_ctx ctx, fcu_matrix out, fcu_matrix a, fcu_matrix b, double alpha);
 /* add_scaled_matrices (transient.rs:72-97) on operands of any patterns: a new
  * matrix *out holding a + alpha * b on the union of the two exported CSC
