@@ -86,3 +86,16 @@ def test_package_imports_without_torch():
             "print('ok')\n") % os.path.join(ROOT, "fenics-rs_b200")
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stderr
+
+
+def test_profile_summaries_give_traffic():
+    """Every profile summary bench.py reads a roofline's DRAM traffic from
+    exists and states it per launch."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for name in ("spmv_bsr3_fp32_elasticity_c2.txt", "spmv_bsr3_fp64_elasticity_c2.txt",
+                 "pcg_persistent_fp32_elasticity_c2.txt", "spmv_bsr3_fp32_elasticity_c2p.txt"):
+        t = bench._profile_traffic(name)
+        assert t is not None and t > 0, name

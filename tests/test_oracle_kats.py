@@ -375,3 +375,45 @@ def test_adjoint_compliance_identity_small():
         tm[c] -= h
         fd = (J(tp)[0] - J(tm)[0]) / (2 * h)
         assert abs(fd - g[c]) <= 1e-6 * abs(g[c]) + 1e-15 * abs(j0) / h
+
+
+def test_add_scaled_matrices_union_semantics():
+    """add_scaled_matrices (transient.rs:72-97) on operands of different
+    patterns, as restated by the oracle: the union pattern with rows sorted
+    per column, explicit zeros of either operand kept, an entry held by both
+    a + (alpha * b) and one held by b alone alpha * b (checked against a
+    dense restatement; scipy's sum would drop the explicit zeros)."""
+    rng = np.random.default_rng(11)
+    n = 23
+
+    def rand_csc(density, seed):
+        r = np.random.default_rng(seed)
+        mask = r.random((n, n)) < density
+        vals = r.standard_normal((n, n))
+        vals[r.random((n, n)) < 0.15] = 0.0
+        cp = np.zeros(n + 1, np.int64)
+        rows, vs = [], []
+        for j in range(n):
+            rr = np.nonzero(mask[:, j])[0]
+            rows.append(rr)
+            vs.append(vals[rr, j])
+            cp[j + 1] = cp[j] + len(rr)
+        return O.Csc(n, cp, np.concatenate(rows).astype(np.int64), np.concatenate(vs)), mask, vals
+
+    A, ma, va = rand_csc(0.2, 1)
+    B, mb, vb = rand_csc(0.1, 2)
+    alpha = float(rng.uniform(-2, 2))
+    C = O.add_scaled_matrices(A, B, alpha)
+    union = ma | mb
+    assert np.array_equal(np.diff(C.colptr), union.sum(axis=0))
+    for j in range(n):
+        rows = np.asarray(C.rowidx[C.colptr[j]:C.colptr[j + 1]])
+        assert np.array_equal(rows, np.nonzero(union[:, j])[0])
+        for k, i in enumerate(rows):
+            v = C.vals[C.colptr[j] + k]
+            if ma[i, j] and mb[i, j]:
+                assert v == va[i, j] + alpha * vb[i, j]
+            elif ma[i, j]:
+                assert v == va[i, j]
+            else:
+                assert v == alpha * vb[i, j]
