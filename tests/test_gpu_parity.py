@@ -93,6 +93,38 @@ def test_elasticity_stiffness(fcu, ctx, dims):
     _assert_csc_equal(A, O.assemble_elasticity_3d(om, 210e9, 0.3))
 
 
+def _star_mesh():
+    """Tetrahedra joining the centre of the unit cube to each boundary
+    triangle of its 3x3x3 Kuhn subdivision: the centre's row couples to all
+    56 boundary vertices (57 blocks), so the row kernels take 32 lanes per
+    row and two chunks, which the box meshes (15 blocks per row at most)
+    never reach."""
+    box = O.unit_cube(3, 3, 3)
+    tri, _, _ = O.boundary_facets_3d(box)
+    used = np.unique(tri)
+    remap = np.full(box.nv, -1, np.int64)
+    remap[used] = np.arange(len(used))
+    coords = np.vstack([box.coords[used], [[0.5, 0.5, 0.5]]])
+    centre = len(used)
+    cells = np.column_stack([np.full(len(tri), centre), remap[tri]]).astype(box.cells.dtype)
+    return O.Mesh(np.ascontiguousarray(coords), np.ascontiguousarray(cells))
+
+
+def test_long_rows_star_mesh(fcu, ctx):
+    om = _star_mesh()
+    fm = _fmesh(fcu, om)
+    V = fcu.FunctionSpace(ctx, fm, fcu.FCU_SPACE_P1_VEC3)
+    K = fcu.Matrix(ctx, V).assemble_elasticity(210e9, 0.3)
+    _assert_csc_equal(K.export_csc(), O.assemble_elasticity_3d(om, 210e9, 0.3))
+    Mm = fcu.Matrix(ctx, V).assemble_mass(7850.0)
+    _assert_csc_equal(Mm.export_csc(), O.assemble_elasticity_mass_3d(om, 7850.0))
+    kappa = np.random.default_rng(8).uniform(0.5, 2.0, om.nc)
+    _assert_csc_equal(fcu.assemble_stiffness_3d(fm, ctx, kappa=kappa), O.assemble_stiffness_3d(om, kappa))
+    for x in (K, Mm):
+        x.close()
+    V.close()
+
+
 def test_elasticity_stiffness_per_cell_modulus_perturbed(fcu, ctx):
     om = _perturbed(O.box_beam, 3.0, 1.0, 1.0, 6, 3, 3, seed=5)
     th = np.random.default_rng(6).uniform(0.01, 1.0, om.nc)
