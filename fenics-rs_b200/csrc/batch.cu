@@ -6,18 +6,21 @@
 // the library's pattern, assembly, load-vector and Dirichlet kernels build
 // the whole batch in one pass each, and block i is rows [off[i], off[i+1]).
 //
-// One persistent launch solves the batch. Each CTA takes the next instance
-// from a queue ordered by estimated cost (largest first) and runs that
-// instance's whole PCG alone: every reduction is CTA-local (shared memory,
-// fixed order), so instances converge, stop and report independently and no
-// grid-wide synchronisation exists. The arithmetic per instance is that of
-// the library's single-system PCG (cg.rs:40-149 for FP64; for mixed, FP32
-// difference-form operator with FP64 r, x and dots and FP64 residual
+// One persistent launch solves the batch. Each thread-block cluster (1 to 8
+// CTAs) takes the next instance from a queue ordered by estimated cost
+// (largest first) and runs that instance's whole PCG: the cluster's CTAs own
+// contiguous shares of its rows, phases are separated by cluster barriers,
+// and every reduction sums the CTAs' partials through distributed shared
+// memory in rank order, so instances converge, stop and report independently
+// and no grid-wide synchronisation exists. The arithmetic per instance is
+// that of the library's single-system PCG (cg.rs:40-149 for FP64; for mixed,
+// FP32 difference-form operator with FP64 r, x and dots and FP64 residual
 // replacement). The launch is captured in a CUDA graph together with the
-// queue reset, and the graph is replayed on later solves. Lanes per row and
-// threads per CTA are picked by timing the candidates on the batch itself
-// (first solve of a matrix and precision), unless FCU_BATCH_VPR /
-// FCU_BATCH_THREADS fix them.
+// queue reset, and the graph is replayed on later solves. Lanes per row,
+// threads per CTA and CTAs per cluster are picked by timing the candidates on
+// the batch itself (first solve of a matrix and precision), unless
+// FCU_BATCH_VPR / FCU_BATCH_THREADS / FCU_BATCH_CLUSTER fix them; a single
+// system (the small-system path of the PCG) takes a shape fixed by rule.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
