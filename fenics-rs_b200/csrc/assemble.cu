@@ -7,13 +7,21 @@
 //                  is the (3i+alpha, 3j+beta) entry of block slot p = (i, j)
 // Both FP64 and FP32 values are written by the same pass.
 //
-// Work decomposition: one warp per row. The warp first evaluates, for each
-// cell that contains the row's node (the row's "contributions", ascending
-// cell id), that cell's element row into shared memory; then each lane owns a
-// slot and sums the entries listed for it, in ascending cell order; finally
-// the row is written with coalesced stores. Each cell is evaluated once per
-// node it has (k times), and every value is written exactly once, so no
-// atomics and no zero-fill pass are needed, and the result is deterministic.
+// Work decomposition: rows are owned, never scattered into, so every value
+// is written exactly once, with no atomics and no zero-fill pass, and every
+// sum runs in a fixed order (the results repeat bit for bit).
+//   * scalar P1 (and the row-gather forms kept for comparison): one warp per
+//     row evaluates each of the row's cells' element rows into shared memory
+//     (the row's "contributions", ascending cell id), then each lane sums the
+//     entries of its slot in ascending cell order;
+//   * P2: per-cell metric records, then three rows per warp, a lane per local
+//     column, adding each contribution's entry into the row's shared-memory
+//     accumulators (k_assemble_p2_rows);
+//   * vector-P1 elasticity and mass: per-cell records (gradients and scale,
+//     or the scale alone), then one lane per off-diagonal 3x3 block summing
+//     the block's cell list, the diagonal block from the row (k_elast_rows,
+//     k_mass_rows_vec).
+// Rows are written with coalesced stores in every form.
 
 #include "internal.cuh"
 

@@ -35,6 +35,14 @@
 // programmatic dependent launch so each kernel is scheduled while its
 // predecessor drains; kernels of a finished solve return at once. The host
 // reads the state once per replay while the next replay is already queued.
+//
+// Mixed solves on 3x3-block matrices (and FP64 ones with FCU_PERSISTENT=2)
+// run instead as the persistent loop k_pcg_persistent: one cooperative launch
+// per stretch between residual replacements, the tiled SpMV's CTAs resident
+// throughout, two bounded grid barriers per iteration in place of kernel
+// boundaries, and the direction formed from (z, p) pairs where the product
+// reads them. Small scalar systems go to the batched kernel as a single
+// instance (batch.cu).
 
 #include <algorithm>
 #include <atomic>
