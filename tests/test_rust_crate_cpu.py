@@ -164,3 +164,18 @@ def test_crate_manifest_and_build_script():
     assert 'name = "fenics-cuda"' in toml and 'links = "fenics_cuda"' in toml
     build = open(os.path.join(CRATE, "build.rs")).read()
     assert "rustc-link-lib=dylib=fenics_cuda" in build
+
+
+def test_integration_reexports_exist_in_crate():
+    """Every item the integration recipe re-exports from the crate
+    (`pub use fenics_cuda::{...}`) is defined public in src/lib.rs."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    doc = open(os.path.join(root, "INTEGRATION.md")).read()
+    lib = open(os.path.join(root, "crates", "fenics-cuda", "src", "lib.rs")).read()
+    names = set()
+    for block in re.findall(r"pub use fenics_cuda::\{([^}]*)\}", doc):
+        names.update(n.strip() for n in block.split(",") if n.strip())
+    assert len(names) >= 15
+    defined = set(re.findall(r"^pub (?:fn|struct|enum) (\w+)", lib, flags=re.M))
+    assert not sorted(names - defined), sorted(names - defined)
